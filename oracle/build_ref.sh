@@ -1,0 +1,31 @@
+#!/bin/sh
+# Builds oracle/_ref/libgxref.so from the reference's own hot-path sources,
+# compiled in place from a reference checkout (default: the path in
+# GX_REFERENCE_ROOT), through the headers in oracle/refshim.  Test
+# infrastructure only: the library pins the oracle and generates the golden
+# vectors.  The reference's own build system is not used (it needs cmake and
+# its empty VecCore/VecGeom/PTL/timemory submodules).
+set -e
+REF=${1:-${GX_REFERENCE_ROOT:-/root/reference}}
+HERE=$(cd "$(dirname "$0")" && pwd)
+OUT="$HERE/_ref"
+SRC="$REF/source/Geant"
+if [ ! -d "$SRC" ]; then
+  echo "build_ref.sh: no reference checkout at $REF" >&2
+  exit 2
+fi
+mkdir -p "$OUT"
+# link the system libstdc++ dynamically: a static copy inside a library that a
+# Python process loads next to another libstdc++ crashes in iostream set-up
+STDCXX=$(${CXX:-g++} -print-file-name=libstdc++.so.6)
+case "$STDCXX" in /*) ;; *) STDCXX=/usr/lib/x86_64-linux-gnu/libstdc++.so.6 ;; esac
+${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
+  -I"$HERE/refshim" -I"$REF/source" \
+  "$HERE/refshim/ref_capi.cpp" \
+  "$SRC/random/src/MRG32k3a.cpp" \
+  "$SRC/proxy/src/Proxy2DVector.cpp" \
+  "$SRC/proxy/src/ProxyPhysicsVector.cu" \
+  "$SRC/proxy/src/ProxyPhysicsTable.cu" \
+  "$SRC/proxy/src/ProxyDataManager.cu" \
+  -x none "$STDCXX" -lm -o "$OUT/libgxref.so"
+echo "built $OUT/libgxref.so"

@@ -1,0 +1,213 @@
+/*
+ * gxo.h -- ORACLE (test infrastructure only).
+ *
+ * A plain-C, scalar CPU restatement of the reference's electromagnetic
+ * particle-transport step path (Geant-RnD/GeantExascalePilot).  It is the
+ * checker for the CUDA product in geantexascalepilot_b200/: only the tests,
+ * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, and never
+ * as the thing measured or shipped.
+ *
+ * Each function cites the reference file:line it restates.  Parity of this
+ * restatement is pinned against the reference's own code compiled in place
+ * (oracle/refshim + oracle/build_ref.sh -> oracle/_ref/libgxref.so); the
+ * generated golden vectors live in tests/golden/.
+ *
+ * Units: mm, MeV, ns (the reference's CLHEP units,
+ * source/Geant/proxy/ProxySystemOfUnits.hpp); magnetic field in tesla.
+ */
+#ifndef GXO_H
+#define GXO_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- MRG32k3a */
+/* source/Geant/random/MRG32k3a.hpp:45-49 -- state is six FP64 integers. */
+typedef struct { double s[6]; } gxo_mrg_t;
+
+double gxo_mrg_u01(gxo_mrg_t *r);                        /* MRG32k3a.cpp:124-163 */
+uint32_t gxo_mrg_next_raw(gxo_mrg_t *r);                 /* numerator of the draw */
+void gxo_mrg_advance(gxo_mrg_t *r, long e, long c);      /* MRG32k3a.cpp:171-178 */
+void gxo_mrg_next_stream(double seed[6], gxo_mrg_t *r);  /* MRG32k3a.cpp:52-58 */
+void gxo_mrg_next_substream(double bg[6], gxo_mrg_t *r); /* MRG32k3a.cpp:61-67 */
+void gxo_mrg_init_stream_id(long id, gxo_mrg_t *r);      /* MRG32k3a.cpp:70-82 */
+void gxo_mrg_seed_child(gxo_mrg_t *parent, gxo_mrg_t *child);
+
+/* batch helpers for ctypes: states are n x 6 doubles, row-major */
+void gxo_mrg_uniform_batch(int n, int k, double *states, double *out);
+void gxo_mrg_substreams(const double seed[6], long first, int n, double *states);
+void gxo_mrg_advance_batch(int n, double *states, long e, long c);
+
+/* ------------------------------------------------------- physics vectors */
+/* source/Geant/proxy/ProxyPhysicsVector.cuh / src/ProxyPhysicsVector.cu */
+typedef struct {
+  int n, type;
+  double emin, emax, dbin, base;
+  double *x, *y, *d2;
+} gxo_pvec_t;
+
+enum {
+  GXO_DEDX_eBrem_em, GXO_DEDX_eBrem_ep, GXO_DEDX_eIoni_em, GXO_DEDX_eIoni_ep,
+  GXO_InverseRange_em, GXO_InverseRange_ep, GXO_Ionisation_em, GXO_Ionisation_ep,
+  GXO_Lambda_compt, GXO_Lambda_conv, GXO_Lambda_eBrem_em, GXO_Lambda_eBrem_ep,
+  GXO_Lambda_eIoni_em, GXO_Lambda_eIoni_ep, GXO_LambdaMod1_msc_em, GXO_LambdaMod1_msc_ep,
+  GXO_LambdaPrim_compt, GXO_LambdaPrim_phot, GXO_Range_em, GXO_Range_ep,
+  GXO_NTABLES
+};
+#define GXO_NMAT 3
+
+/* Seltzer-Berger 2-D table: source/Geant/proxy/Proxy2DVector.hpp:22-56 */
+typedef struct { double x[32]; double y[57]; double v[57][32]; } gxo_sb_t;
+
+typedef struct {
+  gxo_pvec_t vec[GXO_NTABLES][GXO_NMAT];
+  double cut_energy[4][GXO_NMAT]; /* [particle g,e-,e+,p][material], MeV */
+  double cut_length[4][GXO_NMAT]; /* mm */
+  double cut_raw[12];             /* file order, as the reference stores it */
+  gxo_sb_t sb_slot10;             /* br11: the reference's fDataSB[10] */
+  gxo_sb_t sb_ar, sb_pb;          /* br18, br82 */
+  int nshell[101], ishell[101];
+  double binding[1540];           /* eV */
+  int nint[101], cumint[101];
+  double sandia[981][5];
+} gxo_data_t;
+
+gxo_data_t *gxo_data_load(const char *datadir); /* NULL on failure */
+void gxo_data_free(gxo_data_t *d);
+double gxo_pvec_value(const gxo_pvec_t *v, double e);          /* PhysicsVector.cu:469-483 */
+double gxo_pvec_invrange_value(const gxo_pvec_t *v, double r); /* PhysicsVector.cu:491-524 */
+double gxo_table_value(const gxo_data_t *d, int table, int mat, double e);
+double gxo_table_invrange(const gxo_data_t *d, int table, int mat, double r);
+double gxo_sb_value(const gxo_sb_t *t, double x, double y);    /* Proxy2DVector.cpp:37-67 */
+double gxo_get_cut_value(const gxo_data_t *d, int index, int ipart); /* ProxyDataManager.cuh:52-54 */
+void gxo_table_value_batch(const gxo_data_t *d, int table, int mat, int n, const double *e, double *out);
+void gxo_table_invrange_batch(const gxo_data_t *d, int table, int mat, int n, const double *r, double *out);
+
+/* ------------------------------------------------------------ materials */
+typedef struct {
+  double Z, A, density;  /* g/mol, g/cm3 */
+  double n_atoms;        /* 1/mm3 */
+  double n_el;           /* electrons / mm3 */
+  double density_factor; /* Migdal constant x electron density (MeV^-2 scale) */
+} gxo_material_t;
+void gxo_material_make(double Z, double A, double density, gxo_material_t *m);
+
+/* ------------------------------------------------------ interaction I/O */
+/* The model entry points take the primary's kinetic energy and direction and
+ * return the updated primary plus up to two secondaries, as the reference's
+ * SampleSecondaries(TrackState*) does (source/Geant/proxy/ProxyEmModel.hpp:
+ * 79-83).  status: 0 alive, 1 killed. */
+typedef struct {
+  double E, dir[3], edep;
+  int status;
+  int nsec;
+  int sec_type[2];  /* 0 gamma, 1 e-, 2 e+ */
+  double sec_E[2], sec_dir[2][3];
+} gxo_inter_t;
+
+enum { GXO_MODE_QUIRK = 0, GXO_MODE_PHYSICS = 1 };
+typedef struct {
+  int mode;
+  int Z;                 /* element (quirk default 10) */
+  double cut;            /* production cut, MeV (model specific) */
+  double density_factor; /* SB dielectric suppression */
+  const gxo_sb_t *sb;    /* SB table used */
+  const gxo_data_t *data;
+  int charge;            /* -1 e-, +1 e+ for Moller/Bhabha */
+} gxo_model_params_t;
+
+void gxo_rotate_to_lab(double *u, double *v, double *w, double u1, double u2, double u3);
+
+int gxo_kn_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_sg_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_bh_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_sb_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_mb_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_bhabha_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+int gxo_annih_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io);
+double gxo_sg_photo_electron_energy(const gxo_data_t *d, int Z, double e, int mode);
+double gxo_kn_xs_per_atom(double Z, double e);     /* ProxyKleinNishina.hpp:62-93 */
+double gxo_mb_xs_per_atom(double Z, double e);     /* ProxyMollerScattering.hpp:61-89 */
+double gxo_annih_xs_per_electron(double e);
+double gxo_pe_xs_sandia(const gxo_data_t *d, int Z, double density, double e);
+double gxo_coulomb_factor(double Zeff);            /* ProxyEmModel.hpp:114-128 */
+
+/* models: 0 KN, 1 SG, 2 BH, 3 SB, 4 MB, 5 Bhabha, 6 annihilation */
+void gxo_interact_batch(int model, const gxo_model_params_t *p, int n, double *states,
+                        const double *E, const double *dir, double *E_out, double *dir_out,
+                        double *edep, int *status, int *nsec, int *sec_type, double *sec_E,
+                        double *sec_dir);
+
+/* ------------------------------------------------------------ processes */
+/* ProxyEmProcess<T>::PostStepGPIL, source/Geant/proxy/ProxyEmProcess.hpp:122-151 */
+double gxo_post_step_gpil(gxo_mrg_t *r, double lambda_inv, double pstep_prev, double *nil,
+                          double *inv_lambda_saved);
+/* ProxyIonization::AlongStepGPIL / AlongStepDoIt, ProxyIonization.hpp:108-168 */
+double gxo_ioni_along_gpil(const gxo_data_t *d, int mode, int charge, int mat, double e);
+void gxo_ioni_along_doit(const gxo_data_t *d, int mode, int charge, int mat, double step,
+                         double *e, double *edep);
+
+/* --------------------------------------------------------------- helix */
+/* ConstFieldHelixStepper::DoStep, source/Geant/magneticfield/ConstFieldHelixStepper.hpp:164-239 */
+void gxo_helix_dostep(const double B[3], const double pos[3], const double dir[3], double charge,
+                      double momentum, double step, double newpos[3], double newdir[3]);
+/* the same step in mm / MeV / tesla for a field along z (kB2C = -0.299792458) */
+void gxo_helix_dostep_mm(double Bz_tesla, const double pos[3], const double dir[3], double charge,
+                         double momentum, double step, double newpos[3], double newdir[3]);
+void gxo_helix_batch(const double B[3], int n, const double *pos, const double *dir,
+                     const double *charge, const double *mom, const double *step, double *newpos,
+                     double *newdir);
+
+/* ------------------------------------------------------------ transport */
+typedef struct {
+  int geometry;            /* 0: single box of material box_mat; 1: layered calorimeter */
+  int axis;                /* layering / box axis (0 x, 1 y, 2 z) */
+  int nlayers;
+  double t_abs, t_gap;     /* absorber (Pb) and gap (LAr) thickness, mm */
+  double half_trans;       /* half transverse size, mm */
+  double box_half[3];      /* geometry 0: half sizes; box centred at box_centre */
+  double box_centre[3];
+  int box_mat;
+  double Bz;               /* tesla, along z */
+  int charged_local;       /* 1: charged secondaries deposit locally (gamma-only transport) */
+  int max_steps;           /* per-track safety cap */
+  double seed[6];
+  long first_substream;    /* substream index of primary 0 */
+  int nthreads;
+  int score_events;        /* number of event tallies (>=1) */
+} gxo_config_t;
+
+typedef struct {
+  int type;         /* 0 gamma, 1 e-, 2 e+ */
+  double E, pos[3], dir[3];
+  int event;
+} gxo_primary_t;
+
+typedef struct {
+  double *edep;          /* [score_events][nvol] FP64 */
+  int nvol;
+  double escaped;        /* kinetic energy leaving the world */
+  long long steps;       /* track-steps (OneStep iterations) */
+  long long substeps;    /* field propagation sub-steps */
+  long long tracks;      /* tracks transported (primaries + secondaries) */
+  long long secondaries[3];
+  long long n_pair, n_annih;
+  long long errors;
+  int *primary_steps;    /* optional per-primary step count of the primary track */
+} gxo_result_t;
+
+int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
+                  const gxo_primary_t *prims, gxo_result_t *res);
+/* flat-array front end for ctypes */
+int gxo_transport_flat(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
+                       const int *type, const double *E, const double *pos, const double *dir,
+                       const int *event, double *edep, int nvol, double *escaped,
+                       long long *counters, int *primary_steps);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,36 @@
+import os
+import subprocess
+import sys
+
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+sys.path.insert(0, HERE)
+sys.path.insert(0, REPO)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200)")
+
+
+def _ensure_oracle():
+    so = os.path.join(REPO, "oracle", "liboracle.so")
+    if not os.path.exists(so):
+        subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle")])
+    return so
+
+
+@pytest.fixture(scope="session")
+def oracle():
+    _ensure_oracle()
+    from oracle_ctypes import Oracle
+    return Oracle()
+
+
+@pytest.fixture(scope="session")
+def golden():
+    import numpy as np
+    d = os.path.join(HERE, "golden")
+    return {k: np.load(os.path.join(d, k + ".npz")) for k in
+            ("mrg", "tables", "models_quirk", "xs", "processes", "helix")}

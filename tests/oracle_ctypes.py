@@ -1,0 +1,329 @@
+"""ctypes front ends for the two CPU checkers (test infrastructure).
+
+``Oracle`` wraps oracle/liboracle.so, the plain-C restatement of the
+reference's transport path.  ``Reference`` wraps oracle/_ref/libgxref.so,
+the reference's own code compiled in place (only present where a reference
+checkout was available at build time; its table and Seltzer-Berger entry
+points need the reference's data directory as working directory).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DATA_DIR = os.path.join(REPO, "geantexascalepilot_b200", "data")
+ORACLE_SO = os.path.join(REPO, "oracle", "liboracle.so")
+REF_SO = os.path.join(REPO, "oracle", "_ref", "libgxref.so")
+REF_DATA_CWD = os.path.join(os.environ.get("GX_REFERENCE_ROOT", "/root/reference"),
+                            "source/Geant/proxy/test/BasicCpuTransport")
+
+P = C.c_void_p
+D = C.c_double
+I = C.c_int
+L = C.c_long
+
+
+def dp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def ip(a):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def lp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_longlong))
+
+
+class ModelParams(C.Structure):
+    _fields_ = [("mode", I), ("Z", I), ("cut", D), ("density_factor", D), ("sb", P), ("data", P),
+                ("charge", I)]
+
+
+class Config(C.Structure):
+    _fields_ = [("geometry", I), ("axis", I), ("nlayers", I), ("t_abs", D), ("t_gap", D),
+                ("half_trans", D), ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I),
+                ("Bz", D), ("charged_local", I), ("max_steps", I), ("seed", D * 6),
+                ("first_substream", L), ("nthreads", I), ("score_events", I)]
+
+
+MODEL_IDS = {"kn": 0, "sg": 1, "bh": 2, "sb": 3, "mb": 4, "bhabha": 5, "annih": 6}
+# byte offsets of the SB tables inside gxo_data_t (computed from the struct layout)
+_NTABLES, _NMAT = 20, 3
+_PVEC_SIZE = 8 + 4 * 8 + 3 * 8  # n,type (2 ints) + 4 doubles + 3 pointers
+_SB_SIZE = (32 + 57 + 57 * 32) * 8
+_SB_OFF = _NTABLES * _NMAT * _PVEC_SIZE + (4 * _NMAT) * 8 * 2 + 12 * 8
+
+
+class Oracle:
+    def __init__(self, path=ORACLE_SO, datadir=DATA_DIR):
+        if not os.path.exists(path):
+            raise RuntimeError("oracle library missing: %s (run __graft_entry__.build())" % path)
+        self.lib = lib = C.CDLL(path)
+        lib.gxo_data_load.restype = P
+        lib.gxo_data_load.argtypes = [C.c_char_p]
+        lib.gxo_mrg_uniform_batch.argtypes = [I, I, C.POINTER(D), C.POINTER(D)]
+        lib.gxo_mrg_substreams.argtypes = [C.POINTER(D), L, I, C.POINTER(D)]
+        lib.gxo_mrg_advance_batch.argtypes = [I, C.POINTER(D), L, L]
+        lib.gxo_mrg_init_stream_id.argtypes = [L, C.POINTER(D)]
+        lib.gxo_mrg_next_stream.argtypes = [C.POINTER(D), C.POINTER(D)]
+        lib.gxo_table_value_batch.argtypes = [P, I, I, I, C.POINTER(D), C.POINTER(D)]
+        lib.gxo_table_invrange_batch.argtypes = [P, I, I, I, C.POINTER(D), C.POINTER(D)]
+        lib.gxo_get_cut_value.restype = D
+        lib.gxo_get_cut_value.argtypes = [P, I, I]
+        lib.gxo_sb_value.restype = D
+        lib.gxo_sb_value.argtypes = [P, D, D]
+        lib.gxo_interact_batch.argtypes = [I, C.POINTER(ModelParams), I] + [C.POINTER(D)] * 6 + [
+            C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(D), C.POINTER(D)]
+        for f in ("gxo_kn_xs_per_atom", "gxo_mb_xs_per_atom"):
+            getattr(lib, f).restype = D
+            getattr(lib, f).argtypes = [D, D]
+        lib.gxo_annih_xs_per_electron.restype = D
+        lib.gxo_annih_xs_per_electron.argtypes = [D]
+        lib.gxo_coulomb_factor.restype = D
+        lib.gxo_coulomb_factor.argtypes = [D]
+        lib.gxo_sg_photo_electron_energy.restype = D
+        lib.gxo_sg_photo_electron_energy.argtypes = [P, I, D, I]
+        lib.gxo_pe_xs_sandia.restype = D
+        lib.gxo_pe_xs_sandia.argtypes = [P, I, D, D]
+        lib.gxo_post_step_gpil.restype = D
+        lib.gxo_post_step_gpil.argtypes = [C.POINTER(D), D, D, C.POINTER(D), C.POINTER(D)]
+        lib.gxo_ioni_along_gpil.restype = D
+        lib.gxo_ioni_along_gpil.argtypes = [P, I, I, I, D]
+        lib.gxo_ioni_along_doit.argtypes = [P, I, I, I, D, C.POINTER(D), C.POINTER(D)]
+        lib.gxo_helix_batch.argtypes = [C.POINTER(D), I] + [C.POINTER(D)] * 7
+        lib.gxo_helix_dostep_mm.argtypes = [D] + [C.POINTER(D)] * 2 + [D, D, D] + [C.POINTER(D)] * 2
+        lib.gxo_transport_flat.restype = I
+        lib.gxo_transport_flat.argtypes = [P, C.POINTER(Config), I, C.POINTER(I), C.POINTER(D), C.POINTER(D),
+                                           C.POINTER(D), C.POINTER(I), C.POINTER(D), I, C.POINTER(D),
+                                           C.POINTER(C.c_longlong), C.POINTER(I)]
+        self.data = lib.gxo_data_load(datadir.encode())
+        if not self.data:
+            raise RuntimeError("oracle could not load physics data from %s" % datadir)
+
+    # ------------------------------------------------------------ RNG
+    def mrg_draws(self, states, k):
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6).copy()
+        out = np.zeros((k, st.shape[0]))
+        self.lib.gxo_mrg_uniform_batch(st.shape[0], k, dp(st), dp(out))
+        return out, st
+
+    def substreams(self, seed, first, n):
+        s = np.ascontiguousarray(seed, dtype=np.float64)
+        out = np.zeros((n, 6))
+        self.lib.gxo_mrg_substreams(dp(s), first, n, dp(out))
+        return out
+
+    def advance(self, states, e, c):
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6).copy()
+        self.lib.gxo_mrg_advance_batch(st.shape[0], dp(st), e, c)
+        return st
+
+    def stream_id_state(self, sid):
+        s = np.zeros(6)
+        self.lib.gxo_mrg_init_stream_id(sid, dp(s))
+        return s
+
+    # ----------------------------------------------------------- tables
+    def table_value(self, table, mat, e):
+        e = np.ascontiguousarray(e, dtype=np.float64)
+        out = np.zeros_like(e)
+        self.lib.gxo_table_value_batch(self.data, table, mat, e.size, dp(e), dp(out))
+        return out
+
+    def table_invrange(self, table, mat, r):
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        out = np.zeros_like(r)
+        self.lib.gxo_table_invrange_batch(self.data, table, mat, r.size, dp(r), dp(out))
+        return out
+
+    def cut_value(self, index, ipart):
+        return self.lib.gxo_get_cut_value(self.data, index, ipart)
+
+    def sb_table_ptr(self, which):
+        """which: 'slot10' (br11), 'ar' (br18), 'pb' (br82)"""
+        k = {"slot10": 0, "ar": 1, "pb": 2}[which]
+        return C.c_void_p(self.data + _SB_OFF + k * _SB_SIZE)
+
+    def sb_value(self, which, x, y):
+        return self.lib.gxo_sb_value(self.sb_table_ptr(which), x, y)
+
+    # ----------------------------------------------------------- models
+    def params(self, mode=0, Z=10, cut=0.0, density_factor=0.0, sb="slot10", charge=-1):
+        return ModelParams(mode, Z, cut, density_factor, self.sb_table_ptr(sb), self.data, charge)
+
+    def interact(self, model, states, E, dirs, params):
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6).copy()
+        n = st.shape[0]
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(n, 3)
+        out = dict(E=np.zeros(n), dir=np.zeros((n, 3)), edep=np.zeros(n), status=np.zeros(n, np.int32),
+                   nsec=np.zeros(n, np.int32), sec_type=np.zeros((n, 2), np.int32), sec_E=np.zeros((n, 2)),
+                   sec_dir=np.zeros((n, 2, 3)))
+        self.lib.gxo_interact_batch(MODEL_IDS[model], C.byref(params), n, dp(st), dp(E), dp(dirs), dp(out["E"]),
+                                    dp(out["dir"]), dp(out["edep"]), ip(out["status"]), ip(out["nsec"]),
+                                    ip(out["sec_type"]), dp(out["sec_E"]), dp(out["sec_dir"]))
+        out["states"] = st
+        return out
+
+    # ------------------------------------------------------- processes
+    def post_step_gpil(self, state, lam, pstep_prev, nil, saved):
+        st = np.ascontiguousarray(state, dtype=np.float64).copy()
+        nil_c, saved_c = D(nil), D(saved)
+        step = self.lib.gxo_post_step_gpil(dp(st), lam, pstep_prev, C.byref(nil_c), C.byref(saved_c))
+        return step, nil_c.value, saved_c.value, st
+
+    def ioni_along_gpil(self, mode, charge, mat, e):
+        return self.lib.gxo_ioni_along_gpil(self.data, mode, charge, mat, e)
+
+    def ioni_along_doit(self, mode, charge, mat, step, e):
+        ec, ed = D(e), D(0.0)
+        self.lib.gxo_ioni_along_doit(self.data, mode, charge, mat, step, C.byref(ec), C.byref(ed))
+        return ec.value, ed.value
+
+    def helix(self, B, pos, dirs, charge, mom, step):
+        n = len(charge)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (pos, dirs, charge, mom, step)]
+        npos, ndir = np.zeros((n, 3)), np.zeros((n, 3))
+        self.lib.gxo_helix_batch(dp(B), n, *[dp(a) for a in args], dp(npos), dp(ndir))
+        return npos, ndir
+
+    # -------------------------------------------------------- transport
+    def transport(self, cfg, types, E, pos, dirs, events=None, nvol=1, nevents=1):
+        n = len(types)
+        types = np.ascontiguousarray(types, dtype=np.int32)
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(n, 3)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(n, 3)
+        ev = np.ascontiguousarray(events if events is not None else np.zeros(n), dtype=np.int32)
+        edep = np.zeros((nevents, nvol))
+        esc = D(0.0)
+        counters = np.zeros(9, dtype=np.int64)
+        psteps = np.zeros(n, dtype=np.int32)
+        rc = self.lib.gxo_transport_flat(self.data, C.byref(cfg), n, ip(types), dp(E), dp(pos), dp(dirs), ip(ev),
+                                         dp(edep), nvol, C.byref(esc), lp(counters), ip(psteps))
+        assert rc == 0
+        names = ["steps", "substeps", "tracks", "sec_gamma", "sec_electron", "sec_positron", "n_pair", "n_annih",
+                 "errors"]
+        res = dict(zip(names, [int(c) for c in counters]))
+        res.update(edep=edep, escaped=esc.value, primary_steps=psteps)
+        return res
+
+
+class Reference:
+    """The reference's own code (oracle/_ref/libgxref.so)."""
+
+    def __init__(self, path=REF_SO):
+        if not os.path.exists(path):
+            raise RuntimeError("reference harness missing: %s" % path)
+        self.lib = lib = C.CDLL(path)
+        lib.gxref_mrg_draws.argtypes = [C.POINTER(D), I, C.POINTER(D), C.POINTER(D)]
+        lib.gxref_mrg_stream_id.argtypes = [L, I, C.POINTER(D)]
+        lib.gxref_mrg_advance.argtypes = [C.POINTER(D), L, L]
+        lib.gxref_tables_init.restype = I
+        for f in ("gxref_table_value", "gxref_table_invrange"):
+            getattr(lib, f).restype = D
+            getattr(lib, f).argtypes = [I, I, D]
+        lib.gxref_cut_value.restype = D
+        lib.gxref_cut_value.argtypes = [I, I]
+        lib.gxref_sb2d_value.restype = D
+        lib.gxref_sb2d_value.argtypes = [I, D, D]
+        lib.gxref_interact.argtypes = [I, I] + [C.POINTER(D)] * 6 + [C.POINTER(I)] * 3 + [C.POINTER(D)] * 2
+        for f in ("gxref_kn_xs", "gxref_mb_xs"):
+            getattr(lib, f).restype = D
+            getattr(lib, f).argtypes = [D, D]
+        lib.gxref_sg_photo_energy.restype = D
+        lib.gxref_sg_photo_energy.argtypes = [I, D]
+        lib.gxref_coulomb.restype = D
+        lib.gxref_coulomb.argtypes = [D]
+        lib.gxref_post_step_gpil.restype = D
+        lib.gxref_post_step_gpil.argtypes = [I, C.POINTER(D), D, D, C.POINTER(D), C.POINTER(D), I]
+        lib.gxref_ioni_along_gpil.restype = D
+        lib.gxref_ioni_along_gpil.argtypes = [I, D]
+        lib.gxref_ioni_along_doit.argtypes = [I, D, C.POINTER(D), C.POINTER(D)]
+        lib.gxref_helix.argtypes = [C.POINTER(D), I] + [C.POINTER(D)] * 7
+        self._cwd_ready = False
+
+    def _in_data_dir(self, fn, *a):
+        old = os.getcwd()
+        os.chdir(REF_DATA_CWD)
+        try:
+            return fn(*a)
+        finally:
+            os.chdir(old)
+
+    def mrg_draws(self, seed, k):
+        s = np.ascontiguousarray(seed, dtype=np.float64)
+        out, st = np.zeros(k), np.zeros(6)
+        self.lib.gxref_mrg_draws(dp(s), k, dp(out), dp(st))
+        return out, st
+
+    def stream_id_draws(self, sid, k):
+        out = np.zeros(k)
+        self.lib.gxref_mrg_stream_id(sid, k, dp(out))
+        return out
+
+    def advance(self, state, e, c):
+        s = np.ascontiguousarray(state, dtype=np.float64).copy()
+        self.lib.gxref_mrg_advance(dp(s), e, c)
+        return s
+
+    def init_tables(self):
+        return self._in_data_dir(self.lib.gxref_tables_init)
+
+    def table_value(self, table, mat, e):
+        self.init_tables()
+        return np.array([self.lib.gxref_table_value(table, mat, float(x)) for x in np.atleast_1d(e)])
+
+    def table_invrange(self, table, mat, r):
+        self.init_tables()
+        return np.array([self.lib.gxref_table_invrange(table, mat, float(x)) for x in np.atleast_1d(r)])
+
+    def cut_value(self, index, ipart):
+        self.init_tables()
+        return self.lib.gxref_cut_value(index, ipart)
+
+    def sb2d_value(self, Z, x, y):
+        return self._in_data_dir(self.lib.gxref_sb2d_value, Z, x, y)
+
+    def interact(self, model, states, E, dirs):
+        st = np.ascontiguousarray(states, dtype=np.float64).reshape(-1, 6).copy()
+        n = st.shape[0]
+        E = np.ascontiguousarray(E, dtype=np.float64)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(n, 3)
+        out = dict(E=np.zeros(n), dir=np.zeros((n, 3)), edep=np.zeros(n), status=np.zeros(n, np.int32),
+                   nsec=np.zeros(n, np.int32), sec_type=np.zeros((n, 2), np.int32), sec_E=np.zeros((n, 2)),
+                   sec_dir=np.zeros((n, 2, 3)))
+        self._in_data_dir(self.lib.gxref_interact, MODEL_IDS[model], n, dp(st), dp(E), dp(dirs), dp(out["E"]),
+                          dp(out["dir"]), dp(out["edep"]), ip(out["status"]), ip(out["nsec"]),
+                          ip(out["sec_type"]), dp(out["sec_E"]), dp(out["sec_dir"]))
+        out["states"] = st
+        return out
+
+    def post_step_gpil(self, process, state, e, pstep_prev, nil, saved, mat=2):
+        self.init_tables()
+        st = np.ascontiguousarray(state, dtype=np.float64).copy()
+        nil_c, saved_c = D(nil), D(saved)
+        step = self._in_data_dir(self.lib.gxref_post_step_gpil, process, dp(st), e, pstep_prev, C.byref(nil_c),
+                                 C.byref(saved_c), mat)
+        return step, nil_c.value, saved_c.value, st
+
+    def ioni_along_gpil(self, mat, e):
+        self.init_tables()
+        return self._in_data_dir(self.lib.gxref_ioni_along_gpil, mat, e)
+
+    def ioni_along_doit(self, mat, step, e):
+        self.init_tables()
+        ec, ed = D(e), D(0.0)
+        self._in_data_dir(self.lib.gxref_ioni_along_doit, mat, step, C.byref(ec), C.byref(ed))
+        return ec.value, ed.value
+
+    def helix(self, B, pos, dirs, charge, mom, step):
+        n = len(charge)
+        B = np.ascontiguousarray(B, dtype=np.float64)
+        args = [np.ascontiguousarray(a, dtype=np.float64) for a in (pos, dirs, charge, mom, step)]
+        npos, ndir = np.zeros((n, 3)), np.zeros((n, 3))
+        self.lib.gxref_helix(dp(B), n, *[dp(a) for a in args], dp(npos), dp(ndir))
+        return npos, ndir
