@@ -1,0 +1,100 @@
+"""ctypes binding of libgxb200.so (the C ABI declared in include/gx_abi.h).
+
+The library is the product: there is no fallback.  If it is missing the
+import of the package raises, and every call checks the returned status and
+raises ``GxError`` with the library's own message.
+"""
+import ctypes as C
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libgxb200.so")
+DATA_DIR = os.path.join(PKG, "data")
+
+GX_OK, GX_ERR_ARG, GX_ERR_CUDA, GX_ERR_DATA, GX_ERR_OVERFLOW, GX_ERR_ITERCAP, GX_ERR_NODEVICE = 0, -1, -2, -3, -4, -5, -6
+
+
+class GxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("gx error %d: %s" % (code, msg))
+        self.code = code
+
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError("libgxb200.so is not built (%s); run __graft_entry__.build() or "
+                      "python geantexascalepilot_b200/build.py" % LIB_PATH)
+
+lib = C.CDLL(LIB_PATH)
+
+P = C.c_void_p
+I = C.c_int
+D = C.c_double
+LL = C.c_longlong
+PD = C.POINTER(C.c_double)
+
+
+class ModelParams(C.Structure):
+    _fields_ = [("mode", I), ("Z", I), ("cut", D), ("density_factor", D), ("sb_table", I)]
+
+
+class TransportConfig(C.Structure):
+    _fields_ = [("geometry", I), ("axis", I), ("nlayers", I), ("t_abs", D), ("t_gap", D), ("half_trans", D),
+                ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I), ("Bz", D), ("charged_local", I),
+                ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
+                ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
+                ("graph_iters", I), ("profile", I)]
+
+
+class TransportStats(C.Structure):
+    _fields_ = [("steps", LL), ("substeps", LL), ("tracks", LL), ("secondaries", LL * 3), ("n_pair", LL),
+                ("n_annih", LL), ("errors", LL), ("escaped", D), ("iterations", LL), ("peak_in_flight", LL),
+                ("kernel_ms", D), ("step_ms", D * 3), ("step_launches", LL * 3), ("tracks_read", LL * 3),
+                ("tracks_written", LL * 3), ("bytes_per_track", LL)]
+
+    def as_dict(self):
+        return {"steps": self.steps, "substeps": self.substeps, "tracks": self.tracks,
+                "sec_gamma": self.secondaries[0], "sec_electron": self.secondaries[1],
+                "sec_positron": self.secondaries[2], "n_pair": self.n_pair, "n_annih": self.n_annih,
+                "errors": self.errors, "escaped": self.escaped, "iterations": self.iterations,
+                "peak_in_flight": self.peak_in_flight, "kernel_ms": self.kernel_ms,
+                "step_ms": list(self.step_ms), "step_launches": list(self.step_launches),
+                "tracks_read": list(self.tracks_read), "tracks_written": list(self.tracks_written),
+                "bytes_per_track": self.bytes_per_track}
+
+
+_SIGS = {
+    "gx_last_error_string": (C.c_char_p, []),
+    "gx_version": (I, []),
+    "gx_ctx_create": (I, [C.c_char_p, I, C.POINTER(P)]),
+    "gx_ctx_destroy": (I, [P]),
+    "gx_rng_substreams": (I, [PD, LL, I, P, P]),
+    "gx_rng_advance": (I, [P, I, LL, LL, P]),
+    "gx_rng_uniform": (I, [P, I, I, P, P]),
+    "gx_rng_stream_id": (I, [C.POINTER(LL), I, P, P]),
+    "gx_table_value": (I, [P, I, I, P, P, I, P]),
+    "gx_table_invrange": (I, [P, I, I, P, P, I, P]),
+    "gx_sb_value": (I, [P, I, P, P, P, I, P]),
+    "gx_cut_value": (I, [P, I, I, PD]),
+    "gx_interact": (I, [P, I, C.POINTER(ModelParams), I] + [P] * 11 + [P]),
+    "gx_xs_per_atom": (I, [I, D, P, P, I, P]),
+    "gx_post_step_gpil": (I, [P, I, I, I] + [P] * 6 + [P]),
+    "gx_ioni_along_gpil": (I, [P, I, I, P, P, P, I, P]),
+    "gx_ioni_along_doit": (I, [P, I, I, P, P, P, P, I, P]),
+    "gx_helix_dostep": (I, [PD, D, I] + [P] * 15 + [P]),
+    "gx_transport_config_default": (None, [C.POINTER(TransportConfig)]),
+    "gx_transport_run": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P, C.POINTER(TransportStats), P]),
+    "gx_transport_run_host": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P,
+                                  C.POINTER(TransportStats)]),
+}
+for _name, (_res, _args) in _SIGS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+EXPORTED = sorted(_SIGS)
+
+
+def check(rc):
+    if rc != GX_OK:
+        raise GxError(rc, lib.gx_last_error_string().decode(errors="replace"))
+    return rc

@@ -1,0 +1,312 @@
+"""Host-side mirror of the reference's interfaces for the EM transport path.
+
+Class and method names follow the reference (ProxyDataManager, MRG32k3a,
+Proxy<Model>::SampleSecondaries, Proxy<Process>::PostStepGPIL,
+ConstFieldHelixStepper::DoStepArr, ...) but every method works on a batch of
+tracks held in torch CUDA tensors and calls the CUDA kernels through the C ABI
+(include/gx_abi.h).  There is no CPU path: without a CUDA device the context
+cannot be created and every call raises.
+"""
+import ctypes as C
+
+import torch
+
+from . import _lib
+from ._lib import GxError, ModelParams, TransportConfig, TransportStats, check, lib
+
+# physics-table ids (ProxyPhysicsTableIndex.hpp:23-45)
+TABLES = ["DEDX.eBrem.e-", "DEDX.eBrem.e+", "DEDX.eIoni.e-", "DEDX.eIoni.e+", "InverseRange.eIoni.e-",
+          "InverseRange.eIoni.e+", "Ionisation.eIoni.e-", "Ionisation.eIoni.e+", "Lambda.compt.gamma",
+          "Lambda.conv.gamma", "Lambda.eBrem.e-", "Lambda.eBrem.e+", "Lambda.eIoni.e-", "Lambda.eIoni.e+",
+          "LambdaMod1.msc.e-", "LambdaMod1.msc.e+", "LambdaPrim.compt.gamma", "LambdaPrim.phot.gamma",
+          "Range.eIoni.e-", "Range.eIoni.e+"]
+KLEIN_NISHINA, SAUTER_GAVRILA, BETHE_HEITLER, SELTZER_BERGER, MOLLER, BHABHA, ANNIHILATION = range(7)
+MODE_QUIRK, MODE_PHYSICS = 0, 1
+GAMMA, ELECTRON, POSITRON = 0, 1, 2
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _dev(x, dtype):
+    if isinstance(x, torch.Tensor):
+        return x.to(device="cuda", dtype=dtype).contiguous()
+    return torch.as_tensor(x, dtype=dtype, device="cuda").contiguous()
+
+
+class ProxyDataManager:
+    """Physics tables, cuts and Seltzer-Berger data on one device
+    (ProxyDataManager, source/Geant/proxy/ProxyDataManager.cuh:27-83)."""
+
+    def __init__(self, datadir=_lib.DATA_DIR, device=0):
+        h = C.c_void_p()
+        check(lib.gx_ctx_create(datadir.encode(), device, C.byref(h)))
+        self.handle = h
+        self.device = device
+
+    def close(self):
+        if self.handle:
+            lib.gx_ctx_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ProxyPhysicsTable::Value(index, E) of table `table`
+    def table_value(self, table, mat, E):
+        E = _dev(E, torch.float64)
+        out = torch.empty_like(E)
+        check(lib.gx_table_value(self.handle, table, mat, _ptr(E), _ptr(out), E.numel(), _stream()))
+        return out
+
+    # ProxyPhysicsVector::InvRangeValue
+    def inv_range_value(self, table, mat, r):
+        r = _dev(r, torch.float64)
+        out = torch.empty_like(r)
+        check(lib.gx_table_invrange(self.handle, table, mat, _ptr(r), _ptr(out), r.numel(), _stream()))
+        return out
+
+    # Proxy2DVector::Value on SB table 0 (br11), 1 (br18), 2 (br82)
+    def sb_value(self, which, x, y):
+        x = _dev(x, torch.float64)
+        y = _dev(y, torch.float64)
+        out = torch.empty_like(x)
+        check(lib.gx_sb_value(self.handle, which, _ptr(x), _ptr(y), _ptr(out), x.numel(), _stream()))
+        return out
+
+    def GetCutValue(self, index, ipart):
+        v = C.c_double()
+        check(lib.gx_cut_value(self.handle, index, ipart, C.byref(v)))
+        return v.value
+
+
+class MRG32k3a:
+    """Batches of MRG32k3a streams as (6, n) uint32 CUDA tensors
+    (source/Geant/random/MRG32k3a.hpp)."""
+
+    @staticmethod
+    def substreams(seed, first, n):
+        s = (C.c_double * 6)(*[float(v) for v in seed])
+        out = torch.empty((6, n), dtype=torch.int32, device="cuda")
+        check(lib.gx_rng_substreams(s, first, n, _ptr(out), _stream()))
+        return out
+
+    @staticmethod
+    def from_states(states):
+        """n x 6 array of the reference's FP64 words -> (6, n) device tensor"""
+        t = torch.as_tensor(states, dtype=torch.float64).reshape(-1, 6).t().contiguous()
+        return t.to(torch.int64).to(torch.int32).cuda()
+
+    @staticmethod
+    def to_states(t):
+        """(6, n) device tensor -> n x 6 float64 CPU tensor of the six integers"""
+        return (t.cpu().to(torch.int64) & 0xFFFFFFFF).to(torch.float64).t().contiguous()
+
+    @staticmethod
+    def uniform(states, k):
+        n = states.shape[1]
+        out = torch.empty((k, n), dtype=torch.float64, device="cuda")
+        check(lib.gx_rng_uniform(_ptr(states), n, k, _ptr(out), _stream()))
+        return out
+
+    @staticmethod
+    def advance(states, e, c):
+        check(lib.gx_rng_advance(_ptr(states), states.shape[1], e, c, _stream()))
+        return states
+
+    @staticmethod
+    def stream_id(ids):
+        ids = list(ids)
+        arr = (C.c_longlong * len(ids))(*ids)
+        out = torch.empty((6, len(ids)), dtype=torch.int32, device="cuda")
+        check(lib.gx_rng_stream_id(arr, len(ids), _ptr(out), _stream()))
+        return out
+
+
+class _Model:
+    model_id = -1
+
+    def __init__(self, dm, mode=MODE_QUIRK, Z=10, cut=0.0, density_factor=0.0, sb_table=0):
+        self.dm = dm
+        self.params = ModelParams(mode, Z, cut, density_factor, sb_table)
+
+    def SampleSecondaries(self, E, direction, states):
+        """ProxyEmModel<T>::SampleSecondaries for a batch; states are advanced."""
+        E = _dev(E, torch.float64)
+        d = _dev(direction, torch.float64).reshape(-1, 3)
+        n = E.numel()
+        o = {"E": torch.empty(n, dtype=torch.float64, device="cuda"),
+             "dir": torch.empty((n, 3), dtype=torch.float64, device="cuda"),
+             "edep": torch.empty(n, dtype=torch.float64, device="cuda"),
+             "status": torch.empty(n, dtype=torch.int32, device="cuda"),
+             "nsec": torch.empty(n, dtype=torch.int32, device="cuda"),
+             "sec_type": torch.empty((n, 2), dtype=torch.int32, device="cuda"),
+             "sec_E": torch.empty((n, 2), dtype=torch.float64, device="cuda"),
+             "sec_dir": torch.empty((n, 2, 3), dtype=torch.float64, device="cuda")}
+        check(lib.gx_interact(self.dm.handle, self.model_id, C.byref(self.params), n, _ptr(states), _ptr(E), _ptr(d),
+                              _ptr(o["E"]), _ptr(o["dir"]), _ptr(o["edep"]), _ptr(o["status"]), _ptr(o["nsec"]),
+                              _ptr(o["sec_type"]), _ptr(o["sec_E"]), _ptr(o["sec_dir"]), _stream()))
+        return o
+
+    def CrossSectionPerAtom(self, Z, E):
+        E = _dev(E, torch.float64)
+        out = torch.empty_like(E)
+        check(lib.gx_xs_per_atom(self.model_id, float(Z), _ptr(E), _ptr(out), E.numel(), _stream()))
+        return out
+
+
+class ProxyKleinNishina(_Model):
+    model_id = KLEIN_NISHINA
+
+
+class ProxySauterGavrila(_Model):
+    model_id = SAUTER_GAVRILA
+
+
+class ProxyBetheHeitler(_Model):
+    model_id = BETHE_HEITLER
+
+
+class ProxySeltzerBerger(_Model):
+    model_id = SELTZER_BERGER
+
+
+class ProxyMollerScattering(_Model):
+    model_id = MOLLER
+
+
+class ProxyBhabhaScattering(_Model):
+    model_id = BHABHA
+
+
+class ProxyAnnihilation(_Model):
+    model_id = ANNIHILATION
+
+
+class _Process:
+    process_id = -1
+
+    def __init__(self, dm):
+        self.dm = dm
+
+    def PostStepGPIL(self, E, pstep_prev, nil, saved, states, mat=2):
+        """ProxyEmProcess<T>::PostStepGPIL; nil and saved are updated in place."""
+        E = _dev(E, torch.float64)
+        ps = _dev(pstep_prev, torch.float64)
+        step = torch.empty_like(E)
+        check(lib.gx_post_step_gpil(self.dm.handle, self.process_id, mat, E.numel(), _ptr(states), _ptr(E), _ptr(ps),
+                                    _ptr(nil), _ptr(saved), _ptr(step), _stream()))
+        return step
+
+
+class ProxyCompton(_Process):
+    process_id = 0
+
+
+class ProxyConversion(_Process):
+    process_id = 1
+
+
+class ProxyPhotoElectric(_Process):
+    process_id = 2
+
+
+class ProxyBremsstrahlung(_Process):
+    process_id = 3
+
+
+class ProxyIonization(_Process):
+    process_id = 4
+
+    def AlongStepGPIL(self, mat, E, mode=MODE_QUIRK, charge=-1):
+        m = _dev(mat, torch.int32)
+        E = _dev(E, torch.float64)
+        out = torch.empty_like(E)
+        check(lib.gx_ioni_along_gpil(self.dm.handle, mode, charge, _ptr(m), _ptr(E), _ptr(out), E.numel(), _stream()))
+        return out
+
+    def AlongStepDoIt(self, mat, step, E, mode=MODE_QUIRK, charge=-1):
+        """returns (E after, energy deposited)"""
+        m = _dev(mat, torch.int32)
+        s = _dev(step, torch.float64)
+        E = _dev(E, torch.float64).clone()
+        edep = torch.zeros_like(E)
+        check(lib.gx_ioni_along_doit(self.dm.handle, mode, charge, _ptr(m), _ptr(s), _ptr(E), _ptr(edep), E.numel(),
+                                     _stream()))
+        return E, edep
+
+
+class ConstFieldHelixStepper:
+    """ConstFieldHelixStepper (source/Geant/magneticfield/ConstFieldHelixStepper.hpp)."""
+
+    def __init__(self, B, kB2C=-0.299792458e-3):
+        self.B = (C.c_double * 3)(*[float(b) for b in B])
+        self.kB2C = kB2C
+
+    def DoStepArr(self, pos, direction, charge, momentum, step):
+        pos = _dev(pos, torch.float64).reshape(-1, 3)
+        d = _dev(direction, torch.float64).reshape(-1, 3)
+        q = _dev(charge, torch.float64)
+        p = _dev(momentum, torch.float64)
+        s = _dev(step, torch.float64)
+        n = q.numel()
+        cols = [pos[:, k].contiguous() for k in range(3)] + [d[:, k].contiguous() for k in range(3)]
+        outs = [torch.empty(n, dtype=torch.float64, device="cuda") for _ in range(6)]
+        check(lib.gx_helix_dostep(self.B, self.kB2C, n, *[_ptr(c) for c in cols], _ptr(q), _ptr(p), _ptr(s),
+                                  *[_ptr(o) for o in outs], _stream()))
+        return torch.stack(outs[:3], 1), torch.stack(outs[3:], 1)
+
+
+def default_config():
+    cfg = TransportConfig()
+    lib.gx_transport_config_default(C.byref(cfg))
+    return cfg
+
+
+def transport(dm, cfg, types, E, pos, direction, events=None, nvol=None, primary_steps=False, edep=None):
+    """Transport primaries to completion (the reference's DoStep/OneStep loop).
+
+    Inputs are CUDA tensors (or array-likes copied to the device).  Returns
+    (edep [nevents, nvol] FP64 tensor, stats dict, per-primary step counts or None).
+    """
+    t = _dev(types, torch.int32)
+    E = _dev(E, torch.float64)
+    p = _dev(pos, torch.float64).reshape(-1, 3)
+    d = _dev(direction, torch.float64).reshape(-1, 3)
+    ev = _dev(events, torch.int32) if events is not None else None
+    n = t.numel()
+    if nvol is None:
+        nvol = 2 * cfg.nlayers if cfg.geometry == 1 else 1
+    if edep is None:
+        edep = torch.zeros((cfg.nevents, nvol), dtype=torch.float64, device="cuda")
+    ps = torch.zeros(n, dtype=torch.int32, device="cuda") if primary_steps else None
+    st = TransportStats()
+    check(lib.gx_transport_run(dm.handle, C.byref(cfg), n, _ptr(t), _ptr(E), _ptr(p), _ptr(d), _ptr(ev), _ptr(edep),
+                               nvol, _ptr(ps), C.byref(st), _stream()))
+    return edep, st.as_dict(), ps
+
+
+def transport_host(dm, cfg, types, E, pos, direction, events=None, nvol=None):
+    """The same from host (numpy) buffers; copies happen inside the call."""
+    import numpy as np
+    t = np.ascontiguousarray(types, dtype=np.int32)
+    E = np.ascontiguousarray(E, dtype=np.float64)
+    p = np.ascontiguousarray(pos, dtype=np.float64)
+    d = np.ascontiguousarray(direction, dtype=np.float64)
+    ev = np.ascontiguousarray(events, dtype=np.int32) if events is not None else None
+    if nvol is None:
+        nvol = 2 * cfg.nlayers if cfg.geometry == 1 else 1
+    edep = np.zeros((cfg.nevents, nvol))
+    st = TransportStats()
+    vp = lambda a: C.c_void_p(a.ctypes.data) if a is not None else None  # noqa: E731
+    check(lib.gx_transport_run_host(dm.handle, C.byref(cfg), t.size, vp(t), vp(E), vp(p), vp(d), vp(ev), vp(edep),
+                                    nvol, None, C.byref(st)))
+    return edep, st.as_dict()

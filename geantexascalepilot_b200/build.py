@@ -1,0 +1,86 @@
+"""Build the CUDA library of this package in-tree.
+
+Compiles every csrc/*.cu for sm_100a (B200) with nvcc and links
+geantexascalepilot_b200/lib/libgxb200.so.  Nothing is JIT-compiled at run
+time; the library is loaded with ctypes by geantexascalepilot_b200._lib.
+"""
+import concurrent.futures as cf
+import glob
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(PKG, "csrc")
+LIBDIR = os.path.join(PKG, "lib")
+BUILD = os.path.join(os.path.dirname(PKG), "_build")
+LIB = os.path.join(LIBDIR, "libgxb200.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xcompiler", "-Wno-unused-function"]
+
+
+def nvcc():
+    for c in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if c and os.path.exists(c):
+            return c
+    raise RuntimeError("nvcc not found")
+
+
+def system_libstdcxx():
+    """The shared libstdc++ the host process uses: a static copy inside a
+    library that is loaded next to another libstdc++ breaks iostream set-up."""
+    for c in ("/usr/lib/x86_64-linux-gnu/libstdc++.so.6", "/lib/x86_64-linux-gnu/libstdc++.so.6"):
+        if os.path.exists(c):
+            return c
+    return None
+
+
+# The per-function batch kernels reproduce the reference's FP64 arithmetic
+# operation by operation: no fused multiply-adds there, so they round like the
+# host code (only the transcendental functions differ).  The transport engine
+# keeps contraction.
+PER_FILE = {"gx_kernels.cu": ["-fmad=false"]}
+
+
+def _compile(src, verbose):
+    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+    deps = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(os.path.dirname(PKG), "include", "gx_abi.h"), src,
+                                                     os.path.abspath(__file__)]
+    if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
+        return obj, ""
+    extra = PER_FILE.get(os.path.basename(src), [])
+    cmd = [nvcc()] + ARCH + FLAGS + extra + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("nvcc failed for %s:\n%s\n%s" % (src, r.stdout, r.stderr))
+    return obj, r.stderr
+
+
+def build(verbose=False):
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+    with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
+        results = list(ex.map(lambda s: _compile(s, verbose), srcs))
+    objs = [o for o, _ in results]
+    if verbose:
+        for _, log in results:
+            if log:
+                print(log, file=sys.stderr)
+    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
+        return LIB
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+    cxx = system_libstdcxx()
+    if cxx:
+        cmd += ["-Xlinker", cxx]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv))

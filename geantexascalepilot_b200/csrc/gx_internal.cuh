@@ -1,0 +1,31 @@
+// gx_internal.cuh -- shared declarations of the C-ABI implementation files.
+#pragma once
+
+#include "../../include/gx_abi.h"
+#include "gx_device.cuh"
+
+#include <vector>
+
+namespace gx {
+
+struct Engine; // transport buffers, kept across calls (gx_transport.cu)
+
+struct Ctx {
+  int device = 0;
+  int num_sms = 148;
+  Data host;            // host copy (device pointers inside)
+  Data *dev = nullptr;  // device copy
+  std::vector<void *> owned;
+  Engine *engine = nullptr;
+};
+
+int set_error(int code, const char *fmt, ...);
+int cuda_error(cudaError_t e, const char *what);
+void jump_matrix(int comp, long long e, long long c, uint64_t out[9]);
+void mat_mul(const uint64_t A[9], const uint64_t B[9], uint64_t C[9], uint64_t m);
+void mat_vec(const uint64_t A[9], uint64_t v[3], uint64_t m);
+void release_engine(Ctx *c);
+
+inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
+
+} // namespace gx

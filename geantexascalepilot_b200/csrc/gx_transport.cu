@@ -1,0 +1,1255 @@
+// gx_transport.cu -- the transport engine: every alive track takes one step
+// per iteration, in FP64 or FP32-mixed arithmetic.
+//
+// Layout in HBM: per particle type (gamma, e-, e+) two SoA track stores of
+// `capacity` slots (current / next) and one overflow stack.  A step kernel
+// reads the current store of its type, runs one OneStep per track and writes
+// the survivor and its secondaries to the next stores through warp-aggregated
+// slot reservations (prefix sums over the warp, one atomic per warp and type),
+// so the stores stay compact and particle-pure without a separate compaction
+// pass.  Tracks that do not fit go to the stack and are re-injected when the
+// stores drain; primaries are injected on the device, with per-primary
+// MRG32k3a substreams by skip-ahead, whenever fewer than `refill_below`
+// tracks are in flight.  The per-iteration launch sequence (refill, three
+// step kernels, finish) is captured once in a CUDA graph and replayed.
+//
+// The "plain" engine runs the same step code as one kernel over one mixed
+// store, launched and synchronised from the host every iteration, in FP64: the
+// straightforward GPU loop the batched engine is measured against.
+#include "gx_internal.cuh"
+
+#include <algorithm>
+#include <type_traits>
+#include <cmath>
+#include <cstring>
+
+namespace gx {
+
+// ------------------------------------------------------------------ layout
+template <class R> struct Store {
+  double *x, *y, *z;
+  R *dx, *dy, *dz, *E, *n0, *n1, *n2;
+  uint32_t *rng; // 6 planes of cap words
+  int *vol, *event, *prim, *type;
+  long long cap;
+};
+
+struct Geom {
+  int geometry, axis, nlayers, box_mat, charged_local, nvol, nevents;
+  double t_abs, pitch, x0, total, half_trans, Bz;
+  double box_half[3], box_centre[3];
+};
+
+constexpr int kNStat = 16;
+enum { S_STEPS, S_SUBSTEPS, S_TRACKS, S_SEC0, S_SEC1, S_SEC2, S_PAIR, S_ANNIH, S_ERR, S_OVERFLOW,
+       S_READ0, S_READ1, S_READ2, S_WRITE0, S_WRITE1, S_WRITE2 };
+
+struct Ctl {
+  int parity;
+  int err_flags;
+  long long count[2][3];
+  long long stack_count[3];
+  long long prim_next, nprim;
+  long long take_stack[3], take_prim; // refill plan
+  long long stack_dst[3], stack_src[3];
+  long long in_flight, pending, peak, iterations;
+  unsigned long long stat[kNStat];
+  double escaped;
+};
+
+struct Prims {
+  const int *type, *event;
+  const double *E, *pos, *dir;
+  double seed[6];
+  long long first_substream;
+  const uint64_t *jump;
+};
+
+template <class R> struct Args {
+  const Data *d;
+  Ctl *ctl;
+  Store<R> st[2][3];
+  Store<R> stack[3];
+  Geom g;
+  Prims p;
+  double *edep;
+  int *pstep;
+  int nstores;
+  long long refill_below;
+};
+
+// ---------------------------------------------------------------- geometry
+// The layered calorimeter along axis a: layer k occupies [x0 + k pitch,
+// x0 + (k+1) pitch), absorber first.  vol = 2 layer + slab; -1 outside.
+__device__ __forceinline__ int vol_material(const Geom &g, int vol)
+{
+  return g.geometry == 0 ? g.box_mat : ((vol & 1) ? 2 : 1);
+}
+__device__ __forceinline__ void slab_bounds(const Geom &g, int vol, double &lo, double &hi)
+{
+  if (g.geometry == 0) {
+    lo = g.box_centre[g.axis] - g.box_half[g.axis];
+    hi = g.box_centre[g.axis] + g.box_half[g.axis];
+    return;
+  }
+  double base = g.x0 + (vol >> 1) * g.pitch;
+  lo = (vol & 1) ? base + g.t_abs : base;
+  hi = (vol & 1) ? base + g.pitch : base + g.t_abs;
+}
+__device__ __forceinline__ double thalf(const Geom &g, int b) { return g.geometry == 0 ? g.box_half[b] : g.half_trans; }
+__device__ __forceinline__ double tcentre(const Geom &g, int b) { return g.geometry == 0 ? g.box_centre[b] : 0.0; }
+
+__device__ int locate(const Geom &g, const double *p, const double *d)
+{
+  const double tol = 1e-12;
+  int a = g.axis;
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    double h = thalf(g, b), q = p[b] - tcentre(g, b);
+    if (q > h || q < -h) return -1;
+    if ((q > h - tol && d[b] > 0) || (q < -h + tol && d[b] < 0)) return -1;
+  }
+  if (g.geometry == 0) {
+    double q = p[a] - g.box_centre[a], h = g.box_half[a];
+    if (q > h || q < -h) return -1;
+    if ((q > h - tol && d[a] > 0) || (q < -h + tol && d[a] < 0)) return -1;
+    return 0;
+  }
+  double u = p[a] - g.x0;
+  if (u < -tol || u > g.total + tol) return -1;
+  if ((u < tol && d[a] < 0) || (u > g.total - tol && d[a] > 0)) return -1;
+  int layer = (int)floor(u / g.pitch);
+  layer = min(max(layer, 0), g.nlayers - 1);
+  double q = u - layer * g.pitch;
+  if (q < tol && d[a] < 0 && layer > 0) return 2 * (layer - 1) + 1;
+  if (q > g.pitch - tol && d[a] > 0 && layer + 1 < g.nlayers) return 2 * (layer + 1);
+  if (fabs(q - g.t_abs) < tol) return 2 * layer + (d[a] > 0 ? 1 : 0);
+  return 2 * layer + (q < g.t_abs ? 0 : 1);
+}
+
+__device__ __forceinline__ double dist_to_out(const Geom &g, int vol, const double *p, const double *d, int &plane)
+{
+  int a = g.axis;
+  double lo, hi, dist = 1.7976931348623157e308;
+  slab_bounds(g, vol, lo, hi);
+  plane = 0;
+  if (d[a] > 0) {
+    dist = (hi - p[a]) / d[a];
+    plane = 1;
+  } else if (d[a] < 0) {
+    dist = (lo - p[a]) / d[a];
+    plane = -1;
+  }
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    double h = thalf(g, b), q = p[b] - tcentre(g, b), t = 1.7976931348623157e308;
+    if (d[b] > 0)
+      t = (h - q) / d[b];
+    else if (d[b] < 0)
+      t = (-h - q) / d[b];
+    if (t < dist) {
+      dist = t;
+      plane = 2;
+    }
+  }
+  return dist < 0 ? 0 : dist;
+}
+
+__device__ __forceinline__ double safety(const Geom &g, int vol, const double *p)
+{
+  int a = g.axis;
+  double lo, hi;
+  slab_bounds(g, vol, lo, hi);
+  double s = fmin(p[a] - lo, hi - p[a]);
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    s = fmin(s, thalf(g, b) - fabs(p[b] - tcentre(g, b)));
+  }
+  return s < 0 ? 0 : s;
+}
+
+__device__ __forceinline__ int next_volume(const Geom &g, int vol, int plane)
+{
+  if (plane == 2 || g.geometry == 0) return -1;
+  int nv = vol + (plane > 0 ? 1 : -1);
+  return (nv < 0 || nv >= 2 * g.nlayers) ? -1 : nv;
+}
+
+// ---------------------------------------------------------- cross sections
+template <class R> __device__ __forceinline__ R lambda_tab(const Data &d, int t, int mat, R e)
+{
+  const VecDesc &v = d.vec[t][mat];
+  if ((double)e <= v.emin) return R(0);
+  return vec_value_fast<R>(d, v, e);
+}
+
+// Macroscopic cross sections (1/mm): gamma {Compton, conversion, photo-electric},
+// e- {ionisation, brems}, e+ {ionisation, brems, annihilation}.
+template <class R> __device__ __forceinline__ void cross_sections(const Data &d, int type, int mat, R e, R xs[3])
+{
+  xs[0] = xs[1] = xs[2] = R(0);
+  if (type == 0) {
+    xs[0] = (e < R(1)) ? vec_value_fast<R>(d, d.vec[GX_Lambda_compt][mat], e)
+                       : vec_value_fast<R>(d, d.vec[GX_LambdaPrim_compt][mat], e) / e;
+    xs[1] = lambda_tab<R>(d, GX_Lambda_conv, mat, e);
+    xs[2] = (e >= R(0.2)) ? vec_value_fast<R>(d, d.vec[GX_LambdaPrim_phot][mat], e) / e
+                          : (R)pe_xs_sandia(d, (int)d.mat_Z[mat], d.mat_density[mat], (double)e);
+  } else if (type == 1) {
+    xs[0] = lambda_tab<R>(d, GX_Lambda_eIoni_em, mat, e);
+    xs[1] = lambda_tab<R>(d, GX_Lambda_eBrem_em, mat, e);
+  } else {
+    xs[0] = lambda_tab<R>(d, GX_Lambda_eIoni_ep, mat, e);
+    xs[1] = lambda_tab<R>(d, GX_Lambda_eBrem_ep, mat, e);
+    xs[2] = (R)(d.mat_nel[mat] * annih_xs_per_electron(d.pi_rcl2, (double)e));
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (!(xs[i] > R(0))) xs[i] = R(0);
+}
+
+// ProxyIonization::AlongStepGPIL in physics mode (Geant4 step function, length cut)
+template <class R> __device__ __forceinline__ R range_limit(const Data &d, int type, int mat, R e)
+{
+  const R dR = R(0.2), finalRange = R(10.0);
+  R range = vec_value_fast<R>(d, d.vec[type == 2 ? GX_Range_ep : GX_Range_em][mat], e);
+  if (e < R(kMinE)) range *= e / R(kMinE);
+  R cut = (R)d.cut_length[1][mat];
+  R finR = (finalRange < cut) ? finalRange : cut;
+  if (range <= finR) return range;
+  return range * dR + finR * (R(1) - dR) * (R(2) - finR / range);
+}
+
+// ProxyIonization::AlongStepDoIt in physics mode; the inverse range (used when
+// the loss exceeds 1%, i.e. near the end of the range) is evaluated in FP64.
+template <class R> __device__ __forceinline__ R along_loss(const Data &d, int type, int mat, double step, R &e)
+{
+  bool ep = type == 2;
+  R energy = e;
+  R range = vec_value_fast<R>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], energy);
+  if (step >= (double)range || energy <= R(kMinE)) {
+    e = R(0);
+    return energy;
+  }
+  R dedx = vec_value_fast<R>(d, d.vec[ep ? GX_DEDX_eIoni_ep : GX_DEDX_eIoni_em][mat], energy);
+  if (energy < R(kMinE)) dedx *= M<R>::sqrt(energy / R(kMinE));
+  R eloss = (R)step * dedx;
+  if (eloss > energy * R(0.01)) {
+    double r64 = vec_value_fast<double>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], (double)energy) - step;
+    eloss = (R)((double)energy - vec_invrange_ref(d, d.vec[ep ? GX_InverseRange_ep : GX_InverseRange_em][mat], r64));
+  }
+  R finalE = energy - eloss;
+  if (finalE < R(kMinE)) {
+    eloss += finalE;
+    finalE = R(0);
+  }
+  e = finalE;
+  return eloss > R(0) ? eloss : R(0);
+}
+
+// ---------------------------------------------------------------- one step
+template <class R> struct Track {
+  int type, vol, event, prim;
+  double pos[3];
+  R dir[3], E, nil[3];
+  Mrg rng;
+};
+
+struct Local {
+  // deposits go to a shared-memory tally when it fits, else to global memory
+  double *sm_edep;
+  double *g_edep;
+  int nvol, nevents, sm_bins;
+  double escaped;
+  unsigned int st[kNStat];
+  int err;
+  __device__ __forceinline__ void deposit(int event, int vol, double e)
+  {
+    if (vol < 0 || vol >= nvol || e == 0.0) return;
+    if (event < 0 || event >= nevents) { // a primary with an event index outside the tally
+      err |= kErrOverflow;
+      return;
+    }
+    int bin = event * nvol + vol;
+    if (bin < sm_bins)
+      atomicAdd(&sm_edep[bin], e);
+    else
+      atomicAdd(&g_edep[bin], e);
+  }
+};
+
+template <class R> struct Secs {
+  int n;
+  int type[2];
+  R E[2], dir[2][3];
+};
+
+// Helix sub-steps in Bz (FieldPropagationHandler::Propagate / PropagateInVolume,
+// magneticfield/src/FieldPropagationHandler.cpp:87-360), FP64.
+template <class R>
+__device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool &crossed, int &newvol, Local &L)
+{
+  const double eps = 0.1; // gEpsDeflection = 1e-2 cm
+  double charge = (t.type == 1) ? -1.0 : 1.0;
+  double E = (double)t.E;
+  double p = ::sqrt(E * (E + 2.0 * kEMass));
+  double pos[3] = {t.pos[0], t.pos[1], t.pos[2]};
+  double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+  double remaining = pstep, total = 0.0;
+  const double B[3] = {0.0, 0.0, g.Bz};
+  crossed = false;
+  newvol = t.vol;
+  for (int it = 0; it < 10000; ++it) {
+    int plane;
+    double saf = safety(g, t.vol, pos);
+    double snext = (saf > remaining) ? remaining
+                                     : fmax(2e-9, fmin(dist_to_out(g, t.vol, pos, dir, plane), remaining) + 2e-9);
+    double step_gp = fmax(fmin(remaining, 1e-4), snext);
+    double pt = p * ::sqrt(fmax(1.0 - dir[2] * dir[2], 0.0));
+    double step_field = 1.7976931348623157e308;
+    if (pt > 0.0) step_field = fmax(2.0 * ::sqrt(eps / (0.299792458 * fabs(g.Bz) / pt)), saf);
+    double s = fmin(fmin(step_gp, step_field), remaining);
+    double np[3], nd[3];
+    if (pt > 0.0) {
+      helix_dostep(kB2C_mm, B, pos, dir, charge, p, s, np, nd);
+      double m = ::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+      nd[0] /= m;
+      nd[1] /= m;
+      nd[2] /= m;
+    } else {
+      for (int k = 0; k < 3; ++k) {
+        np[k] = pos[k] + s * dir[k];
+        nd[k] = dir[k];
+      }
+    }
+    for (int k = 0; k < 3; ++k) {
+      pos[k] = np[k];
+      dir[k] = nd[k];
+    }
+    total += s;
+    remaining -= s;
+    L.st[S_SUBSTEPS]++;
+    int v = locate(g, pos, dir);
+    if (v != t.vol || remaining <= 1e-10) {
+      if (v != t.vol) {
+        crossed = true;
+        newvol = v;
+      }
+      for (int k = 0; k < 3; ++k) {
+        t.pos[k] = pos[k];
+        t.dir[k] = (R)dir[k];
+      }
+      return total;
+    }
+  }
+  L.err |= kErrFieldCap;
+  L.st[S_ERR]++;
+  crossed = true;
+  newvol = -2;
+  for (int k = 0; k < 3; ++k) {
+    t.pos[k] = pos[k];
+    t.dir[k] = (R)dir[k];
+  }
+  return total;
+}
+
+template <class R>
+__device__ void run_model(const Data &d, const Geom &g, Track<R> &t, int proc, Secs<R> &sec, Local &L)
+{
+  int mat = vol_material(g, t.vol);
+  ModelParams mp;
+  mp.mode = 1;
+  mp.Z = (int)d.mat_Z[mat];
+  mp.cut = 0.0;
+  mp.density_factor = d.mat_dfactor[mat];
+  mp.sb = d.sb + ((mat == 1) ? 2 : 1);
+  Inter<R> io;
+  io.E = t.E;
+  io.dir[0] = t.dir[0];
+  io.dir[1] = t.dir[1];
+  io.dir[2] = t.dir[2];
+  io.edep = R(0);
+  io.status = 0;
+  io.nsec = 0;
+  int err = 0;
+  if (t.type == 0) {
+    if (proc == 0)
+      kn_sample(t.rng, mp, io, &err);
+    else if (proc == 1) {
+      bh_sample(t.rng, mp, io, &err);
+      if (io.nsec == 2) L.st[S_PAIR]++;
+    } else
+      sg_sample(t.rng, d, mp, io, &err);
+  } else if (proc == 0) {
+    mp.cut = d.cut_energy[1][mat];
+    if (t.type == 1)
+      mb_sample(t.rng, mp, io, &err);
+    else
+      bhabha_sample(t.rng, mp, io, &err);
+  } else if (proc == 1) {
+    mp.cut = d.cut_energy[0][mat];
+    sb_sample(t.rng, mp, io, &err);
+  } else {
+    annih_sample(t.rng, io, &err);
+    L.st[S_ANNIH]++;
+  }
+  if (err) {
+    L.err |= err;
+    L.st[S_ERR]++;
+  }
+  L.deposit(t.event, t.vol, (double)io.edep);
+  t.E = io.E;
+  t.dir[0] = io.dir[0];
+  t.dir[1] = io.dir[1];
+  t.dir[2] = io.dir[2];
+  for (int s = 0; s < io.nsec; ++s) {
+    if (g.charged_local && io.sec_type[s] != 0) {
+      L.deposit(t.event, t.vol, (double)io.sec_E[s]);
+      continue;
+    }
+    int k = sec.n++;
+    sec.type[k] = io.sec_type[s];
+    sec.E[k] = io.sec_E[s];
+    sec.dir[k][0] = io.sec_dir[s][0];
+    sec.dir[k][1] = io.sec_dir[s][1];
+    sec.dir[k][2] = io.sec_dir[s][2];
+  }
+  if (io.status == 1) t.E = R(0);
+}
+
+// One OneStep (test_BasicCpuTransport.cpp:408-497 / InnerStep :358-403) in
+// physics mode; the oracle's one_step is the same algorithm in the same
+// order of random draws.  Returns false when the track is finished.
+template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
+{
+  sec.n = 0;
+  int mat = vol_material(g, t.vol);
+  int np = (t.type == 1) ? 2 : 3;
+  bool charged = t.type != 0;
+  R xs[3];
+  cross_sections<R>(d, t.type, mat, t.E, xs);
+  for (int i = 0; i < np; ++i)
+    if (t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(t.rng.template u<R>());
+  R pstep = R(3.0e38);
+  int sel = -1;
+  for (int i = 0; i < np; ++i)
+    if (xs[i] > R(0)) {
+      R s = t.nil[i] / xs[i];
+      if (s < pstep) {
+        pstep = s;
+        sel = i;
+      }
+    }
+  if (charged) {
+    R slim = range_limit<R>(d, t.type, mat, t.E);
+    if (slim < pstep) {
+      pstep = slim;
+      sel = -1;
+    }
+  }
+  int vol0 = t.vol, newvol = t.vol;
+  bool crossed = false;
+  double step;
+  if (!charged || g.Bz == 0.0) {
+    int plane;
+    double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+    double dd = dist_to_out(g, t.vol, t.pos, dir, plane);
+    double ps = (double)pstep;
+    if (dd < ps) {
+      step = dd;
+      crossed = true;
+      newvol = next_volume(g, t.vol, plane);
+      for (int k = 0; k < 3; ++k) t.pos[k] += step * dir[k];
+      if (plane != 2) {
+        double lo, hi;
+        slab_bounds(g, t.vol, lo, hi);
+        t.pos[g.axis] = plane > 0 ? hi : lo;
+      }
+    } else {
+      step = ps;
+      for (int k = 0; k < 3; ++k) t.pos[k] += step * dir[k];
+    }
+  } else {
+    step = field_propagate(g, t, (double)pstep, crossed, newvol, L);
+  }
+  for (int i = 0; i < np; ++i) t.nil[i] -= (R)step * xs[i];
+  L.st[S_STEPS]++;
+  if (newvol == -2) {
+    L.deposit(t.event, vol0, (double)t.E);
+    return false;
+  }
+  if (charged) {
+    R eloss = along_loss<R>(d, t.type, mat, step, t.E);
+    L.deposit(t.event, vol0, (double)eloss);
+    if (t.E <= R(0)) {
+      if (t.type == 2) {
+        int v = crossed ? newvol : vol0;
+        if (v >= 0) {
+          t.vol = v;
+          run_model(d, g, t, 2, sec, L);
+        } else {
+          L.escaped += 2.0 * kEMass;
+        }
+      }
+      return false;
+    }
+  }
+  if (crossed) {
+    t.vol = newvol;
+    if (newvol < 0) {
+      L.escaped += (double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0);
+      return false;
+    }
+    return true;
+  }
+  if (sel >= 0) {
+    t.nil[sel] = R(-1);
+    run_model(d, g, t, sel, sec, L);
+    if (t.E <= R(0)) return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------- load / store
+template <class R> __device__ __forceinline__ void load_track(const Store<R> &s, long long i, int ptype, Track<R> &t)
+{
+  t.type = (ptype < 3) ? ptype : s.type[i];
+  t.pos[0] = s.x[i];
+  t.pos[1] = s.y[i];
+  t.pos[2] = s.z[i];
+  t.dir[0] = s.dx[i];
+  t.dir[1] = s.dy[i];
+  t.dir[2] = s.dz[i];
+  t.E = s.E[i];
+  t.nil[0] = s.n0[i];
+  t.nil[1] = s.n1[i];
+  t.nil[2] = s.n2[i];
+  t.rng.load(s.rng, s.cap, i);
+  t.vol = s.vol[i];
+  t.event = s.event[i];
+  t.prim = s.prim[i];
+}
+
+template <class R> __device__ __forceinline__ void store_track(const Store<R> &s, long long i, const Track<R> &t)
+{
+  s.x[i] = t.pos[0];
+  s.y[i] = t.pos[1];
+  s.z[i] = t.pos[2];
+  s.dx[i] = t.dir[0];
+  s.dy[i] = t.dir[1];
+  s.dz[i] = t.dir[2];
+  s.E[i] = t.E;
+  s.n0[i] = t.nil[0];
+  s.n1[i] = t.nil[1];
+  s.n2[i] = t.nil[2];
+  t.rng.store(s.rng, s.cap, i);
+  s.vol[i] = t.vol;
+  s.event[i] = t.event;
+  s.prim[i] = t.prim;
+  if (s.type) s.type[i] = t.type;
+}
+
+__device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
+
+// Reserve `cnt` consecutive slots per lane in counter *ctr: one atomic per
+// warp, returns this lane's first slot.
+__device__ __forceinline__ long long warp_reserve(unsigned long long *ctr, int cnt)
+{
+  unsigned lane = lane_id();
+  int incl = cnt;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    int v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= (unsigned)off) incl += v;
+  }
+  int total = __shfl_sync(0xffffffffu, incl, 31);
+  unsigned long long base = 0;
+  if (lane == 31 && total > 0) base = atomicAdd(ctr, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  return (long long)base + incl - cnt;
+}
+
+// Write a track to store q, or to q's overflow stack when the store is full.
+template <class R> __device__ __forceinline__ void put_track(const Args<R> &a, int q, long long idx, const Track<R> &t, Local &L)
+{
+  const Store<R> &s = a.st[a.ctl->parity ^ 1][q];
+  if (idx < s.cap) {
+    store_track(s, idx, t);
+    return;
+  }
+  unsigned long long j = atomicAdd((unsigned long long *)&a.ctl->stack_count[q], 1ULL);
+  if ((long long)j < a.stack[q].cap) {
+    store_track(a.stack[q], (long long)j, t);
+  } else {
+    // no room anywhere: the track is retired and its energy scored where it is
+    L.err |= kErrOverflow;
+    L.st[S_OVERFLOW]++;
+    L.deposit(t.event, t.vol, (double)t.E);
+  }
+}
+
+// ----------------------------------------------------------------- kernels
+// PT: particle type of the store (0, 1, 2), or 3 for the single mixed store.
+template <class R, int PT> __global__ void __launch_bounds__(256) k_step(Args<R> a)
+{
+  extern __shared__ double sm_edep[];
+  __shared__ unsigned long long sm_stat[kNStat];
+  __shared__ double sm_esc;
+  __shared__ int sm_err;
+  const Data &d = *a.d;
+  Ctl *ctl = a.ctl;
+  const int par = ctl->parity;
+  const int store_id = (PT < 3) ? PT : 0;
+  const long long n = min(ctl->count[par][store_id], a.st[par][store_id].cap);
+  Local L;
+  L.nvol = a.g.nvol;
+  L.nevents = a.g.nevents;
+  L.g_edep = a.edep;
+  L.sm_edep = sm_edep;
+  L.sm_bins = 0;
+  {
+    int bins = 0;
+    // shared-memory tally if the whole table fits in 6 KB
+    long long all = (long long)a.g.nvol * 1; // event rows other than 0 go to global memory
+    if (all <= 768) bins = (int)all;
+    L.sm_bins = bins;
+    for (int k = threadIdx.x; k < bins; k += blockDim.x) sm_edep[k] = 0.0;
+  }
+  if (threadIdx.x < kNStat) sm_stat[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    sm_esc = 0.0;
+    sm_err = 0;
+  }
+  __syncthreads();
+  L.escaped = 0.0;
+  L.err = 0;
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
+
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    long long i = base + threadIdx.x;
+    bool active = i < n;
+    Track<R> t;
+    Secs<R> sec;
+    sec.n = 0;
+    bool alive = false;
+    if (active) {
+      load_track(a.st[par][store_id], i, PT, t);
+      L.st[S_READ0 + store_id]++;
+      alive = one_step(d, a.g, t, sec, L);
+      if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
+    }
+    // slots per destination store
+    int cnt[3] = {0, 0, 0};
+    int dst_surv = (a.nstores == 1) ? 0 : (active ? t.type : 0);
+    if (alive) cnt[dst_surv]++;
+    for (int k = 0; k < sec.n; ++k) cnt[(a.nstores == 1) ? 0 : sec.type[k]]++;
+    long long first[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      if (q < a.nstores)
+        first[q] = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]);
+      else
+        first[q] = 0;
+    }
+    if (active) {
+      long long next[3] = {first[0], first[1], first[2]};
+      // secondaries first take their streams from the parent, in order
+      for (int k = 0; k < sec.n; ++k) {
+        Track<R> c;
+        c.type = sec.type[k];
+        c.pos[0] = t.pos[0];
+        c.pos[1] = t.pos[1];
+        c.pos[2] = t.pos[2];
+        c.dir[0] = sec.dir[k][0];
+        c.dir[1] = sec.dir[k][1];
+        c.dir[2] = sec.dir[k][2];
+        c.E = sec.E[k];
+        c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
+        t.rng.seed_child(c.rng);
+        c.vol = t.vol;
+        c.event = t.event;
+        c.prim = -1;
+        int q = (a.nstores == 1) ? 0 : c.type;
+        put_track(a, q, next[q]++, c, L);
+        L.st[S_SEC0 + c.type]++;
+        L.st[S_WRITE0 + store_id]++;
+      }
+      if (alive) {
+        put_track(a, dst_surv, next[dst_surv]++, t, L);
+        L.st[S_WRITE0 + store_id]++;
+      }
+    }
+  }
+  // flush block-local tallies
+  L.st[S_TRACKS] = 0;
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k)
+    if (L.st[k]) atomicAdd(&sm_stat[k], (unsigned long long)L.st[k]);
+  if (L.escaped != 0.0) atomicAdd(&sm_esc, L.escaped);
+  if (L.err) atomicOr(&sm_err, L.err);
+  __syncthreads();
+  for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x)
+    if (sm_edep[k] != 0.0) atomicAdd(&a.edep[k], sm_edep[k]);
+  if (threadIdx.x < kNStat && sm_stat[threadIdx.x]) atomicAdd(&ctl->stat[threadIdx.x], sm_stat[threadIdx.x]);
+  if (threadIdx.x == 0) {
+    if (sm_esc != 0.0) atomicAdd(&ctl->escaped, sm_esc);
+    if (sm_err) atomicOr(&ctl->err_flags, sm_err);
+  }
+}
+
+// End of an iteration: the next stores become current, the refill plan for
+// the following iteration is made.  One thread.
+__global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores, long long refill_below,
+                         long long stack_cap)
+{
+  int par = ctl->parity, np = par ^ 1;
+  const long long cap[3] = {cap0, cap1, cap2};
+  long long fl = 0;
+  for (int q = 0; q < nstores; ++q) {
+    // pushes past the end of a full stack were not written (and were counted as errors)
+    ctl->stack_count[q] = min(ctl->stack_count[q], stack_cap);
+    ctl->count[np][q] = min(ctl->count[np][q], cap[q]);
+    ctl->count[par][q] = 0;
+    fl += ctl->count[np][q];
+  }
+  ctl->parity = np;
+  ctl->iterations++;
+  // refill plan: deferred tracks first (most recent first), then primaries
+  long long budget = refill_below - fl;
+  long long pend = ctl->nprim - ctl->prim_next;
+  for (int q = 0; q < nstores; ++q) {
+    long long room = cap[q] - ctl->count[np][q];
+    long long take = 0;
+    if (budget > 0) take = min(min(ctl->stack_count[q], room), budget);
+    // reserve the slots now: deferred tracks land at the end of the store,
+    // primaries are appended after them by the refill kernel
+    ctl->take_stack[q] = take;
+    ctl->stack_dst[q] = ctl->count[np][q];
+    ctl->count[np][q] += take;
+    ctl->stack_count[q] -= take;
+    ctl->stack_src[q] = ctl->stack_count[q];
+    budget -= take;
+    pend += ctl->stack_count[q];
+  }
+  long long tp = 0;
+  if (budget > 0) tp = min(budget, ctl->nprim - ctl->prim_next);
+  ctl->take_prim = tp;
+  ctl->in_flight = fl;
+  ctl->pending = pend;
+  if (fl > ctl->peak) ctl->peak = fl;
+}
+
+__device__ __forceinline__ void jump_matvec(const uint64_t *A, uint64_t v[3], uint64_t m)
+{
+  uint64_t r[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    uint64_t acc = 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) acc = ((A[3 * i + k] * v[k]) % m + acc) % m;
+    r[i] = acc;
+  }
+  v[0] = r[0];
+  v[1] = r[1];
+  v[2] = r[2];
+}
+
+// Execute the refill plan: move deferred tracks back from the stacks, then
+// inject primaries (MRG32k3a substream first_substream + primary index).
+template <class R> __global__ void k_refill(Args<R> a)
+{
+  Ctl *ctl = a.ctl;
+  int par = ctl->parity;
+  long long ts[3] = {ctl->take_stack[0], ctl->take_stack[1], ctl->take_stack[2]};
+  long long tp = ctl->take_prim;
+  long long total = ts[0] + ts[1] + ts[2] + tp;
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+    long long j = i;
+    int q = 0;
+    while (q < 3 && j >= ts[q]) {
+      j -= ts[q];
+      ++q;
+    }
+    if (q < 3) {
+      Track<R> t;
+      load_track(a.stack[q], ctl->stack_src[q] + j, (a.nstores == 1) ? 3 : q, t);
+      store_track(a.st[par][q], ctl->stack_dst[q] + j, t);
+      continue;
+    }
+    long long pi = ctl->prim_next + j;
+    Track<R> t;
+    t.type = a.p.type[pi];
+    t.E = (R)a.p.E[pi];
+    for (int k = 0; k < 3; ++k) {
+      t.pos[k] = a.p.pos[3 * pi + k];
+      t.dir[k] = (R)a.p.dir[3 * pi + k];
+    }
+    double dd[3] = {a.p.dir[3 * pi], a.p.dir[3 * pi + 1], a.p.dir[3 * pi + 2]};
+    t.vol = locate(a.g, t.pos, dd);
+    t.nil[0] = t.nil[1] = t.nil[2] = R(-1);
+    t.event = a.p.event ? a.p.event[pi] : 0;
+    t.prim = (int)pi;
+    unsigned long long kk = (unsigned long long)(a.p.first_substream + pi);
+    uint64_t v1[3] = {(uint64_t)a.p.seed[0], (uint64_t)a.p.seed[1], (uint64_t)a.p.seed[2]};
+    uint64_t v2[3] = {(uint64_t)a.p.seed[3], (uint64_t)a.p.seed[4], (uint64_t)a.p.seed[5]};
+    for (int b = 0; kk != 0 && b < 64; ++b, kk >>= 1)
+      if (kk & 1ULL) {
+        jump_matvec(a.p.jump + 9 * b, v1, 4294967087ULL);
+        jump_matvec(a.p.jump + 9 * (64 + b), v2, 4294944443ULL);
+      }
+    for (int k = 0; k < 3; ++k) {
+      t.rng.s[k] = (double)v1[k];
+      t.rng.s[3 + k] = (double)v2[k];
+    }
+    atomicAdd(&ctl->stat[S_TRACKS], 1ULL);
+    if (t.vol < 0) {
+      atomicAdd(&ctl->escaped, (double)t.E);
+      continue;
+    }
+    int qs = (a.nstores == 1) ? 0 : t.type;
+    unsigned long long slot = atomicAdd((unsigned long long *)&ctl->count[par][qs], 1ULL);
+    if ((long long)slot < a.st[par][qs].cap) {
+      store_track(a.st[par][qs], (long long)slot, t);
+    } else {
+      atomicOr(&ctl->err_flags, (int)kErrOverflow);
+      atomicAdd(&ctl->stat[S_OVERFLOW], 1ULL);
+    }
+  }
+}
+
+// Bookkeeping after a refill: the primary cursor.  One thread.
+__global__ void k_refill_done(Ctl *ctl)
+{
+  for (int q = 0; q < 3; ++q) ctl->take_stack[q] = 0;
+  ctl->prim_next += ctl->take_prim;
+  ctl->take_prim = 0;
+}
+
+__global__ void k_count_new_tracks(Ctl *ctl)
+{
+  // every secondary becomes a track exactly once
+  ctl->stat[S_TRACKS] += ctl->stat[S_SEC0] + ctl->stat[S_SEC1] + ctl->stat[S_SEC2];
+}
+
+// ------------------------------------------------------------------ engine
+struct Engine {
+  int precision = -1, engine = -1;
+  long long cap = 0, stack_cap = 0;
+  void *pool = nullptr;
+  size_t pool_bytes = 0;
+  Ctl *ctl = nullptr;
+  Ctl *h_ctl = nullptr; // pinned mirror
+  cudaGraphExec_t graph = nullptr;
+  int graph_iters = 0;
+  std::vector<char> graph_args; // launch arguments the graph was captured with
+  cudaStream_t s1 = nullptr, s2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_j1 = nullptr, ev_j2 = nullptr;
+};
+
+// Lay the SoA planes of one store out from `base + off` (256-byte aligned);
+// with base == 0 it only measures.
+template <class R> static Store<R> carve(uintptr_t base, size_t &off, long long cap, bool with_type)
+{
+  Store<R> s;
+  auto take = [&](size_t bytes) {
+    uintptr_t q = base + off;
+    off += (bytes + 255) & ~size_t(255);
+    return q;
+  };
+  s.cap = cap;
+  s.x = (double *)take(cap * sizeof(double));
+  s.y = (double *)take(cap * sizeof(double));
+  s.z = (double *)take(cap * sizeof(double));
+  s.dx = (R *)take(cap * sizeof(R));
+  s.dy = (R *)take(cap * sizeof(R));
+  s.dz = (R *)take(cap * sizeof(R));
+  s.E = (R *)take(cap * sizeof(R));
+  s.n0 = (R *)take(cap * sizeof(R));
+  s.n1 = (R *)take(cap * sizeof(R));
+  s.n2 = (R *)take(cap * sizeof(R));
+  s.rng = (uint32_t *)take(6 * cap * sizeof(uint32_t));
+  s.vol = (int *)take(cap * sizeof(int));
+  s.event = (int *)take(cap * sizeof(int));
+  s.prim = (int *)take(cap * sizeof(int));
+  s.type = with_type ? (int *)take(cap * sizeof(int)) : nullptr;
+  return s;
+}
+
+void release_engine(Ctx *c)
+{
+  Engine *e = c->engine;
+  if (!e) return;
+  if (e->graph) cudaGraphExecDestroy(e->graph);
+  if (e->pool) cudaFree(e->pool);
+  if (e->ctl) cudaFree(e->ctl);
+  if (e->h_ctl) cudaFreeHost(e->h_ctl);
+  if (e->s1) cudaStreamDestroy(e->s1);
+  if (e->s2) cudaStreamDestroy(e->s2);
+  if (e->ev_fork) cudaEventDestroy(e->ev_fork);
+  if (e->ev_j1) cudaEventDestroy(e->ev_j1);
+  if (e->ev_j2) cudaEventDestroy(e->ev_j2);
+  delete e;
+  c->engine = nullptr;
+}
+
+int launch_substreams(const double seed[6], long long first, int n, uint32_t *d_states, cudaStream_t s);
+int get_jump_table(uint64_t **out);
+
+template <class R> struct Launch {
+  Args<R> a;
+  int block, grid, smem;
+};
+
+template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent)
+{
+  k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+  k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
+  if (L.a.nstores == 1) {
+    k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+  } else if (!concurrent) {
+    k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
+    k_step<R, 1><<<L.grid, L.block, L.smem, s>>>(L.a);
+    k_step<R, 2><<<L.grid, L.block, L.smem, s>>>(L.a);
+  } else {
+    // the three particle types step concurrently: gamma on s, e- on s1, e+ on s2
+    cudaEventRecord(e->ev_fork, s);
+    cudaStreamWaitEvent(e->s1, e->ev_fork, 0);
+    cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
+    k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
+    k_step<R, 1><<<L.grid, L.block, L.smem, e->s1>>>(L.a);
+    k_step<R, 2><<<L.grid, L.block, L.smem, e->s2>>>(L.a);
+    cudaEventRecord(e->ev_j1, e->s1);
+    cudaEventRecord(e->ev_j2, e->s2);
+    cudaStreamWaitEvent(s, e->ev_j1, 0);
+    cudaStreamWaitEvent(s, e->ev_j2, 0);
+  }
+  k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
+                           L.a.refill_below, L.a.stack[0].cap);
+}
+
+template <class R>
+static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
+               const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
+               int *d_pstep, gx_transport_stats *stats, cudaStream_t s)
+{
+  const int prec = std::is_same<R, float>::value ? 1 : 0;
+  const bool batched = cfg->engine == 1;
+  const int nstores = batched ? 3 : 1;
+  long long cap = cfg->capacity > 0 ? cfg->capacity : (batched ? (1LL << 22) : (3LL << 22));
+  long long stack_cap = std::max(2 * cap, 1LL << 20);
+  Engine *&E = C->engine;
+  if (E && (E->precision != prec || E->engine != cfg->engine || E->cap != cap)) release_engine(C);
+  cudaError_t err;
+  if (!E) {
+    E = new Engine();
+    E->precision = prec;
+    E->engine = cfg->engine;
+    E->cap = cap;
+    E->stack_cap = stack_cap;
+    size_t bytes = 0;
+    for (int b = 0; b < 2; ++b)
+      for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, cap, !batched);
+    for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, stack_cap, !batched);
+    err = cudaMalloc(&E->pool, bytes);
+    if (err != cudaSuccess) {
+      release_engine(C);
+      return cuda_error(err, "transport track stores");
+    }
+    E->pool_bytes = bytes;
+    if ((err = cudaMalloc((void **)&E->ctl, sizeof(Ctl))) != cudaSuccess ||
+        (err = cudaMallocHost((void **)&E->h_ctl, sizeof(Ctl))) != cudaSuccess) {
+      release_engine(C);
+      return cuda_error(err, "transport control block");
+    }
+    cudaStreamCreateWithFlags(&E->s1, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&E->s2, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&E->ev_fork, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&E->ev_j1, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&E->ev_j2, cudaEventDisableTiming);
+  }
+  Launch<R> L;
+  std::memset(&L.a, 0, sizeof(L.a));
+  size_t off = 0;
+  uintptr_t base = (uintptr_t)E->pool;
+  for (int b = 0; b < 2; ++b)
+    for (int q = 0; q < nstores; ++q) L.a.st[b][q] = carve<R>(base, off, cap, !batched);
+  for (int q = 0; q < nstores; ++q) L.a.stack[q] = carve<R>(base, off, stack_cap, !batched);
+  for (int q = nstores; q < 3; ++q) {
+    L.a.st[0][q] = L.a.st[0][0];
+    L.a.st[1][q] = L.a.st[1][0];
+    L.a.stack[q] = L.a.stack[0];
+  }
+  if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
+  L.a.d = C->dev;
+  L.a.ctl = E->ctl;
+  Geom &g = L.a.g;
+  g.geometry = cfg->geometry;
+  g.axis = cfg->axis;
+  g.nlayers = cfg->nlayers;
+  g.box_mat = cfg->box_mat;
+  g.charged_local = cfg->charged_local;
+  g.nvol = nvol;
+  g.nevents = cfg->nevents;
+  g.t_abs = cfg->t_abs;
+  g.pitch = cfg->t_abs + cfg->t_gap;
+  g.x0 = -0.5 * cfg->nlayers * g.pitch;
+  g.total = cfg->nlayers * g.pitch;
+  g.half_trans = cfg->half_trans;
+  g.Bz = cfg->Bz;
+  for (int k = 0; k < 3; ++k) {
+    g.box_half[k] = cfg->box_half[k];
+    g.box_centre[k] = cfg->box_centre[k];
+  }
+  uint64_t *jt;
+  int rc = get_jump_table(&jt);
+  if (rc) return rc;
+  L.a.p.type = d_type;
+  L.a.p.event = d_event;
+  L.a.p.E = d_E;
+  L.a.p.pos = d_pos;
+  L.a.p.dir = d_dir;
+  for (int k = 0; k < 6; ++k) L.a.p.seed[k] = cfg->seed[k];
+  L.a.p.first_substream = cfg->first_substream;
+  L.a.p.jump = jt;
+  L.a.edep = d_edep;
+  L.a.pstep = d_pstep;
+  L.a.nstores = nstores;
+  L.a.refill_below = cfg->refill_below > 0 ? std::min(cfg->refill_below, cap) : cap / 2;
+  L.block = cfg->block_size > 0 ? cfg->block_size : 256;
+  int bpsm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 4;
+  L.grid = C->num_sms * bpsm;
+  L.smem = 768 * sizeof(double);
+
+  Ctl h;
+  std::memset(&h, 0, sizeof(h));
+  h.nprim = nprim;
+  h.iterations = -1; // the planning launch below is not an iteration
+  err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
+  if (err != cudaSuccess) return cuda_error(err, "transport control init");
+  // first refill plan
+  k_finish<<<1, 1, 0, s>>>(E->ctl, cap, cap, cap, nstores, L.a.refill_below, stack_cap);
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  cudaEventRecord(t0, s);
+  const long long max_iter = 2000000LL;
+  long long iters = 0;
+  double step_ms[3] = {0, 0, 0};
+  long long step_launches[3] = {0, 0, 0};
+  if (!batched || cfg->profile) {
+    // plain loop (and the profiling pass): launch, synchronise, look at the
+    // counters, every iteration
+    cudaEvent_t ea[3], eb[3];
+    for (int q = 0; q < 3; ++q) {
+      cudaEventCreate(&ea[q]);
+      cudaEventCreate(&eb[q]);
+    }
+    for (;;) {
+      if (cfg->profile) {
+        k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+        k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
+        for (int q = 0; q < nstores; ++q) {
+          cudaEventRecord(ea[q], s);
+          if (!batched)
+            k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+          else if (q == 0)
+            k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
+          else if (q == 1)
+            k_step<R, 1><<<L.grid, L.block, L.smem, s>>>(L.a);
+          else
+            k_step<R, 2><<<L.grid, L.block, L.smem, s>>>(L.a);
+          cudaEventRecord(eb[q], s);
+        }
+        k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
+                                 L.a.refill_below, L.a.stack[0].cap);
+      } else {
+        enqueue_iteration(L, E, s, false);
+      }
+      cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+      if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport iteration");
+      if (cfg->profile)
+        for (int q = 0; q < nstores; ++q) {
+          float t = 0;
+          cudaEventElapsedTime(&t, ea[q], eb[q]);
+          step_ms[q] += t;
+          step_launches[q]++;
+        }
+      ++iters;
+      if (E->h_ctl->in_flight == 0 && E->h_ctl->pending == 0) break;
+      if (iters > max_iter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
+    }
+    for (int q = 0; q < 3; ++q) {
+      cudaEventDestroy(ea[q]);
+      cudaEventDestroy(eb[q]);
+    }
+  } else {
+    int G = cfg->graph_iters > 0 ? cfg->graph_iters : 16;
+    // (re)capture the iteration graph when the launch arguments change
+    std::vector<char> key(sizeof(L.a) + 3 * sizeof(int));
+    std::memcpy(key.data(), &L.a, sizeof(L.a));
+    int extra[3] = {G, L.block, L.grid};
+    std::memcpy(key.data() + sizeof(L.a), extra, sizeof(extra));
+    if (!E->graph || E->graph_args != key) {
+      if (E->graph) {
+        cudaGraphExecDestroy(E->graph);
+        E->graph = nullptr;
+      }
+      cudaStream_t cs;
+      cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+      cudaGraph_t graph;
+      if ((err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
+        return cuda_error(err, "graph capture");
+      for (int k = 0; k < G; ++k) enqueue_iteration(L, E, cs, true);
+      cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, cs);
+      if ((err = cudaStreamEndCapture(cs, &graph)) != cudaSuccess) return cuda_error(err, "graph capture end");
+      err = cudaGraphInstantiate(&E->graph, graph, 0);
+      cudaGraphDestroy(graph);
+      cudaStreamDestroy(cs);
+      if (err != cudaSuccess) return cuda_error(err, "graph instantiate");
+      E->graph_iters = G;
+      E->graph_args = key;
+    }
+    for (;;) {
+      if ((err = cudaGraphLaunch(E->graph, s)) != cudaSuccess) return cuda_error(err, "graph launch");
+      if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport graph");
+      iters += G;
+      if (E->h_ctl->in_flight == 0 && E->h_ctl->pending == 0) break;
+      if (iters > max_iter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
+    }
+  }
+  k_count_new_tracks<<<1, 1, 0, s>>>(E->ctl);
+  cudaEventRecord(t1, s);
+  cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+  if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport end");
+  float ms = 0;
+  cudaEventElapsedTime(&ms, t0, t1);
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  const Ctl &c = *E->h_ctl;
+  if (stats) {
+    stats->steps = (long long)c.stat[S_STEPS];
+    stats->substeps = (long long)c.stat[S_SUBSTEPS];
+    stats->tracks = (long long)c.stat[S_TRACKS];
+    for (int q = 0; q < 3; ++q) stats->secondaries[q] = (long long)c.stat[S_SEC0 + q];
+    stats->n_pair = (long long)c.stat[S_PAIR];
+    stats->n_annih = (long long)c.stat[S_ANNIH];
+    stats->errors = (long long)(c.stat[S_ERR] + c.stat[S_OVERFLOW]);
+    stats->escaped = c.escaped;
+    stats->iterations = c.iterations;
+    stats->peak_in_flight = c.peak;
+    stats->kernel_ms = ms;
+    for (int q = 0; q < 3; ++q) {
+      stats->step_ms[q] = step_ms[q];
+      stats->step_launches[q] = step_launches[q];
+      stats->tracks_read[q] = (long long)c.stat[S_READ0 + q];
+      stats->tracks_written[q] = (long long)c.stat[S_WRITE0 + q];
+    }
+    stats->bytes_per_track = (long long)(3 * sizeof(double) + 7 * sizeof(R) + 6 * sizeof(uint32_t) +
+                                         3 * sizeof(int) + (batched ? 0 : sizeof(int)));
+  }
+  if (c.err_flags & kErrOverflow) return set_error(GX_ERR_OVERFLOW, "transport: track stores and stacks full");
+  if (c.err_flags) return set_error(GX_ERR_ITERCAP, "transport: an iteration cap was hit (flags %d)", c.err_flags);
+  return GX_OK;
+}
+
+} // namespace gx
+
+using namespace gx;
+
+extern "C" {
+
+void gx_transport_config_default(gx_transport_config *c)
+{
+  std::memset(c, 0, sizeof(*c));
+  c->geometry = 1;
+  c->axis = 2;
+  c->nlayers = 50;
+  c->t_abs = 2.3;
+  c->t_gap = 5.7;
+  c->half_trans = 200.0;
+  c->box_mat = 1;
+  c->max_steps = 1000000;
+  for (int k = 0; k < 6; ++k) c->seed[k] = 12345.0;
+  c->nevents = 1;
+  c->precision = 0;
+  c->engine = 1;
+}
+
+int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
+                     const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
+                     int *d_primary_steps, gx_transport_stats *stats, gx_stream_t s)
+{
+  if (!ctx || !cfg) return set_error(GX_ERR_ARG, "gx_transport_run: null argument");
+  if (nprim < 0 || (nprim > 0 && (!d_type || !d_E || !d_pos || !d_dir)) || !d_edep || nvol <= 0)
+    return set_error(GX_ERR_ARG, "gx_transport_run: bad arguments");
+  if (cfg->geometry == 1 && (cfg->nlayers <= 0 || cfg->t_abs <= 0 || cfg->t_gap <= 0 || cfg->half_trans <= 0 ||
+                             nvol < 2 * cfg->nlayers))
+    return set_error(GX_ERR_ARG, "gx_transport_run: bad calorimeter (nvol must be >= 2 nlayers)");
+  if (cfg->axis < 0 || cfg->axis > 2 || cfg->precision < 0 || cfg->precision > 1 || cfg->engine < 0 ||
+      cfg->engine > 1 || cfg->nevents < 1)
+    return set_error(GX_ERR_ARG, "gx_transport_run: bad config");
+  if (cfg->box_mat < 0 || cfg->box_mat > 2) return set_error(GX_ERR_ARG, "gx_transport_run: bad box material");
+  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
+    return set_error(GX_ERR_ARG, "gx_transport_run: block_size must be a multiple of 32, at most 256");
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  cudaSetDevice(C->device);
+  if (cfg->precision == 1)
+    return run<float>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
+                      stream_of(s));
+  return run<double>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
+                     stream_of(s));
+}
+
+int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *h_type,
+                          const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
+                          double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats)
+{
+  if (!ctx || !cfg || nprim < 0 || !h_edep || nvol <= 0) return set_error(GX_ERR_ARG, "gx_transport_run_host: bad arguments");
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  cudaSetDevice(C->device);
+  size_t n = (size_t)(nprim > 0 ? nprim : 1), nt = (size_t)cfg->nevents * nvol;
+  int *dt = nullptr, *dev = nullptr, *dps = nullptr;
+  double *dE = nullptr, *dp = nullptr, *dd = nullptr, *ded = nullptr;
+  cudaStream_t s;
+  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  cudaError_t e = cudaSuccess;
+  int rc = GX_OK;
+  if ((e = cudaMallocAsync((void **)&dt, n * sizeof(int), s)) || (e = cudaMallocAsync((void **)&dE, n * sizeof(double), s)) ||
+      (e = cudaMallocAsync((void **)&dp, 3 * n * sizeof(double), s)) ||
+      (e = cudaMallocAsync((void **)&dd, 3 * n * sizeof(double), s)) ||
+      (e = cudaMallocAsync((void **)&ded, nt * sizeof(double), s)))
+    rc = cuda_error(e, "gx_transport_run_host alloc");
+  if (!rc && h_event && (e = cudaMallocAsync((void **)&dev, n * sizeof(int), s))) rc = cuda_error(e, "alloc");
+  if (!rc && h_primary_steps && (e = cudaMallocAsync((void **)&dps, n * sizeof(int), s))) rc = cuda_error(e, "alloc");
+  if (!rc && nprim > 0) {
+    cudaMemcpyAsync(dt, h_type, nprim * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dE, h_E, nprim * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dp, h_pos, 3 * nprim * sizeof(double), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(dd, h_dir, 3 * nprim * sizeof(double), cudaMemcpyHostToDevice, s);
+    if (dev) cudaMemcpyAsync(dev, h_event, nprim * sizeof(int), cudaMemcpyHostToDevice, s);
+  }
+  if (!rc) {
+    cudaMemsetAsync(ded, 0, nt * sizeof(double), s);
+    if (dps) cudaMemsetAsync(dps, 0, n * sizeof(int), s);
+    rc = gx_transport_run(ctx, cfg, nprim, dt, dE, dp, dd, dev, ded, nvol, dps, stats, reinterpret_cast<gx_stream_t>(s));
+  }
+  if (!rc) {
+    cudaMemcpyAsync(h_edep, ded, nt * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (dps) cudaMemcpyAsync(h_primary_steps, dps, nprim * sizeof(int), cudaMemcpyDeviceToHost, s);
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_error(e, "gx_transport_run_host copy back");
+  }
+  cudaFreeAsync(dt, s);
+  cudaFreeAsync(dE, s);
+  cudaFreeAsync(dp, s);
+  cudaFreeAsync(dd, s);
+  cudaFreeAsync(ded, s);
+  if (dev) cudaFreeAsync(dev, s);
+  if (dps) cudaFreeAsync(dps, s);
+  cudaStreamSynchronize(s);
+  cudaStreamDestroy(s);
+  return rc;
+}
+
+} // extern "C"

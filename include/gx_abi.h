@@ -1,0 +1,209 @@
+/*
+ * gx_abi.h -- C ABI of the B200-native EM particle-transport step path.
+ *
+ * Every entry point is extern "C", takes plain pointers and sizes, returns an
+ * int status (GX_OK = 0, negative on error; gx_last_error_string() explains)
+ * and never throws.  Pointers named d_* are device pointers; calls that take a
+ * cudaStream_t are asynchronous on that stream.  The caller owns all buffers
+ * it passes in (as the reference's ProxyDeviceManager does,
+ * source/Geant/proxy/src/ProxyDeviceManager.cpp:100-204).
+ *
+ * Units: mm, MeV, ns (the reference's CLHEP units,
+ * source/Geant/proxy/ProxySystemOfUnits.hpp); field in tesla.
+ *
+ * MRG32k3a states are six uint32 words per stream, stored as six planes of n
+ * words (word k of stream i at index k * n + i).  The words are the six
+ * integers the reference keeps as doubles (MRG32k3a.hpp:45-49).
+ */
+#ifndef GX_ABI_H
+#define GX_ABI_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *gx_stream_t; /* a cudaStream_t */
+
+enum {
+  GX_OK = 0,
+  GX_ERR_ARG = -1,      /* bad argument */
+  GX_ERR_CUDA = -2,     /* a CUDA call failed */
+  GX_ERR_DATA = -3,     /* physics data missing or malformed */
+  GX_ERR_OVERFLOW = -4, /* a track store or stack ran out of room */
+  GX_ERR_ITERCAP = -5,  /* an iteration cap was hit (tracks retired, see stats) */
+  GX_ERR_NODEVICE = -6  /* no CUDA device */
+};
+
+/* physics-table ids, source/Geant/proxy/ProxyPhysicsTableIndex.hpp:23-45 */
+enum {
+  GX_DEDX_eBrem_em, GX_DEDX_eBrem_ep, GX_DEDX_eIoni_em, GX_DEDX_eIoni_ep,
+  GX_InverseRange_em, GX_InverseRange_ep, GX_Ionisation_em, GX_Ionisation_ep,
+  GX_Lambda_compt, GX_Lambda_conv, GX_Lambda_eBrem_em, GX_Lambda_eBrem_ep,
+  GX_Lambda_eIoni_em, GX_Lambda_eIoni_ep, GX_LambdaMod1_msc_em, GX_LambdaMod1_msc_ep,
+  GX_LambdaPrim_compt, GX_LambdaPrim_phot, GX_Range_em, GX_Range_ep,
+  GX_NTABLES
+};
+
+/* interaction models (the reference's ProxyEmModel family, plus the two e+
+ * models it lacks) */
+enum { GX_KLEIN_NISHINA, GX_SAUTER_GAVRILA, GX_BETHE_HEITLER, GX_SELTZER_BERGER, GX_MOLLER,
+       GX_BHABHA, GX_ANNIHILATION };
+/* processes for gx_post_step_gpil, source/Geant/proxy/ProxyProcessIndex.cuh:23-41 */
+enum { GX_PROC_COMPTON, GX_PROC_CONVERSION, GX_PROC_PHOTOELECTRIC, GX_PROC_BREMSSTRAHLUNG,
+       GX_PROC_IONIZATION };
+enum { GX_MODE_QUIRK = 0, GX_MODE_PHYSICS = 1 };
+
+typedef struct gx_ctx gx_ctx;
+
+/* ------------------------------------------------------------- context */
+const char *gx_last_error_string(void);
+int gx_version(void);
+/* Loads the Geant4-format ASCII tables, cut table, Seltzer-Berger and shell
+ * data from datadir and relocates them to the device.  Replaces
+ * ProxyDataManager::ProxyDataManager + RetrievePhysicsData + RetrieveCutsTable
+ * + RelocatePhysicsData (source/Geant/proxy/src/ProxyDataManager.cu:27-163). */
+int gx_ctx_create(const char *datadir, int device, gx_ctx **out);
+int gx_ctx_destroy(gx_ctx *ctx);
+
+/* --------------------------------------------------------------- RNG */
+/* Streams i = 0..n-1 start at substream (first + i) of the stream whose first
+ * state is seed: seed * A^((first + i) 2^76), computed on the device by
+ * skip-ahead.  Equivalent to (first + i) calls of MRG32k3a::AdvanceState(76, 0)
+ * (source/Geant/random/src/MRG32k3a.cpp:167-178). */
+int gx_rng_substreams(const double seed[6], long long first, int n, uint32_t *d_states, gx_stream_t s);
+/* MRG32k3a::AdvanceState(e, c) applied to every stream (MRG32k3a.cpp:167-205). */
+int gx_rng_advance(uint32_t *d_states, int n, long long e, long long c, gx_stream_t s);
+/* k draws per stream, out[j * n + i]: RNG<MRG32k3a>::Uniform(State_t*)
+ * (source/Geant/random/RNG.hpp:67-70, MRG32k3a.cpp:124-163). */
+int gx_rng_uniform(uint32_t *d_states, int n, int k, double *d_out, gx_stream_t s);
+/* MRG32k3a::Initialize(long streamId) (MRG32k3a.cpp:69-82), one state per id. */
+int gx_rng_stream_id(const long long *h_ids, int n, uint32_t *d_states, gx_stream_t s);
+
+/* ------------------------------------------------------------- tables */
+/* ProxyPhysicsTable::Value(mat, E) (ProxyPhysicsTable.cu:121-125 ->
+ * ProxyPhysicsVector::Value, ProxyPhysicsVector.cu:469-483), FP64. */
+int gx_table_value(gx_ctx *ctx, int table, int mat, const double *d_E, double *d_out, int n, gx_stream_t s);
+/* ProxyPhysicsVector::InvRangeValue (ProxyPhysicsVector.cu:491-524). */
+int gx_table_invrange(gx_ctx *ctx, int table, int mat, const double *d_r, double *d_out, int n, gx_stream_t s);
+/* Proxy2DVector::Value (Proxy2DVector.cpp:37-67) on Seltzer-Berger table
+ * which: 0 = br11 (the reference's hard-coded slot 10), 1 = br18, 2 = br82. */
+int gx_sb_value(gx_ctx *ctx, int which, const double *d_x, const double *d_y, double *d_out, int n,
+                gx_stream_t s);
+/* ProxyDataManager::GetCutValue(index, ipart) (ProxyDataManager.cuh:52-54), host. */
+int gx_cut_value(gx_ctx *ctx, int index, int ipart, double *out);
+
+/* ------------------------------------------------------------- models */
+typedef struct {
+  int mode;              /* GX_MODE_QUIRK: the reference's hard-coded values; GX_MODE_PHYSICS */
+  int Z;                 /* element for physics mode */
+  double cut;            /* production cut (MeV) for SB, Moller, Bhabha in physics mode */
+  double density_factor; /* SB dielectric suppression factor */
+  int sb_table;          /* 0 br11, 1 br18, 2 br82 */
+} gx_model_params;
+
+/* A batch of ProxyEmModel<T>::SampleSecondaries(TrackState*) calls
+ * (source/Geant/proxy/ProxyEmModel.hpp:79-83; ProxyKleinNishina.hpp:96-166,
+ * ProxySauterGavrila.hpp:67-130, ProxyBetheHeitler.hpp:64-182,
+ * ProxySeltzerBerger.hpp:204-286, ProxyMollerScattering.hpp:92-159).
+ * Track i has kinetic energy d_E[i], direction d_dir[3i..3i+2] and stream i
+ * of d_rng; outputs: updated energy / direction / deposit / status (1 killed),
+ * number of secondaries and up to two secondaries (type 0 gamma, 1 e-, 2 e+;
+ * energies d_sec_E[2i+k], directions d_sec_dir[6i+3k..]).  The reference
+ * builds its secondaries and drops them; these are returned. */
+int gx_interact(gx_ctx *ctx, int model, const gx_model_params *p, int n, uint32_t *d_rng, const double *d_E,
+                const double *d_dir, double *d_E_out, double *d_dir_out, double *d_edep, int *d_status,
+                int *d_nsec, int *d_sec_type, double *d_sec_E, double *d_sec_dir, gx_stream_t s);
+/* CrossSectionPerAtom(Z, E) of Klein-Nishina (ProxyKleinNishina.hpp:62-93) or
+ * Moller (ProxyMollerScattering.hpp:61-89), mm^2. */
+int gx_xs_per_atom(int model, double Z, const double *d_E, double *d_out, int n, gx_stream_t s);
+
+/* ---------------------------------------------------------- processes */
+/* ProxyEmProcess<T>::PostStepGPIL (ProxyEmProcess.hpp:122-151) for a batch:
+ * reads lambda from the process's table at material mat (the reference
+ * forces mat = 2 at :133), updates NIL d_nil and the saved 1/lambda d_saved,
+ * returns the proposed step. */
+int gx_post_step_gpil(gx_ctx *ctx, int process, int mat, int n, uint32_t *d_rng, const double *d_E,
+                      const double *d_pstep_prev, double *d_nil, double *d_saved, double *d_step,
+                      gx_stream_t s);
+/* ProxyIonization::AlongStepGPIL (ProxyIonization.hpp:108-128). */
+int gx_ioni_along_gpil(gx_ctx *ctx, int mode, int charge, const int *d_mat, const double *d_E, double *d_out,
+                       int n, gx_stream_t s);
+/* ProxyIonization::AlongStepDoIt (ProxyIonization.hpp:130-168): d_E updated, d_edep added to. */
+int gx_ioni_along_doit(gx_ctx *ctx, int mode, int charge, const int *d_mat, const double *d_step, double *d_E,
+                       double *d_edep, int n, gx_stream_t s);
+
+/* -------------------------------------------------------------- helix */
+/* ConstFieldHelixStepper::DoStepArr (ConstFieldHelixStepper.hpp:249-302):
+ * SoA inputs and outputs; kB2C is the reference's -0.299792458e-3 for
+ * GeV / kilogauss / cm, or -0.299792458 for MeV / tesla / mm. */
+int gx_helix_dostep(const double B[3], double kB2C, int n, const double *d_posx, const double *d_posy,
+                    const double *d_posz, const double *d_dirx, const double *d_diry, const double *d_dirz,
+                    const double *d_charge, const double *d_momentum, const double *d_step, double *d_newposx,
+                    double *d_newposy, double *d_newposz, double *d_newdirx, double *d_newdiry,
+                    double *d_newdirz, gx_stream_t s);
+
+/* ---------------------------------------------------------- transport */
+typedef struct {
+  int geometry;            /* 0: one box of material box_mat; 1: layered calorimeter */
+  int axis;                /* layering (or box) axis: 0 x, 1 y, 2 z */
+  int nlayers;
+  double t_abs, t_gap;     /* absorber (Pb) and gap (LAr) thickness, mm */
+  double half_trans;       /* calorimeter half transverse size, mm */
+  double box_half[3], box_centre[3];
+  int box_mat;             /* 1 Pb, 2 LAr */
+  double Bz;               /* tesla, along z */
+  int charged_local;       /* 1: e-/e+ secondaries deposit their kinetic energy locally */
+  int max_steps;           /* per-track step cap (retired with an error count above it) */
+  double seed[6];
+  long long first_substream;
+  int nevents;             /* tally rows */
+  /* engine */
+  int precision;           /* 0 FP64, 1 FP32-mixed */
+  int engine;              /* 0 plain loop (one mixed queue, host-driven), 1 batched (per-type queues, graph) */
+  int block_size;          /* threads per block (0: default) */
+  int blocks_per_sm;       /* resident blocks per SM for the grid (0: default) */
+  long long capacity;      /* track slots per particle type (0: default) */
+  long long refill_below;  /* inject / refill when fewer tracks than this are in flight (0: default) */
+  int graph_iters;         /* iterations per CUDA-graph launch between host checks (0: default) */
+  int profile;             /* 1: no graph; CUDA events around every step kernel (per-kernel times in stats) */
+} gx_transport_config;
+
+typedef struct {
+  long long steps, substeps, tracks;
+  long long secondaries[3];
+  long long n_pair, n_annih, errors;
+  double escaped;
+  long long iterations;
+  long long peak_in_flight;
+  double kernel_ms;        /* device time of the whole transport loop, CUDA events */
+  /* per step kernel (gamma, e-, e+; the plain engine uses entry 0): */
+  double step_ms[3];       /* summed device time (profile mode only) */
+  long long step_launches[3];
+  long long tracks_read[3];    /* track records read */
+  long long tracks_written[3]; /* track records written (survivors and secondaries) */
+  long long bytes_per_track;   /* size of one track record in the stores */
+} gx_transport_stats;
+
+void gx_transport_config_default(gx_transport_config *cfg);
+/* Transports nprim primaries (device arrays: type 0 gamma / 1 e- / 2 e+,
+ * kinetic energy, position xyz, direction xyz, event index) to completion and
+ * adds their energy deposits to d_edep[event * nvol + volume] (FP64).
+ * Replaces the reference's DoStep / OneStep / InnerStep loop
+ * (source/Geant/proxy/test/test_BasicCpuTransport.cpp:358-550) and its
+ * device-side launch wrappers (source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).
+ * d_primary_steps (optional) receives the step count of each primary track. */
+int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type,
+                     const double *d_E, const double *d_pos, const double *d_dir, const int *d_event,
+                     double *d_edep, int nvol, int *d_primary_steps, gx_transport_stats *stats, gx_stream_t s);
+/* The same from host buffers: copies the primaries in and the tallies out
+ * inside the call (h_edep is overwritten). */
+int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *h_type,
+                          const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
+                          double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

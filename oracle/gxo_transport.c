@@ -101,11 +101,11 @@ static double trans_centre(const world_t *w, int b)
   return w->c->geometry == 0 ? w->c->box_centre[b] : 0.0;
 }
 
-/* Locate a point; on a plane (within 1e-9 mm) the direction picks the side. */
+/* Locate a point; on a plane (within 1e-12 mm) the direction picks the side. */
 static int locate(const world_t *w, const double *p, const double *d)
 {
   const gxo_config_t *c = w->c;
-  const double tol = 1e-9;
+  const double tol = 1e-12;
   int a = c->axis;
   for (int b = 0; b < 3; ++b) {
     if (b == a) continue;
