@@ -55,6 +55,8 @@ struct Ctl {
   long long in_flight, pending, peak, iterations;
   unsigned long long stat[kNStat];
   double escaped;
+  const double *cumE; // inclusive prefix sum of the primary energies
+  double wave_energy; // primary energy injected per wave, at most
 };
 
 struct Prims {
@@ -173,6 +175,34 @@ __device__ __forceinline__ int next_volume(const Geom &g, int vol, int plane)
   if (plane == 2 || g.geometry == 0) return -1;
   int nv = vol + (plane > 0 ? 1 : -1);
   return (nv < 0 || nv >= 2 * g.nlayers) ? -1 : nv;
+}
+
+// Volume after a helix sub-step that started in vol.  An end point within
+// kSnap of a face it is moving out through (or past it) is put on that face
+// and enters the neighbour; otherwise the point is located.  The reference
+// pushes 2e-9 mm past the straight-line boundary and locates the helix end
+// point, which lands within rounding of the plane often enough for ulp-level
+// differences to decide the crossing; the snap distance is far from both.
+constexpr double kSnap = 1e-6;
+__device__ __forceinline__ int relocate(const Geom &g, int vol, double *p, const double *d)
+{
+  int a = g.axis;
+  double lo, hi;
+  slab_bounds(g, vol, lo, hi);
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    double h = thalf(g, b), q = p[b] - tcentre(g, b);
+    if ((d[b] > 0 && h - q < kSnap) || (d[b] < 0 && q + h < kSnap)) return -1;
+  }
+  if (d[a] > 0 && hi - p[a] < kSnap) {
+    p[a] = hi;
+    return next_volume(g, vol, 1);
+  }
+  if (d[a] < 0 && p[a] - lo < kSnap) {
+    p[a] = lo;
+    return next_volume(g, vol, -1);
+  }
+  return locate(g, p, d);
 }
 
 // ---------------------------------------------------------- cross sections
@@ -328,7 +358,7 @@ __device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool
     total += s;
     remaining -= s;
     L.st[S_SUBSTEPS]++;
-    int v = locate(g, pos, dir);
+    int v = relocate(g, t.vol, pos, dir);
     if (v != t.vol || remaining <= 1e-10) {
       if (v != t.vol) {
         crossed = true;
@@ -732,12 +762,50 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
     budget -= take;
     pend += ctl->stack_count[q];
   }
+  // primaries: a wave carries at most wave_energy (a shower's population peaks
+  // in proportion to its energy, long after the wave is injected)
   long long tp = 0;
-  if (budget > 0) tp = min(budget, ctl->nprim - ctl->prim_next);
+  if (budget > 0 && ctl->prim_next < ctl->nprim) {
+    long long lo = ctl->prim_next, hi = min(ctl->nprim, ctl->prim_next + budget);
+    double e0 = lo > 0 ? ctl->cumE[lo - 1] : 0.0;
+    // largest k in (lo, hi] with cumE[k - 1] - e0 <= wave_energy; at least one primary
+    long long a = lo + 1, b = hi;
+    while (a < b) {
+      long long m = (a + b + 1) / 2;
+      if (ctl->cumE[m - 1] - e0 <= ctl->wave_energy)
+        a = m;
+      else
+        b = m - 1;
+    }
+    tp = a - lo;
+  }
   ctl->take_prim = tp;
   ctl->in_flight = fl;
   ctl->pending = pend;
   if (fl > ctl->peak) ctl->peak = fl;
+}
+
+// Inclusive prefix sum of the primary energies, one block: each thread scans a
+// contiguous chunk, the chunk totals are scanned in shared memory.
+__global__ void __launch_bounds__(1024) k_prefix_energy(const double *__restrict__ E, long long n,
+                                                        double *__restrict__ out)
+{
+  __shared__ double part[1024];
+  int t = threadIdx.x, nt = blockDim.x;
+  long long chunk = (n + nt - 1) / nt;
+  long long b = t * chunk, e = min(n, b + chunk);
+  double s = 0.0;
+  for (long long i = b; i < e; ++i) s += E[i];
+  part[t] = s;
+  __syncthreads();
+  if (t == 0)
+    for (int k = 1; k < nt; ++k) part[k] += part[k - 1];
+  __syncthreads();
+  double run = t > 0 ? part[t - 1] : 0.0;
+  for (long long i = b; i < e; ++i) {
+    run += E[i];
+    out[i] = run;
+  }
 }
 
 __device__ __forceinline__ void jump_matvec(const uint64_t *A, uint64_t v[3], uint64_t m)
@@ -844,6 +912,8 @@ struct Engine {
   cudaGraphExec_t graph = nullptr;
   int graph_iters = 0;
   std::vector<char> graph_args; // launch arguments the graph was captured with
+  double *cumE = nullptr;
+  long long cumE_cap = 0;
   cudaStream_t s1 = nullptr, s2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_j1 = nullptr, ev_j2 = nullptr;
 };
@@ -884,6 +954,7 @@ void release_engine(Ctx *c)
   if (e->graph) cudaGraphExecDestroy(e->graph);
   if (e->pool) cudaFree(e->pool);
   if (e->ctl) cudaFree(e->ctl);
+  if (e->cumE) cudaFree(e->cumE);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->s1) cudaStreamDestroy(e->s1);
   if (e->s2) cudaStreamDestroy(e->s2);
@@ -937,8 +1008,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   const int prec = std::is_same<R, float>::value ? 1 : 0;
   const bool batched = cfg->engine == 1;
   const int nstores = batched ? 3 : 1;
-  long long cap = cfg->capacity > 0 ? cfg->capacity : (batched ? (1LL << 22) : (3LL << 22));
-  long long stack_cap = std::max(2 * cap, 1LL << 20);
+  long long cap = cfg->capacity > 0 ? cfg->capacity : (batched ? (1LL << 24) : (3LL << 24));
+  long long stack_cap = std::max(cap, 1LL << 20);
   Engine *&E = C->engine;
   if (E && (E->precision != prec || E->engine != cfg->engine || E->cap != cap)) release_engine(C);
   cudaError_t err;
@@ -1022,10 +1093,22 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.grid = C->num_sms * bpsm;
   L.smem = 768 * sizeof(double);
 
+  if (nprim > E->cumE_cap) {
+    if (E->cumE) cudaFree(E->cumE);
+    E->cumE = nullptr;
+    E->cumE_cap = 0;
+    if ((err = cudaMalloc((void **)&E->cumE, sizeof(double) * nprim)) != cudaSuccess)
+      return cuda_error(err, "transport primary energies");
+    E->cumE_cap = nprim;
+  }
+  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, E->cumE);
   Ctl h;
   std::memset(&h, 0, sizeof(h));
   h.nprim = nprim;
   h.iterations = -1; // the planning launch below is not an iteration
+  h.cumE = E->cumE;
+  // a 10 GeV shower peaks near 800 tracks in flight: ~0.08 per MeV of primary energy
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
   err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return cuda_error(err, "transport control init");
   // first refill plan

@@ -168,6 +168,7 @@ typedef struct {
   long long refill_below;  /* inject / refill when fewer tracks than this are in flight (0: default) */
   int graph_iters;         /* iterations per CUDA-graph launch between host checks (0: default) */
   int profile;             /* 1: no graph; CUDA events around every step kernel (per-kernel times in stats) */
+  double wave_energy;      /* primary energy (MeV) injected per wave, at most (0: from capacity) */
 } gx_transport_config;
 
 typedef struct {

@@ -188,6 +188,32 @@ static int next_volume(const world_t *w, int vol, int plane)
   return (nv < 0 || nv >= 2 * w->c->nlayers) ? -1 : nv;
 }
 
+/* Volume after a helix sub-step started in vol: an end point within 1e-6 mm
+ * of a face it moves out through (or past it) is put on the face and enters
+ * the neighbour; otherwise the point is located (the engine's rule, so that
+ * crossings do not hinge on rounding near the reference's 2e-9 mm push). */
+static int relocate(const world_t *w, int vol, double *p, const double *d)
+{
+  const double snap = 1e-6;
+  int a = w->c->axis;
+  double lo, hi;
+  slab_bounds(w, vol, &lo, &hi);
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    double h = trans_half(w, b), q = p[b] - trans_centre(w, b);
+    if ((d[b] > 0 && h - q < snap) || (d[b] < 0 && q + h < snap)) return -1;
+  }
+  if (d[a] > 0 && hi - p[a] < snap) {
+    p[a] = hi;
+    return next_volume(w, vol, 1);
+  }
+  if (d[a] < 0 && p[a] - lo < snap) {
+    p[a] = lo;
+    return next_volume(w, vol, -1);
+  }
+  return locate(w, p, d);
+}
+
 /* -------------------------------------------------------- cross sections */
 static double lambda_table(const world_t *w, int table, int mat, double e)
 {
@@ -311,7 +337,7 @@ static double field_propagate(const world_t *w, track_t *tr, double pstep, int *
     total += s;
     remaining -= s;
     t->substeps++;
-    int v = locate(w, tr->pos, tr->dir);
+    int v = relocate(w, tr->vol, tr->pos, tr->dir);
     if (v != tr->vol) {
       *crossed = 1;
       *newvol = v;
