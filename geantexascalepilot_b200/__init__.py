@@ -11,5 +11,5 @@ from .api import (ANNIHILATION, BETHE_HEITLER, BHABHA, ELECTRON, GAMMA, KLEIN_NI
                   MRG32k3a, ProxyAnnihilation, ProxyBetheHeitler, ProxyBhabhaScattering, ProxyBremsstrahlung,
                   ProxyCompton, ProxyConversion, ProxyDataManager, ProxyIonization, ProxyKleinNishina,
                   ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, default_config,
-                  transport, transport_host)
+                  transport, transport_host, transport_noalloc)
 from . import configs  # noqa: F401

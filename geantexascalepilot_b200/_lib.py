@@ -85,6 +85,8 @@ _SIGS = {
     "gx_transport_run": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P, C.POINTER(TransportStats), P]),
     "gx_transport_run_host": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P,
                                   C.POINTER(TransportStats)]),
+    "gx_transport_run_noalloc": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I,
+                                     C.POINTER(TransportStats), P]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)

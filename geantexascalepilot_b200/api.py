@@ -310,3 +310,28 @@ def transport_host(dm, cfg, types, E, pos, direction, events=None, nvol=None):
     check(lib.gx_transport_run_host(dm.handle, C.byref(cfg), t.size, vp(t), vp(E), vp(p), vp(d), vp(ev), vp(edep),
                                     nvol, None, C.byref(st)))
     return edep, st.as_dict()
+
+
+NOALLOC_CAPACITY = 16384
+NOALLOC_MAX_PRIMARIES = 4096
+
+
+def transport_noalloc(dm, cfg, types, E, pos, direction, events=None, nvol=None, edep=None):
+    """gx_transport_run_noalloc: the plain FP64 loop on the library's static
+    device array, for callers that cannot allocate device memory while they
+    run (at most 4096 primaries, 16384 tracks in flight).  Inputs must already
+    be CUDA tensors if the caller wants no allocation at all; array-likes are
+    copied to the device here, by torch."""
+    t = _dev(types, torch.int32)
+    E = _dev(E, torch.float64)
+    p = _dev(pos, torch.float64).reshape(-1, 3)
+    d = _dev(direction, torch.float64).reshape(-1, 3)
+    ev = _dev(events, torch.int32) if events is not None else None
+    if nvol is None:
+        nvol = 2 * cfg.nlayers if cfg.geometry == 1 else 1
+    if edep is None:
+        edep = torch.zeros((cfg.nevents, nvol), dtype=torch.float64, device="cuda")
+    st = TransportStats()
+    check(lib.gx_transport_run_noalloc(dm.handle, C.byref(cfg), t.numel(), _ptr(t), _ptr(E), _ptr(p), _ptr(d),
+                                       _ptr(ev), _ptr(edep), nvol, C.byref(st), _stream()))
+    return edep, st.as_dict()

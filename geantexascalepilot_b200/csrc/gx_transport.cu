@@ -19,6 +19,7 @@
 #include "gx_internal.cuh"
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 #include <cmath>
 #include <cstring>
@@ -1336,3 +1337,204 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
 }
 
 } // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free transport (gx_transport_run_noalloc).
+//
+// For callers that must not allocate device memory while they run -- a host
+// framework whose caching allocator owns the device memory, a process under a
+// fixed memory budget, a time-critical loop that cannot absorb the implicit
+// device synchronisation of cudaMalloc/cudaFree -- this entry point runs the
+// plain FP64 loop on one static device array owned by the library instead of
+// allocating track stores, the control block, the primary-energy prefix sums
+// and the skip-ahead table.  Limits: at most kNoallocCapacity tracks in
+// flight (mixed store), as many deferred on the stack, at most
+// kNoallocMaxPrimaries primaries per call.  The array is shared by every call
+// on a device and keeps the last call's contents; each call rewrites the parts
+// that must start from zero (the control block) before its first launch.
+// Calls that overlap on the GPU (two streams, two host threads) race on it.
+// The first call on a device sets up that device (cudaGetSymbolAddress and
+// the skip-ahead table upload) and should come before any stream capture.
+namespace gx {
+
+constexpr long long kNoallocCapacity = 16384;
+constexpr int kNoallocMaxPrimaries = 4096;
+constexpr size_t kNoallocStoreBytes = 120 * (size_t)kNoallocCapacity; // FP64 record with type field
+constexpr size_t kNoallocCtlBytes = 4096;
+constexpr size_t kNoallocCumEBytes = sizeof(double) * kNoallocMaxPrimaries;
+constexpr size_t kNoallocJumpBytes = sizeof(uint64_t) * 2 * 64 * 9;
+constexpr size_t kNoallocBytes = 3 * kNoallocStoreBytes + kNoallocCtlBytes + kNoallocCumEBytes + kNoallocJumpBytes;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoallocBytes];
+
+static std::mutex g_noalloc_mu;
+static unsigned char *g_noalloc_ptr[64] = {nullptr};
+
+// Once per device, with that device current: the device address of the
+// static array, and the skip-ahead table written into it.
+static int noalloc_setup(int dev, unsigned char **out)
+{
+  static_assert(sizeof(Ctl) <= kNoallocCtlBytes, "control block does not fit");
+  if (dev < 0 || dev >= 64) return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: device index %d", dev);
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return cuda_error(e, "gx_transport_run_noalloc: cudaGetSymbolAddress");
+    uint64_t h[2][64][9];
+    const uint64_t m[2] = {4294967087ULL, 4294944443ULL};
+    for (int c = 0; c < 2; ++c) {
+      uint64_t P[9];
+      jump_matrix(c, 76, 0, P);
+      for (int b = 0; b < 64; ++b) {
+        std::memcpy(h[c][b], P, sizeof(P));
+        mat_mul(P, P, P, m[c]);
+      }
+    }
+    unsigned char *base = (unsigned char *)p;
+    e = cudaMemcpy(base + 3 * kNoallocStoreBytes + kNoallocCtlBytes + kNoallocCumEBytes, h, sizeof(h),
+                   cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_error(e, "gx_transport_run_noalloc: skip-ahead table");
+    g_noalloc_ptr[dev] = base;
+  }
+  *out = g_noalloc_ptr[dev];
+  return GX_OK;
+}
+
+} // namespace gx
+
+extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type,
+                                        const double *d_E, const double *d_pos, const double *d_dir,
+                                        const int *d_event, double *d_edep, int nvol, gx_transport_stats *stats,
+                                        gx_stream_t stream)
+{
+  using namespace gx;
+  if (!ctx || !cfg) return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: null argument");
+  if (nprim < 0 || (nprim > 0 && (!d_type || !d_E || !d_pos || !d_dir)) || !d_edep || nvol <= 0)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: bad arguments");
+  if (nprim > kNoallocMaxPrimaries)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: %d primaries exceed the static limit of %d", nprim,
+                     kNoallocMaxPrimaries);
+  if (cfg->precision != 0)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: FP64 only (precision must be 0)");
+  if (cfg->geometry == 1 && (cfg->nlayers <= 0 || cfg->t_abs <= 0 || cfg->t_gap <= 0 || cfg->half_trans <= 0 ||
+                             nvol < 2 * cfg->nlayers))
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: bad calorimeter (nvol must be >= 2 nlayers)");
+  if (cfg->axis < 0 || cfg->axis > 2 || cfg->nevents < 1 || cfg->box_mat < 0 || cfg->box_mat > 2)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: bad config");
+  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: block_size must be a multiple of 32, at most 256");
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  cudaError_t err = cudaSetDevice(C->device);
+  if (err != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: cudaSetDevice");
+  unsigned char *base = nullptr;
+  int rc = noalloc_setup(C->device, &base);
+  if (rc) return rc;
+  cudaStream_t s = stream_of(stream);
+  const long long cap = kNoallocCapacity;
+
+  Launch<double> L;
+  std::memset(&L.a, 0, sizeof(L.a));
+  size_t off = 0;
+  uintptr_t b = (uintptr_t)base;
+  L.a.st[0][0] = carve<double>(b, off, cap, true);
+  L.a.st[1][0] = carve<double>(b, off, cap, true);
+  L.a.stack[0] = carve<double>(b, off, cap, true);
+  if (off != 3 * kNoallocStoreBytes) return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: layout");
+  for (int q = 1; q < 3; ++q) {
+    L.a.st[0][q] = L.a.st[0][0];
+    L.a.st[1][q] = L.a.st[1][0];
+    L.a.stack[q] = L.a.stack[0];
+  }
+  Ctl *ctl = (Ctl *)(base + 3 * kNoallocStoreBytes);
+  double *cumE = (double *)(base + 3 * kNoallocStoreBytes + kNoallocCtlBytes);
+  const uint64_t *jump = (const uint64_t *)(base + 3 * kNoallocStoreBytes + kNoallocCtlBytes + kNoallocCumEBytes);
+  L.a.d = C->dev;
+  L.a.ctl = ctl;
+  Geom &g = L.a.g;
+  g.geometry = cfg->geometry;
+  g.axis = cfg->axis;
+  g.nlayers = cfg->nlayers;
+  g.box_mat = cfg->box_mat;
+  g.charged_local = cfg->charged_local;
+  g.nvol = nvol;
+  g.nevents = cfg->nevents;
+  g.t_abs = cfg->t_abs;
+  g.pitch = cfg->t_abs + cfg->t_gap;
+  g.x0 = -0.5 * cfg->nlayers * g.pitch;
+  g.total = cfg->nlayers * g.pitch;
+  g.half_trans = cfg->half_trans;
+  g.Bz = cfg->Bz;
+  for (int k = 0; k < 3; ++k) {
+    g.box_half[k] = cfg->box_half[k];
+    g.box_centre[k] = cfg->box_centre[k];
+  }
+  L.a.p.type = d_type;
+  L.a.p.event = d_event;
+  L.a.p.E = d_E;
+  L.a.p.pos = d_pos;
+  L.a.p.dir = d_dir;
+  for (int k = 0; k < 6; ++k) L.a.p.seed[k] = cfg->seed[k];
+  L.a.p.first_substream = cfg->first_substream;
+  L.a.p.jump = jump;
+  L.a.edep = d_edep;
+  L.a.pstep = nullptr;
+  L.a.nstores = 1;
+  L.a.refill_below = cfg->refill_below > 0 ? std::min(cfg->refill_below, cap) : cap / 2;
+  L.block = cfg->block_size > 0 ? cfg->block_size : 256;
+  L.grid = C->num_sms * (cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 4);
+  L.smem = 768 * sizeof(double);
+
+  // the control block starts from zero on every call
+  Ctl h;
+  std::memset(&h, 0, sizeof(h));
+  h.nprim = nprim;
+  h.iterations = -1;
+  h.cumE = cumE;
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
+  if ((err = cudaMemcpyAsync(ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+      (err = cudaStreamSynchronize(s)) != cudaSuccess)
+    return cuda_error(err, "gx_transport_run_noalloc: control block");
+  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, cumE);
+  k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, L.a.refill_below, cap);
+  Ctl hc;
+  long long iters = 0;
+  for (;;) {
+    k_refill<double><<<L.grid, L.block, 0, s>>>(L.a);
+    k_refill_done<<<1, 1, 0, s>>>(ctl);
+    k_step<double, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+    k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, L.a.refill_below, cap);
+    if ((err = cudaGetLastError()) != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: launch");
+    if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+        (err = cudaStreamSynchronize(s)) != cudaSuccess)
+      return cuda_error(err, "gx_transport_run_noalloc: iteration");
+    ++iters;
+    if (hc.in_flight == 0 && hc.pending == 0) break;
+    if (iters > 2000000LL) return set_error(GX_ERR_ITERCAP, "gx_transport_run_noalloc: iteration cap");
+  }
+  k_count_new_tracks<<<1, 1, 0, s>>>(ctl);
+  if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
+      (err = cudaStreamSynchronize(s)) != cudaSuccess)
+    return cuda_error(err, "gx_transport_run_noalloc: end");
+  if (stats) {
+    std::memset(stats, 0, sizeof(*stats));
+    stats->steps = (long long)hc.stat[S_STEPS];
+    stats->substeps = (long long)hc.stat[S_SUBSTEPS];
+    stats->tracks = (long long)hc.stat[S_TRACKS];
+    for (int q = 0; q < 3; ++q) stats->secondaries[q] = (long long)hc.stat[S_SEC0 + q];
+    stats->n_pair = (long long)hc.stat[S_PAIR];
+    stats->n_annih = (long long)hc.stat[S_ANNIH];
+    stats->errors = (long long)(hc.stat[S_ERR] + hc.stat[S_OVERFLOW]);
+    stats->escaped = hc.escaped;
+    stats->iterations = hc.iterations;
+    stats->peak_in_flight = hc.peak;
+    stats->tracks_read[0] = (long long)hc.stat[S_READ0];
+    stats->tracks_written[0] = (long long)hc.stat[S_WRITE0];
+    stats->bytes_per_track = 120;
+  }
+  if (hc.err_flags & kErrOverflow)
+    return set_error(GX_ERR_OVERFLOW, "gx_transport_run_noalloc: more than %lld tracks in flight and deferred",
+                     2 * kNoallocCapacity);
+  if (hc.err_flags) return set_error(GX_ERR_ITERCAP, "gx_transport_run_noalloc: an iteration cap was hit");
+  return GX_OK;
+}

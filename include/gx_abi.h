@@ -204,6 +204,25 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
                           const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
                           double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats);
 
+/* gx_transport_run without any device allocation.  No counterpart in the
+ * reference.  For callers that must not allocate device memory while they
+ * run: a host framework whose caching allocator already owns the device
+ * memory, a process held to a fixed memory budget, or a time-critical loop
+ * that cannot take the implicit device synchronisation of cudaMalloc /
+ * cudaFree.  The plain FP64 loop runs on a static device array owned by the
+ * library (about 5.7 MB, held on every device that loads the library until the
+ * process exits): at most GX_NOALLOC_MAX_PRIMARIES primaries per call, at most
+ * GX_NOALLOC_CAPACITY tracks in flight plus as many deferred; larger inputs
+ * are rejected with GX_ERR_ARG and a message.  precision must be 0 (FP64);
+ * engine is ignored; d_edep is added to as in gx_transport_run.  Every call
+ * shares the array; calls that overlap on the GPU race on it.  The first call
+ * on a device sets that device up and should come before any stream capture. */
+#define GX_NOALLOC_CAPACITY 16384
+#define GX_NOALLOC_MAX_PRIMARIES 4096
+int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type,
+                             const double *d_E, const double *d_pos, const double *d_dir, const int *d_event,
+                             double *d_edep, int nvol, gx_transport_stats *stats, gx_stream_t s);
+
 #ifdef __cplusplus
 }
 #endif
