@@ -280,7 +280,9 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": None, "kernel": ["k_step<float,gamma>", "k_step<float,e->", "k_step<float,e+>"][k],
+                       "traffic": None, "kernel": ["gamma step: k_transport<float,0> + k_interact<float,0,*>",
+                                  "e- step: k_transport<float,1> + k_interact<float,1,*>",
+                                  "e+ step: k_transport<float,2> + k_interact<float,2,*>"][k],
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "algorithmic_bytes_per_launch": nbytes / max(1, stp["step_launches"][k]),
                        "avg_launch_ms": stp["step_ms"][k] / max(1, stp["step_launches"][k]),

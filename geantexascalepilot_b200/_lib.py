@@ -8,7 +8,7 @@ import ctypes as C
 import os
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "lib", "libgxb200.so")
+LIB_PATH = os.environ.get("GX_LIB_PATH") or os.path.join(PKG, "lib", "libgxb200.so")
 DATA_DIR = os.path.join(PKG, "data")
 
 GX_OK, GX_ERR_ARG, GX_ERR_CUDA, GX_ERR_DATA, GX_ERR_OVERFLOW, GX_ERR_ITERCAP, GX_ERR_NODEVICE = 0, -1, -2, -3, -4, -5, -6

@@ -58,6 +58,8 @@ struct Ctl {
   double escaped;
   const double *cumE; // inclusive prefix sum of the primary energies
   double wave_energy; // primary energy injected per wave, at most
+  long long refill_below, stack_cap;
+  long long qcount[3][3]; // interaction queues [particle][process]
 };
 
 struct Prims {
@@ -79,6 +81,8 @@ template <class R> struct Args {
   int *pstep;
   int nstores;
   long long refill_below;
+  int *queue[3][3]; // slot indices of tracks waiting for an interaction (batched engine)
+  long long qcap;
 };
 
 // ---------------------------------------------------------------- geometry
@@ -384,7 +388,8 @@ __device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool
 }
 
 template <class R>
-__device__ void run_model(const Data &d, const Geom &g, Track<R> &t, int proc, Secs<R> &sec, Local &L)
+__device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R> &t, int proc, Secs<R> &sec,
+                                          Local &L)
 {
   int mat = vol_material(g, t.vol);
   ModelParams mp;
@@ -447,12 +452,16 @@ __device__ void run_model(const Data &d, const Geom &g, Track<R> &t, int proc, S
   if (io.status == 1) t.E = R(0);
 }
 
+enum { kDone = 0, kAlive = 1, kInteract = 2 };
+
 // One OneStep (test_BasicCpuTransport.cpp:408-497 / InnerStep :358-403) in
-// physics mode; the oracle's one_step is the same algorithm in the same
-// order of random draws.  Returns false when the track is finished.
-template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
+// physics mode, up to the choice of the post-step interaction: GPIL, step
+// limit, propagation, NIL update, continuous loss.  Returns kDone (track
+// finished), kAlive (no interaction this step) or kInteract with *proc set
+// (for a stopped e+, proc 2 = annihilation at rest, at E = 0).
+template <class R> __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
+                                                                 int *proc)
 {
-  sec.n = 0;
   int mat = vol_material(g, t.vol);
   int np = (t.type == 1) ? 2 : 3;
   bool charged = t.type != 0;
@@ -506,7 +515,7 @@ template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<
   L.st[S_STEPS]++;
   if (newvol == -2) {
     L.deposit(t.event, vol0, (double)t.E);
-    return false;
+    return kDone;
   }
   if (charged) {
     R eloss = along_loss<R>(d, t.type, mat, step, t.E);
@@ -516,28 +525,44 @@ template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<
         int v = crossed ? newvol : vol0;
         if (v >= 0) {
           t.vol = v;
-          run_model(d, g, t, 2, sec, L);
-        } else {
-          L.escaped += 2.0 * kEMass;
+          t.E = R(0);
+          *proc = 2;
+          return kInteract;
         }
+        L.escaped += 2.0 * kEMass;
       }
-      return false;
+      return kDone;
     }
   }
   if (crossed) {
     t.vol = newvol;
     if (newvol < 0) {
       L.escaped += (double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0);
-      return false;
+      return kDone;
     }
-    return true;
+    return kAlive;
   }
   if (sel >= 0) {
     t.nil[sel] = R(-1);
-    run_model(d, g, t, sel, sec, L);
-    if (t.E <= R(0)) return false;
+    *proc = sel;
+    return kInteract;
   }
-  return true;
+  return kAlive;
+}
+
+// The whole OneStep, interaction included (the fused form the plain loop
+// runs); the oracle's one_step is the same algorithm in the same order of
+// random draws.  Returns false when the track is finished.
+template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
+{
+  sec.n = 0;
+  int proc = -1;
+  int r = transport_part(d, g, t, L, &proc);
+  if (r == kInteract) {
+    run_model(d, g, t, proc, sec, L);
+    return t.E > R(0);
+  }
+  return r == kAlive;
 }
 
 // ------------------------------------------------------------- load / store
@@ -729,13 +754,192 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_step(Args<R>
   }
 }
 
+// ------------------------------------------------- batched engine: split step
+// Shared-memory tally and block statistics of one step kernel.
+struct BlockTally {
+  double *sm_edep;
+  unsigned long long *sm_stat;
+  double *sm_esc;
+  int *sm_err;
+};
+
+__device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *edep, double *sm_edep,
+                                            unsigned long long *sm_stat, double *sm_esc, int *sm_err)
+{
+  L.nvol = g.nvol;
+  L.nevents = g.nevents;
+  L.g_edep = edep;
+  L.sm_edep = sm_edep;
+  L.sm_bins = (g.nvol <= 768) ? g.nvol : 0;
+  for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x) sm_edep[k] = 0.0;
+  if (threadIdx.x < kNStat) sm_stat[threadIdx.x] = 0;
+  if (threadIdx.x == 0) {
+    *sm_esc = 0.0;
+    *sm_err = 0;
+  }
+  __syncthreads();
+  L.escaped = 0.0;
+  L.err = 0;
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
+}
+
+__device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, double *sm_edep,
+                                          unsigned long long *sm_stat, double *sm_esc, int *sm_err)
+{
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k)
+    if (L.st[k]) atomicAdd(&sm_stat[k], (unsigned long long)L.st[k]);
+  if (L.escaped != 0.0) atomicAdd(sm_esc, L.escaped);
+  if (L.err) atomicOr(sm_err, L.err);
+  __syncthreads();
+  for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x)
+    if (sm_edep[k] != 0.0) atomicAdd(&edep[k], sm_edep[k]);
+  if (threadIdx.x < kNStat && sm_stat[threadIdx.x]) atomicAdd(&ctl->stat[threadIdx.x], sm_stat[threadIdx.x]);
+  if (threadIdx.x == 0) {
+    if (*sm_esc != 0.0) atomicAdd(&ctl->escaped, *sm_esc);
+    if (*sm_err) atomicOr(&ctl->err_flags, *sm_err);
+  }
+}
+
+// Transport part of the step for every track of type PT: survivors without an
+// interaction go to the next store; a track that interacts is written back in
+// place and its slot index is queued for the interaction kernel of its
+// process (warp prefix sums, one atomic per warp and destination).
+template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(const Args<R> *__restrict__ A)
+{
+  extern __shared__ double sm_edep[];
+  __shared__ unsigned long long sm_stat[kNStat];
+  __shared__ double sm_esc;
+  __shared__ int sm_err;
+  const Args<R> &a = *A;
+  const Data &d = *a.d;
+  Ctl *ctl = a.ctl;
+  const int par = ctl->parity;
+  const Store<R> &cur = a.st[par][PT];
+  const long long n = min(ctl->count[par][PT], cur.cap);
+  if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
+  Local L;
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    long long i = base + threadIdx.x;
+    bool active = i < n;
+    Track<R> t;
+    int r = kDone, proc = -1;
+    if (active) {
+      load_track(cur, i, PT, t);
+      L.st[S_READ0 + PT]++;
+      r = transport_part(d, a.g, t, L, &proc);
+      if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
+    }
+    long long slot = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][PT], r == kAlive ? 1 : 0);
+    long long qslot[3];
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+      if (PT == 1 && p == 2) {
+        qslot[p] = 0;
+        continue;
+      }
+      qslot[p] = warp_reserve((unsigned long long *)&ctl->qcount[PT][p], (r == kInteract && proc == p) ? 1 : 0);
+    }
+    if (r == kAlive) {
+      put_track(a, PT, slot, t, L);
+      L.st[S_WRITE0 + PT]++;
+    } else if (r == kInteract) {
+      store_track(cur, i, t);
+      L.st[S_WRITE0 + PT]++;
+      long long q = qslot[proc];
+      if (q < a.qcap) {
+        a.queue[PT][proc][q] = (int)i;
+      } else {
+        L.err |= kErrOverflow;
+        L.st[S_OVERFLOW]++;
+        L.deposit(t.event, t.vol, (double)t.E);
+      }
+    }
+  }
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+}
+
+// Post-step interaction of process PROC for the queued tracks of type PT: one
+// model per kernel, so a warp runs one sampling algorithm; survivor and
+// secondaries go to the next stores.
+template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_interact(const Args<R> *__restrict__ A)
+{
+  extern __shared__ double sm_edep[];
+  __shared__ unsigned long long sm_stat[kNStat];
+  __shared__ double sm_esc;
+  __shared__ int sm_err;
+  const Args<R> &a = *A;
+  const Data &d = *a.d;
+  Ctl *ctl = a.ctl;
+  const int par = ctl->parity;
+  const Store<R> &cur = a.st[par][PT];
+  const long long n = min(ctl->qcount[PT][PROC], a.qcap);
+  if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
+  const int *queue = a.queue[PT][PROC];
+  Local L;
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    long long j = base + threadIdx.x;
+    bool active = j < n;
+    Track<R> t;
+    Secs<R> sec;
+    sec.n = 0;
+    bool alive = false;
+    if (active) {
+      load_track(cur, (long long)queue[j], PT, t);
+      L.st[S_READ0 + PT]++;
+      run_model(d, a.g, t, PROC, sec, L);
+      alive = t.E > R(0);
+    }
+    int cnt[3] = {0, 0, 0};
+    if (alive) cnt[PT]++;
+    for (int k = 0; k < sec.n; ++k) cnt[sec.type[k]]++;
+    long long first[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) first[q] = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]);
+    if (active) {
+      long long next[3] = {first[0], first[1], first[2]};
+      for (int k = 0; k < sec.n; ++k) {
+        Track<R> c;
+        c.type = sec.type[k];
+        c.pos[0] = t.pos[0];
+        c.pos[1] = t.pos[1];
+        c.pos[2] = t.pos[2];
+        c.dir[0] = sec.dir[k][0];
+        c.dir[1] = sec.dir[k][1];
+        c.dir[2] = sec.dir[k][2];
+        c.E = sec.E[k];
+        c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
+        t.rng.seed_child(c.rng);
+        c.vol = t.vol;
+        c.event = t.event;
+        c.prim = -1;
+        put_track(a, c.type, next[c.type]++, c, L);
+        L.st[S_SEC0 + c.type]++;
+        L.st[S_WRITE0 + PT]++;
+      }
+      if (alive) {
+        put_track(a, PT, next[PT]++, t, L);
+        L.st[S_WRITE0 + PT]++;
+      }
+    }
+  }
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+}
+
 // End of an iteration: the next stores become current, the refill plan for
 // the following iteration is made.  One thread.
-__global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores, long long refill_below,
-                         long long stack_cap)
+__global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores)
 {
   int par = ctl->parity, np = par ^ 1;
   const long long cap[3] = {cap0, cap1, cap2};
+  const long long refill_below = ctl->refill_below, stack_cap = ctl->stack_cap;
+  for (int q = 0; q < 3; ++q)
+    for (int p = 0; p < 3; ++p) ctl->qcount[q][p] = 0;
   long long fl = 0;
   for (int q = 0; q < nstores; ++q) {
     // pushes past the end of a full stack were not written (and were counted as errors)
@@ -826,7 +1030,7 @@ __device__ __forceinline__ void jump_matvec(const uint64_t *A, uint64_t v[3], ui
 
 // Execute the refill plan: move deferred tracks back from the stacks, then
 // inject primaries (MRG32k3a substream first_substream + primary index).
-template <class R> __global__ void k_refill(Args<R> a)
+template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
 {
   Ctl *ctl = a.ctl;
   int par = ctl->parity;
@@ -888,6 +1092,9 @@ template <class R> __global__ void k_refill(Args<R> a)
   }
 }
 
+template <class R> __global__ void k_refill(Args<R> a) { refill_body(a); }
+template <class R> __global__ void k_refill_p(const Args<R> *__restrict__ A) { refill_body(*A); }
+
 // Bookkeeping after a refill: the primary cursor.  One thread.
 __global__ void k_refill_done(Ctl *ctl)
 {
@@ -915,6 +1122,7 @@ struct Engine {
   std::vector<char> graph_args; // launch arguments the graph was captured with
   double *cumE = nullptr;
   long long cumE_cap = 0;
+  void *dargs = nullptr; // device copy of the launch arguments (batched engine)
   cudaStream_t s1 = nullptr, s2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_j1 = nullptr, ev_j2 = nullptr;
 };
@@ -956,6 +1164,7 @@ void release_engine(Ctx *c)
   if (e->pool) cudaFree(e->pool);
   if (e->ctl) cudaFree(e->ctl);
   if (e->cumE) cudaFree(e->cumE);
+  if (e->dargs) cudaFree(e->dargs);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->s1) cudaStreamDestroy(e->s1);
   if (e->s2) cudaStreamDestroy(e->s2);
@@ -976,29 +1185,65 @@ template <class R> struct Launch {
 
 template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent)
 {
-  k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
-  k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
   if (L.a.nstores == 1) {
+    // plain loop: one fused step kernel over the mixed store
+    k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+    k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
     k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
-  } else if (!concurrent) {
-    k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
-    k_step<R, 1><<<L.grid, L.block, L.smem, s>>>(L.a);
-    k_step<R, 2><<<L.grid, L.block, L.smem, s>>>(L.a);
-  } else {
-    // the three particle types step concurrently: gamma on s, e- on s1, e+ on s2
+    k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
+    return;
+  }
+  const Args<R> *A = (const Args<R> *)e->dargs;
+  k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
+  k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
+  cudaStream_t sg = s, se = s, sp = s;
+  if (concurrent) {
+    // gamma on s, e- on s1, e+ on s2
     cudaEventRecord(e->ev_fork, s);
     cudaStreamWaitEvent(e->s1, e->ev_fork, 0);
     cudaStreamWaitEvent(e->s2, e->ev_fork, 0);
-    k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
-    k_step<R, 1><<<L.grid, L.block, L.smem, e->s1>>>(L.a);
-    k_step<R, 2><<<L.grid, L.block, L.smem, e->s2>>>(L.a);
+    se = e->s1;
+    sp = e->s2;
+  }
+  k_transport<R, 0><<<L.grid, L.block, L.smem, sg>>>(A);
+  k_interact<R, 0, 0><<<L.grid, L.block, L.smem, sg>>>(A);
+  k_interact<R, 0, 1><<<L.grid, L.block, L.smem, sg>>>(A);
+  k_interact<R, 0, 2><<<L.grid, L.block, L.smem, sg>>>(A);
+  k_transport<R, 1><<<L.grid, L.block, L.smem, se>>>(A);
+  k_interact<R, 1, 0><<<L.grid, L.block, L.smem, se>>>(A);
+  k_interact<R, 1, 1><<<L.grid, L.block, L.smem, se>>>(A);
+  k_transport<R, 2><<<L.grid, L.block, L.smem, sp>>>(A);
+  k_interact<R, 2, 0><<<L.grid, L.block, L.smem, sp>>>(A);
+  k_interact<R, 2, 1><<<L.grid, L.block, L.smem, sp>>>(A);
+  k_interact<R, 2, 2><<<L.grid, L.block, L.smem, sp>>>(A);
+  if (concurrent) {
     cudaEventRecord(e->ev_j1, e->s1);
     cudaEventRecord(e->ev_j2, e->s2);
     cudaStreamWaitEvent(s, e->ev_j1, 0);
     cudaStreamWaitEvent(s, e->ev_j2, 0);
   }
-  k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
-                           L.a.refill_below, L.a.stack[0].cap);
+  k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
+}
+
+// One particle type's step (transport + its interactions), for the profiling pass.
+template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q)
+{
+  const Args<R> *A = (const Args<R> *)e->dargs;
+  if (q == 0) {
+    k_transport<R, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 0, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 0, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 0, 2><<<L.grid, L.block, L.smem, s>>>(A);
+  } else if (q == 1) {
+    k_transport<R, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 1, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 1, 1><<<L.grid, L.block, L.smem, s>>>(A);
+  } else {
+    k_transport<R, 2><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 2, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 2, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    k_interact<R, 2, 2><<<L.grid, L.block, L.smem, s>>>(A);
+  }
 }
 
 template <class R>
@@ -1024,6 +1269,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     for (int b = 0; b < 2; ++b)
       for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, cap, !batched);
     for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, stack_cap, !batched);
+    if (batched) bytes += 9 * (((size_t)cap * sizeof(int) + 255) & ~size_t(255));
     err = cudaMalloc(&E->pool, bytes);
     if (err != cudaSuccess) {
       release_engine(C);
@@ -1052,6 +1298,14 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     L.a.st[0][q] = L.a.st[0][0];
     L.a.st[1][q] = L.a.st[1][0];
     L.a.stack[q] = L.a.stack[0];
+  }
+  if (batched) {
+    for (int q = 0; q < 3; ++q)
+      for (int pr = 0; pr < 3; ++pr) {
+        L.a.queue[q][pr] = (int *)(base + off);
+        off += ((size_t)cap * sizeof(int) + 255) & ~size_t(255);
+      }
+    L.a.qcap = cap;
   }
   if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
   L.a.d = C->dev;
@@ -1110,16 +1364,24 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   h.cumE = E->cumE;
   // a 10 GeV shower peaks near 800 tracks in flight: ~0.08 per MeV of primary energy
   h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
+  h.refill_below = L.a.refill_below;
+  h.stack_cap = stack_cap;
   err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return cuda_error(err, "transport control init");
   // first refill plan
-  k_finish<<<1, 1, 0, s>>>(E->ctl, cap, cap, cap, nstores, L.a.refill_below, stack_cap);
+  k_finish<<<1, 1, 0, s>>>(E->ctl, cap, cap, cap, nstores);
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, s);
   const long long max_iter = 2000000LL;
   long long iters = 0;
+  if (batched) {
+    if (!E->dargs && (err = cudaMalloc(&E->dargs, sizeof(Args<double>))) != cudaSuccess)
+      return cuda_error(err, "transport arguments");
+    if ((err = cudaMemcpyAsync(E->dargs, &L.a, sizeof(Args<R>), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return cuda_error(err, "transport arguments upload");
+  }
   double step_ms[3] = {0, 0, 0};
   long long step_launches[3] = {0, 0, 0};
   if (!batched || cfg->profile) {
@@ -1132,22 +1394,20 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
     for (;;) {
       if (cfg->profile) {
-        k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+        if (batched)
+          k_refill_p<R><<<L.grid, L.block, 0, s>>>((const Args<R> *)E->dargs);
+        else
+          k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
         k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
           if (!batched)
             k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
-          else if (q == 0)
-            k_step<R, 0><<<L.grid, L.block, L.smem, s>>>(L.a);
-          else if (q == 1)
-            k_step<R, 1><<<L.grid, L.block, L.smem, s>>>(L.a);
           else
-            k_step<R, 2><<<L.grid, L.block, L.smem, s>>>(L.a);
+            enqueue_type(L, E, s, q);
           cudaEventRecord(eb[q], s);
         }
-        k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
-                                 L.a.refill_below, L.a.stack[0].cap);
+        k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
       } else {
         enqueue_iteration(L, E, s, false);
       }
@@ -1170,11 +1430,13 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
   } else {
     int G = cfg->graph_iters > 0 ? cfg->graph_iters : 16;
-    // (re)capture the iteration graph when the launch arguments change
-    std::vector<char> key(sizeof(L.a) + 3 * sizeof(int));
-    std::memcpy(key.data(), &L.a, sizeof(L.a));
-    int extra[3] = {G, L.block, L.grid};
-    std::memcpy(key.data() + sizeof(L.a), extra, sizeof(extra));
+    // (re)capture the iteration graph when its launch shape changes; the
+    // arguments themselves are read from the device copy uploaded above
+    std::vector<char> key(4 * sizeof(int) + 2 * sizeof(void *));
+    int shape[4] = {G, L.block, L.grid, L.smem};
+    const void *ptrs[2] = {E->dargs, E->ctl};
+    std::memcpy(key.data(), shape, sizeof(shape));
+    std::memcpy(key.data() + sizeof(shape), ptrs, sizeof(ptrs));
     if (!E->graph || E->graph_args != key) {
       if (E->graph) {
         cudaGraphExecDestroy(E->graph);
@@ -1492,18 +1754,20 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   h.iterations = -1;
   h.cumE = cumE;
   h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
+  h.refill_below = L.a.refill_below;
+  h.stack_cap = cap;
   if ((err = cudaMemcpyAsync(ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
       (err = cudaStreamSynchronize(s)) != cudaSuccess)
     return cuda_error(err, "gx_transport_run_noalloc: control block");
   if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, cumE);
-  k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, L.a.refill_below, cap);
+  k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
   Ctl hc;
   long long iters = 0;
   for (;;) {
     k_refill<double><<<L.grid, L.block, 0, s>>>(L.a);
     k_refill_done<<<1, 1, 0, s>>>(ctl);
     k_step<double, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
-    k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, L.a.refill_below, cap);
+    k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
     if ((err = cudaGetLastError()) != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: launch");
     if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (err = cudaStreamSynchronize(s)) != cudaSuccess)

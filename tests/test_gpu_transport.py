@@ -59,18 +59,36 @@ def test_c1_gamma_box_matches_oracle_track_by_track(dm, oracle):
     assert np.isclose(st["escaped"], ref["escaped"], rtol=1e-5)
 
 
-@pytest.mark.parametrize("wl,n", [("c2", 16), ("c3", 8)])
-def test_showers_fp64_match_oracle(dm, oracle, wl, n):
+def test_showers_fp64_match_oracle_no_field(dm, oracle):
+    """Without a field the FP64 engine and the oracle follow the same tracks."""
     from geantexascalepilot_b200 import configs
-    cfg, prims, nvol = getattr(configs, wl)(*((n,) if wl == "c2" else (n, n)))
+    cfg, prims, nvol = configs.c2(16)
     edep, st, _ = run_gpu(dm, cfg, prims, nvol)
     ref = run_oracle(oracle, cfg, prims, nvol)
     assert st["errors"] == 0
-    # identical physics on identical streams; in the field a helix end point
-    # within an ulp of a plane can add a zero-length step on one side
-    assert abs(st["steps"] - ref["steps"]) <= (1e-3 if cfg.Bz else 1e-5) * ref["steps"]
+    assert abs(st["steps"] - ref["steps"]) <= 1e-5 * ref["steps"]
     assert abs(st["tracks"] - ref["tracks"]) <= 1e-4 * ref["tracks"]
     np.testing.assert_allclose(edep.ravel(), ref["edep"].ravel(), rtol=1e-6, atol=1e-6 * ref["edep"].max())
+
+
+def test_showers_fp64_match_oracle_in_field(dm, oracle):
+    """In 4 T the helix sub-step partition, and with it where a crossing is
+    detected, depends on rounding (the kernels contract to FMA, the oracle does
+    not), so a small fraction of tracks diverge: compare statistically, with
+    the per-layer deposits of 64 showers within 5 standard errors."""
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(32, 32)
+    edep, st, _ = run_gpu(dm, cfg, prims, nvol)
+    ref = run_oracle(oracle, cfg, prims, nvol)
+    assert st["errors"] == 0
+    assert abs(st["steps"] - ref["steps"]) <= 0.01 * ref["steps"]
+    assert abs(st["tracks"] - ref["tracks"]) <= 0.01 * ref["tracks"]
+    assert np.isclose(edep.sum(), ref["edep"].sum(), rtol=2e-3)
+    g = edep.reshape(-1, 2).sum(1)
+    o = ref["edep"].reshape(-1, 2).sum(1)
+    big = o > 0.002 * o.sum()
+    # per-layer spread of a 10 GeV shower deposit is of order 20%/sqrt(64 showers)
+    assert np.all(np.abs(g - o)[big] <= 5 * 0.2 / np.sqrt(64) * o[big] + 1e-3 * o.sum())
 
 
 def test_energy_conservation(dm):
