@@ -205,7 +205,8 @@ def main():
         for _ in range(steps):
             st = one(precision, engine)
             n_steps += st["steps"]
-            launches += 6 * st["iterations"] + 2
+            # per iteration: refill, refill_done, 3 transport, 8 interaction, finish; plain loop: 4
+            launches += (14 if engine == 1 else 4) * (st["iterations"] + 1) + 3
         ev1.record()
         barrier()
         ms = ev0.elapsed_time(ev1)
