@@ -271,14 +271,23 @@ template <class R> struct Inter {
   int status, nsec;
   int sec_type[2];
   R sec_E[2], sec_dir[2][3];
+  // slot chosen by a branch, not an index, so the record stays in registers
   __device__ __forceinline__ void add(int type, R e, R x, R y, R z)
   {
-    int k = nsec++;
-    sec_type[k] = type;
-    sec_E[k] = e;
-    sec_dir[k][0] = x;
-    sec_dir[k][1] = y;
-    sec_dir[k][2] = z;
+    if (nsec == 0) {
+      sec_type[0] = type;
+      sec_E[0] = e;
+      sec_dir[0][0] = x;
+      sec_dir[0][1] = y;
+      sec_dir[0][2] = z;
+    } else {
+      sec_type[1] = type;
+      sec_E[1] = e;
+      sec_dir[1][0] = x;
+      sec_dir[1][1] = y;
+      sec_dir[1][2] = z;
+    }
+    ++nsec;
   }
 };
 

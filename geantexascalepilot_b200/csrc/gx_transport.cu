@@ -86,6 +86,20 @@ template <class R> struct Args {
 };
 
 // ---------------------------------------------------------------- geometry
+// Component a (the run-time layer axis) of a 3-vector.  Selects instead of an
+// indexed access keep the vectors in registers: an array indexed by a run-time
+// value lives in local memory.
+template <class T> __device__ __forceinline__ T comp(const T *p, int a) { return a == 0 ? p[0] : (a == 1 ? p[1] : p[2]); }
+template <class T> __device__ __forceinline__ void set_comp(T *p, int a, T v)
+{
+  if (a == 0)
+    p[0] = v;
+  else if (a == 1)
+    p[1] = v;
+  else
+    p[2] = v;
+}
+
 // The layered calorimeter along axis a: layer k occupies [x0 + k pitch,
 // x0 + (k+1) pitch), absorber first.  vol = 2 layer + slab; -1 outside.
 __device__ __forceinline__ int vol_material(const Geom &g, int vol)
@@ -95,8 +109,9 @@ __device__ __forceinline__ int vol_material(const Geom &g, int vol)
 __device__ __forceinline__ void slab_bounds(const Geom &g, int vol, double &lo, double &hi)
 {
   if (g.geometry == 0) {
-    lo = g.box_centre[g.axis] - g.box_half[g.axis];
-    hi = g.box_centre[g.axis] + g.box_half[g.axis];
+    const double c = comp(g.box_centre, g.axis), h = comp(g.box_half, g.axis);
+    lo = c - h;
+    hi = c + h;
     return;
   }
   double base = g.x0 + (vol >> 1) * g.pitch;
@@ -106,31 +121,33 @@ __device__ __forceinline__ void slab_bounds(const Geom &g, int vol, double &lo, 
 __device__ __forceinline__ double thalf(const Geom &g, int b) { return g.geometry == 0 ? g.box_half[b] : g.half_trans; }
 __device__ __forceinline__ double tcentre(const Geom &g, int b) { return g.geometry == 0 ? g.box_centre[b] : 0.0; }
 
-__device__ int locate(const Geom &g, const double *p, const double *d)
+__device__ __forceinline__ int locate(const Geom &g, const double *p, const double *d)
 {
   const double tol = 1e-12;
   int a = g.axis;
+#pragma unroll
   for (int b = 0; b < 3; ++b) {
     if (b == a) continue;
     double h = thalf(g, b), q = p[b] - tcentre(g, b);
     if (q > h || q < -h) return -1;
     if ((q > h - tol && d[b] > 0) || (q < -h + tol && d[b] < 0)) return -1;
   }
+  const double pa = comp(p, a), da = comp(d, a);
   if (g.geometry == 0) {
-    double q = p[a] - g.box_centre[a], h = g.box_half[a];
+    double q = pa - comp(g.box_centre, a), h = comp(g.box_half, a);
     if (q > h || q < -h) return -1;
-    if ((q > h - tol && d[a] > 0) || (q < -h + tol && d[a] < 0)) return -1;
+    if ((q > h - tol && da > 0) || (q < -h + tol && da < 0)) return -1;
     return 0;
   }
-  double u = p[a] - g.x0;
+  double u = pa - g.x0;
   if (u < -tol || u > g.total + tol) return -1;
-  if ((u < tol && d[a] < 0) || (u > g.total - tol && d[a] > 0)) return -1;
+  if ((u < tol && da < 0) || (u > g.total - tol && da > 0)) return -1;
   int layer = (int)floor(u / g.pitch);
   layer = min(max(layer, 0), g.nlayers - 1);
   double q = u - layer * g.pitch;
-  if (q < tol && d[a] < 0 && layer > 0) return 2 * (layer - 1) + 1;
-  if (q > g.pitch - tol && d[a] > 0 && layer + 1 < g.nlayers) return 2 * (layer + 1);
-  if (fabs(q - g.t_abs) < tol) return 2 * layer + (d[a] > 0 ? 1 : 0);
+  if (q < tol && da < 0 && layer > 0) return 2 * (layer - 1) + 1;
+  if (q > g.pitch - tol && da > 0 && layer + 1 < g.nlayers) return 2 * (layer + 1);
+  if (fabs(q - g.t_abs) < tol) return 2 * layer + (da > 0 ? 1 : 0);
   return 2 * layer + (q < g.t_abs ? 0 : 1);
 }
 
@@ -140,13 +157,15 @@ __device__ __forceinline__ double dist_to_out(const Geom &g, int vol, const doub
   double lo, hi, dist = 1.7976931348623157e308;
   slab_bounds(g, vol, lo, hi);
   plane = 0;
-  if (d[a] > 0) {
-    dist = (hi - p[a]) / d[a];
+  const double pa = comp(p, a), da = comp(d, a);
+  if (da > 0) {
+    dist = (hi - pa) / da;
     plane = 1;
-  } else if (d[a] < 0) {
-    dist = (lo - p[a]) / d[a];
+  } else if (da < 0) {
+    dist = (lo - pa) / da;
     plane = -1;
   }
+#pragma unroll
   for (int b = 0; b < 3; ++b) {
     if (b == a) continue;
     double h = thalf(g, b), q = p[b] - tcentre(g, b), t = 1.7976931348623157e308;
@@ -167,7 +186,9 @@ __device__ __forceinline__ double safety(const Geom &g, int vol, const double *p
   int a = g.axis;
   double lo, hi;
   slab_bounds(g, vol, lo, hi);
-  double s = fmin(p[a] - lo, hi - p[a]);
+  const double pa = comp(p, a);
+  double s = fmin(pa - lo, hi - pa);
+#pragma unroll
   for (int b = 0; b < 3; ++b) {
     if (b == a) continue;
     s = fmin(s, thalf(g, b) - fabs(p[b] - tcentre(g, b)));
@@ -194,17 +215,19 @@ __device__ __forceinline__ int relocate(const Geom &g, int vol, double *p, const
   int a = g.axis;
   double lo, hi;
   slab_bounds(g, vol, lo, hi);
+#pragma unroll
   for (int b = 0; b < 3; ++b) {
     if (b == a) continue;
     double h = thalf(g, b), q = p[b] - tcentre(g, b);
     if ((d[b] > 0 && h - q < kSnap) || (d[b] < 0 && q + h < kSnap)) return -1;
   }
-  if (d[a] > 0 && hi - p[a] < kSnap) {
-    p[a] = hi;
+  const double pa = comp(p, a), da = comp(d, a);
+  if (da > 0 && hi - pa < kSnap) {
+    set_comp(p, a, hi);
     return next_volume(g, vol, 1);
   }
-  if (d[a] < 0 && p[a] - lo < kSnap) {
-    p[a] = lo;
+  if (da < 0 && pa - lo < kSnap) {
+    set_comp(p, a, lo);
     return next_volume(g, vol, -1);
   }
   return locate(g, p, d);
@@ -316,6 +339,24 @@ template <class R> struct Secs {
   int n;
   int type[2];
   R E[2], dir[2][3];
+  // slot chosen by a branch, not an index, so the record stays in registers
+  __device__ __forceinline__ void add(int ty, R e, const R *u)
+  {
+    if (n == 0) {
+      type[0] = ty;
+      E[0] = e;
+      dir[0][0] = u[0];
+      dir[0][1] = u[1];
+      dir[0][2] = u[2];
+    } else {
+      type[1] = ty;
+      E[1] = e;
+      dir[1][0] = u[0];
+      dir[1][1] = u[1];
+      dir[1][2] = u[2];
+    }
+    ++n;
+  }
 };
 
 // Helix sub-steps in Bz (FieldPropagationHandler::Propagate / PropagateInVolume,
@@ -437,17 +478,14 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
   t.dir[0] = io.dir[0];
   t.dir[1] = io.dir[1];
   t.dir[2] = io.dir[2];
-  for (int s = 0; s < io.nsec; ++s) {
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    if (s >= io.nsec) break;
     if (g.charged_local && io.sec_type[s] != 0) {
       L.deposit(t.event, t.vol, (double)io.sec_E[s]);
       continue;
     }
-    int k = sec.n++;
-    sec.type[k] = io.sec_type[s];
-    sec.E[k] = io.sec_E[s];
-    sec.dir[k][0] = io.sec_dir[s][0];
-    sec.dir[k][1] = io.sec_dir[s][1];
-    sec.dir[k][2] = io.sec_dir[s][2];
+    sec.add(io.sec_type[s], io.sec_E[s], io.sec_dir[s]);
   }
   if (io.status == 1) t.E = R(0);
 }
@@ -467,12 +505,16 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
   bool charged = t.type != 0;
   R xs[3];
   cross_sections<R>(d, t.type, mat, t.E, xs);
-  for (int i = 0; i < np; ++i)
-    if (t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(t.rng.template u<R>());
+  // loops over the three process slots are unrolled with the bound as a guard,
+  // so xs[] and nil[] are indexed by constants and stay in registers
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (i < np && t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(t.rng.template u<R>());
   R pstep = R(3.0e38);
   int sel = -1;
-  for (int i = 0; i < np; ++i)
-    if (xs[i] > R(0)) {
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (i < np && xs[i] > R(0)) {
       R s = t.nil[i] / xs[i];
       if (s < pstep) {
         pstep = s;
@@ -502,7 +544,7 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
       if (plane != 2) {
         double lo, hi;
         slab_bounds(g, t.vol, lo, hi);
-        t.pos[g.axis] = plane > 0 ? hi : lo;
+        set_comp(t.pos, g.axis, plane > 0 ? hi : lo);
       }
     } else {
       step = ps;
@@ -511,7 +553,9 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
   } else {
     step = field_propagate(g, t, (double)pstep, crossed, newvol, L);
   }
-  for (int i = 0; i < np; ++i) t.nil[i] -= (R)step * xs[i];
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (i < np) t.nil[i] -= (R)step * xs[i];
   L.st[S_STEPS]++;
   if (newvol == -2) {
     L.deposit(t.event, vol0, (double)t.E);
@@ -543,7 +587,9 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
     return kAlive;
   }
   if (sel >= 0) {
-    t.nil[sel] = R(-1);
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      if (i == sel) t.nil[i] = R(-1);
     *proc = sel;
     return kInteract;
   }
@@ -644,125 +690,7 @@ template <class R> __device__ __forceinline__ void put_track(const Args<R> &a, i
 }
 
 // ----------------------------------------------------------------- kernels
-// PT: particle type of the store (0, 1, 2), or 3 for the single mixed store.
-template <class R, int PT> __global__ void __launch_bounds__(256) k_step(Args<R> a)
-{
-  extern __shared__ double sm_edep[];
-  __shared__ unsigned long long sm_stat[kNStat];
-  __shared__ double sm_esc;
-  __shared__ int sm_err;
-  const Data &d = *a.d;
-  Ctl *ctl = a.ctl;
-  const int par = ctl->parity;
-  const int store_id = (PT < 3) ? PT : 0;
-  const long long n = min(ctl->count[par][store_id], a.st[par][store_id].cap);
-  Local L;
-  L.nvol = a.g.nvol;
-  L.nevents = a.g.nevents;
-  L.g_edep = a.edep;
-  L.sm_edep = sm_edep;
-  L.sm_bins = 0;
-  {
-    int bins = 0;
-    // shared-memory tally if the whole table fits in 6 KB
-    long long all = (long long)a.g.nvol * 1; // event rows other than 0 go to global memory
-    if (all <= 768) bins = (int)all;
-    L.sm_bins = bins;
-    for (int k = threadIdx.x; k < bins; k += blockDim.x) sm_edep[k] = 0.0;
-  }
-  if (threadIdx.x < kNStat) sm_stat[threadIdx.x] = 0;
-  if (threadIdx.x == 0) {
-    sm_esc = 0.0;
-    sm_err = 0;
-  }
-  __syncthreads();
-  L.escaped = 0.0;
-  L.err = 0;
-#pragma unroll
-  for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
-
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
-    long long i = base + threadIdx.x;
-    bool active = i < n;
-    Track<R> t;
-    Secs<R> sec;
-    sec.n = 0;
-    bool alive = false;
-    if (active) {
-      load_track(a.st[par][store_id], i, PT, t);
-      L.st[S_READ0 + store_id]++;
-      alive = one_step(d, a.g, t, sec, L);
-      if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
-    }
-    // slots per destination store
-    int cnt[3] = {0, 0, 0};
-    int dst_surv = (a.nstores == 1) ? 0 : (active ? t.type : 0);
-    if (alive) cnt[dst_surv]++;
-    for (int k = 0; k < sec.n; ++k) cnt[(a.nstores == 1) ? 0 : sec.type[k]]++;
-    long long first[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      if (q < a.nstores)
-        first[q] = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]);
-      else
-        first[q] = 0;
-    }
-    if (active) {
-      long long next[3] = {first[0], first[1], first[2]};
-      // secondaries first take their streams from the parent, in order
-      for (int k = 0; k < sec.n; ++k) {
-        Track<R> c;
-        c.type = sec.type[k];
-        c.pos[0] = t.pos[0];
-        c.pos[1] = t.pos[1];
-        c.pos[2] = t.pos[2];
-        c.dir[0] = sec.dir[k][0];
-        c.dir[1] = sec.dir[k][1];
-        c.dir[2] = sec.dir[k][2];
-        c.E = sec.E[k];
-        c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
-        t.rng.seed_child(c.rng);
-        c.vol = t.vol;
-        c.event = t.event;
-        c.prim = -1;
-        int q = (a.nstores == 1) ? 0 : c.type;
-        put_track(a, q, next[q]++, c, L);
-        L.st[S_SEC0 + c.type]++;
-        L.st[S_WRITE0 + store_id]++;
-      }
-      if (alive) {
-        put_track(a, dst_surv, next[dst_surv]++, t, L);
-        L.st[S_WRITE0 + store_id]++;
-      }
-    }
-  }
-  // flush block-local tallies
-  L.st[S_TRACKS] = 0;
-#pragma unroll
-  for (int k = 0; k < kNStat; ++k)
-    if (L.st[k]) atomicAdd(&sm_stat[k], (unsigned long long)L.st[k]);
-  if (L.escaped != 0.0) atomicAdd(&sm_esc, L.escaped);
-  if (L.err) atomicOr(&sm_err, L.err);
-  __syncthreads();
-  for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x)
-    if (sm_edep[k] != 0.0) atomicAdd(&a.edep[k], sm_edep[k]);
-  if (threadIdx.x < kNStat && sm_stat[threadIdx.x]) atomicAdd(&ctl->stat[threadIdx.x], sm_stat[threadIdx.x]);
-  if (threadIdx.x == 0) {
-    if (sm_esc != 0.0) atomicAdd(&ctl->escaped, sm_esc);
-    if (sm_err) atomicOr(&ctl->err_flags, sm_err);
-  }
-}
-
-// ------------------------------------------------- batched engine: split step
 // Shared-memory tally and block statistics of one step kernel.
-struct BlockTally {
-  double *sm_edep;
-  unsigned long long *sm_stat;
-  double *sm_esc;
-  int *sm_err;
-};
-
 __device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *edep, double *sm_edep,
                                             unsigned long long *sm_stat, double *sm_esc, int *sm_err)
 {
@@ -770,6 +698,7 @@ __device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *ede
   L.nevents = g.nevents;
   L.g_edep = edep;
   L.sm_edep = sm_edep;
+  // event row 0 of the tally lives in shared memory when it fits in 6 KB
   L.sm_bins = (g.nvol <= 768) ? g.nvol : 0;
   for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x) sm_edep[k] = 0.0;
   if (threadIdx.x < kNStat) sm_stat[threadIdx.x] = 0;
@@ -802,6 +731,115 @@ __device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, doub
   }
 }
 
+// Element q of a 3-array by unrolled compare, so the array stays in registers.
+template <class T> __device__ __forceinline__ T take3(T (&v)[3], int q, T inc)
+{
+  T r = 0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j)
+    if (j == q) {
+      r = v[j];
+      v[j] += inc;
+    }
+  return r;
+}
+
+// After a track's interaction: its secondaries (streams seeded from the
+// parent, in order) and the survivor go to the next stores, destination =
+// particle type, or store 0 with one mixed store.  Every lane of the warp
+// calls this (the slot reservations are warp-wide); `active` lanes write.
+// SRC is the store the tracks were read from (for the write statistics).
+template <class R, int SRC>
+__device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par, bool active, bool alive, Track<R> &t,
+                                            const Secs<R> &sec, Local &L)
+{
+  const bool mixed = a.nstores == 1;
+  int cnt[3] = {0, 0, 0};
+  if (alive) take3(cnt, mixed ? 0 : t.type, 1);
+#pragma unroll
+  for (int k = 0; k < 2; ++k)
+    if (k < sec.n) take3(cnt, mixed ? 0 : sec.type[k], 1);
+  long long next[3];
+#pragma unroll
+  for (int q = 0; q < 3; ++q)
+    next[q] = (q < a.nstores) ? warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]) : 0;
+  if (!active) return;
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    if (k >= sec.n) break;
+    Track<R> c;
+    c.type = sec.type[k];
+    c.pos[0] = t.pos[0];
+    c.pos[1] = t.pos[1];
+    c.pos[2] = t.pos[2];
+    c.dir[0] = sec.dir[k][0];
+    c.dir[1] = sec.dir[k][1];
+    c.dir[2] = sec.dir[k][2];
+    c.E = sec.E[k];
+    c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
+    t.rng.seed_child(c.rng);
+    c.vol = t.vol;
+    c.event = t.event;
+    c.prim = -1;
+    const int q = mixed ? 0 : c.type;
+    put_track(a, q, take3(next, q, 1LL), c, L);
+    unsigned int sc[3] = {L.st[S_SEC0], L.st[S_SEC1], L.st[S_SEC2]};
+    take3(sc, c.type, 1u);
+    L.st[S_SEC0] = sc[0];
+    L.st[S_SEC1] = sc[1];
+    L.st[S_SEC2] = sc[2];
+    L.st[S_WRITE0 + SRC]++;
+  }
+  if (alive) {
+    const int q = mixed ? 0 : t.type;
+    put_track(a, q, take3(next, q, 1LL), t, L);
+    L.st[S_WRITE0 + SRC]++;
+  }
+}
+
+// PT: particle type of the store (0, 1, 2), or 3 for the single mixed store.
+// The fused step (transport and interaction in one kernel) of the plain loop.
+template <class R, int PT> __device__ __forceinline__ void step_body(const Args<R> &a)
+{
+  extern __shared__ double sm_edep[];
+  __shared__ unsigned long long sm_stat[kNStat];
+  __shared__ double sm_esc;
+  __shared__ int sm_err;
+  const Data &d = *a.d;
+  Ctl *ctl = a.ctl;
+  const int par = ctl->parity;
+  constexpr int SRC = (PT < 3) ? PT : 0;
+  const Store<R> &cur = a.st[par][SRC];
+  const long long n = min(ctl->count[par][SRC], cur.cap);
+  Local L;
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
+    long long i = base + threadIdx.x;
+    bool active = i < n;
+    Track<R> t;
+    Secs<R> sec;
+    sec.n = 0;
+    bool alive = false;
+    if (active) {
+      load_track(cur, i, PT, t);
+      L.st[S_READ0 + SRC]++;
+      alive = one_step(d, a.g, t, sec, L);
+      if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
+    }
+    emit_tracks<R, SRC>(a, ctl, par, active, alive, t, sec, L);
+  }
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+}
+
+// Arguments by value (the allocation-free entry point) or from a device copy.
+template <class R, int PT> __global__ void __launch_bounds__(256) k_step(Args<R> a) { step_body<R, PT>(a); }
+template <class R, int PT> __global__ void __launch_bounds__(256) k_step_p(const Args<R> *__restrict__ A)
+{
+  step_body<R, PT>(*A);
+}
+
+// ------------------------------------------------- batched engine: split step
 // Transport part of the step for every track of type PT: survivors without an
 // interaction go to the next store; a track that interacts is written back in
 // place and its slot index is queued for the interaction kernel of its
@@ -834,14 +872,12 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
     long long slot = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][PT], r == kAlive ? 1 : 0);
-    long long qslot[3];
+    long long q = 0;
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
-      if (PT == 1 && p == 2) {
-        qslot[p] = 0;
-        continue;
-      }
-      qslot[p] = warp_reserve((unsigned long long *)&ctl->qcount[PT][p], (r == kInteract && proc == p) ? 1 : 0);
+      if (PT == 1 && p == 2) continue; // e- has two processes
+      long long v = warp_reserve((unsigned long long *)&ctl->qcount[PT][p], (r == kInteract && proc == p) ? 1 : 0);
+      if (p == proc) q = v;
     }
     if (r == kAlive) {
       put_track(a, PT, slot, t, L);
@@ -849,7 +885,6 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
     } else if (r == kInteract) {
       store_track(cur, i, t);
       L.st[S_WRITE0 + PT]++;
-      long long q = qslot[proc];
       if (q < a.qcap) {
         a.queue[PT][proc][q] = (int)i;
       } else {
@@ -895,38 +930,7 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_in
       run_model(d, a.g, t, PROC, sec, L);
       alive = t.E > R(0);
     }
-    int cnt[3] = {0, 0, 0};
-    if (alive) cnt[PT]++;
-    for (int k = 0; k < sec.n; ++k) cnt[sec.type[k]]++;
-    long long first[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) first[q] = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]);
-    if (active) {
-      long long next[3] = {first[0], first[1], first[2]};
-      for (int k = 0; k < sec.n; ++k) {
-        Track<R> c;
-        c.type = sec.type[k];
-        c.pos[0] = t.pos[0];
-        c.pos[1] = t.pos[1];
-        c.pos[2] = t.pos[2];
-        c.dir[0] = sec.dir[k][0];
-        c.dir[1] = sec.dir[k][1];
-        c.dir[2] = sec.dir[k][2];
-        c.E = sec.E[k];
-        c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
-        t.rng.seed_child(c.rng);
-        c.vol = t.vol;
-        c.event = t.event;
-        c.prim = -1;
-        put_track(a, c.type, next[c.type]++, c, L);
-        L.st[S_SEC0 + c.type]++;
-        L.st[S_WRITE0 + PT]++;
-      }
-      if (alive) {
-        put_track(a, PT, next[PT]++, t, L);
-        L.st[S_WRITE0 + PT]++;
-      }
-    }
+    emit_tracks<R, PT>(a, ctl, par, active, alive, t, sec, L);
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
 }
@@ -1185,15 +1189,15 @@ template <class R> struct Launch {
 
 template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent)
 {
+  const Args<R> *A = (const Args<R> *)e->dargs;
   if (L.a.nstores == 1) {
     // plain loop: one fused step kernel over the mixed store
-    k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+    k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
     k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
-    k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+    k_step_p<R, 3><<<L.grid, L.block, L.smem, s>>>(A);
     k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
     return;
   }
-  const Args<R> *A = (const Args<R> *)e->dargs;
   k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
   k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
   cudaStream_t sg = s, se = s, sp = s;
@@ -1376,12 +1380,12 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   cudaEventRecord(t0, s);
   const long long max_iter = 2000000LL;
   long long iters = 0;
-  if (batched) {
-    if (!E->dargs && (err = cudaMalloc(&E->dargs, sizeof(Args<double>))) != cudaSuccess)
-      return cuda_error(err, "transport arguments");
-    if ((err = cudaMemcpyAsync(E->dargs, &L.a, sizeof(Args<R>), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return cuda_error(err, "transport arguments upload");
-  }
+  // the kernels read their arguments from a device copy (indexing a kernel
+  // parameter by a run-time value would copy the whole block to local memory)
+  if (!E->dargs && (err = cudaMalloc(&E->dargs, sizeof(Args<double>))) != cudaSuccess)
+    return cuda_error(err, "transport arguments");
+  if ((err = cudaMemcpyAsync(E->dargs, &L.a, sizeof(Args<R>), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+    return cuda_error(err, "transport arguments upload");
   double step_ms[3] = {0, 0, 0};
   long long step_launches[3] = {0, 0, 0};
   if (!batched || cfg->profile) {
@@ -1394,15 +1398,12 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
     for (;;) {
       if (cfg->profile) {
-        if (batched)
-          k_refill_p<R><<<L.grid, L.block, 0, s>>>((const Args<R> *)E->dargs);
-        else
-          k_refill<R><<<L.grid, L.block, 0, s>>>(L.a);
+        k_refill_p<R><<<L.grid, L.block, 0, s>>>((const Args<R> *)E->dargs);
         k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
           if (!batched)
-            k_step<R, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+            k_step_p<R, 3><<<L.grid, L.block, L.smem, s>>>((const Args<R> *)E->dargs);
           else
             enqueue_type(L, E, s, q);
           cudaEventRecord(eb[q], s);
