@@ -34,6 +34,7 @@ sys.path.insert(0, REPO)
 
 METRIC = "track-steps/s on 1 B200: FP32-mixed vs FP64 GPU, ≤0.5% per-layer Edep diff"
 UNIT = "track-steps/s"
+LAUNCH_KEYS = ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy")
 
 
 def parse():
@@ -46,6 +47,8 @@ def parse():
     p.add_argument("--photons", type=int, default=10000)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
+    p.add_argument("--autotune", action="store_true",
+                   help="sweep the launch settings on the workload first (untimed) and time the winner")
     return p.parse_args()
 
 
@@ -116,7 +119,7 @@ def cpu_baseline(cfg_fn, seconds, nthreads):
     """Time the oracle's step loop on a bounded sample of the workload."""
     sys.path.insert(0, os.path.join(REPO, "tests"))
     from oracle_ctypes import Oracle
-    from test_gpu_transport import oracle_config
+    from oracle_ctypes import oracle_config
     if not os.path.exists(os.path.join(REPO, "oracle", "liboracle.so")):
         subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle")])
     orc = Oracle()
@@ -183,11 +186,20 @@ def main():
            "p": torch.as_tensor(pos, device="cuda"), "d": torch.as_tensor(d, device="cuda")}
     edep = torch.zeros((1, nvol), dtype=torch.float64, device="cuda")
 
-    def one(precision, engine, profile=0):
+    def one(precision, engine, profile=0, primary_steps=False):
         cfg.precision, cfg.engine, cfg.profile = precision, engine, profile
         edep.zero_()
-        _, st, _ = gx.transport(dm, cfg, dev["t"], dev["E"], dev["p"], dev["d"], nvol=nvol, edep=edep)
-        return st
+        keep = [getattr(cfg, k) for k in LAUNCH_KEYS]
+        if engine == 0:  # the plain loop runs with its own defaults
+            for k in LAUNCH_KEYS:
+                setattr(cfg, k, 0)
+        try:
+            _, st, ps = gx.transport(dm, cfg, dev["t"], dev["E"], dev["p"], dev["d"], nvol=nvol, edep=edep,
+                                     primary_steps=primary_steps)
+        finally:
+            for k, v in zip(LAUNCH_KEYS, keep):
+                setattr(cfg, k, v)
+        return (st, ps.cpu().numpy()) if primary_steps else st
 
     def barrier():
         torch.cuda.synchronize()
@@ -219,6 +231,14 @@ def main():
             n_steps = int(c.item())
         return ms, n_steps, launches, st
 
+    tuned = None
+    if args.autotune:
+        cfg.precision, cfg.engine, cfg.profile = 1, 1, 0
+        trials = gx.autotune(dm, cfg, dev["t"], dev["E"], dev["p"], dev["d"], nvol=nvol, repeats=2)
+        tuned = {"best": trials[0], "trials": len(trials),
+                 "default": next((t for t in trials if t["block_size"] == 128 and t["blocks_per_sm"] == 4
+                                  and t["graph_iters"] == 16 and t["wave_energy"] == 0), None)}
+
     # headline: FP32-mixed, batched engine, primaries resident in HBM
     with ClockSampler(local) as clk:
         ms, n_steps, launches, st32 = timed(1, 1, args.steps, args.warmup)
@@ -234,7 +254,11 @@ def main():
                       "1 GPU", "l2": "track stores of several GB per step exceed L2 (no flush needed)"},
            "clocks": clk.summary(), "gpu_launches": launches,
            "track_steps_per_step": n_steps // max(1, args.steps), "primaries_per_s": world * nprim * args.steps / (ms / 1e3),
-           "stats": {k: st32[k] for k in ("steps", "substeps", "tracks", "iterations", "peak_in_flight", "errors")}}
+           "stats": {k: st32[k] for k in ("steps", "substeps", "tracks", "iterations", "peak_in_flight", "errors")},
+           "launch": {"block": cfg.block_size or 128, "blocks_per_sm": cfg.blocks_per_sm or 4,
+                      "graph_iters": cfg.graph_iters or 16}}
+    if tuned:
+        out["autotune"] = tuned
 
     # FP64 comparisons on the same streams
     if not args.no_fp64:
@@ -254,6 +278,13 @@ def main():
         out["layer_edep_rel_diff_fp32_vs_fp64"] = {"max": float(rel.max()), "mean": float(rel.mean()),
                                                    "total": float(abs(lay32.sum() - lay64.sum()) / lay64.sum()),
                                                    "layers_compared": int(big.sum())}
+        # step-count distributions of the primaries, FP32-mixed vs FP64 (untimed runs)
+        from scipy.stats import ks_2samp
+        _, p32 = one(1, 1, primary_steps=True)
+        _, p64 = one(0, 1, primary_steps=True)
+        ks = ks_2samp(p32, p64)
+        out["primary_step_count_ks_fp32_vs_fp64"] = {"statistic": float(ks.statistic), "pvalue": float(ks.pvalue),
+                                                     "mean_fp32": float(p32.mean()), "mean_fp64": float(p64.mean())}
 
     # e2e through the host-buffer entry point
     cfg.precision, cfg.engine, cfg.profile = 1, 1, 0
@@ -269,25 +300,35 @@ def main():
     out["e2e"] = {"value": world * e2e_steps / dt, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                   "d2h_bytes_per_step": int(nvol * 8)}
 
-    # roofline of the dominant step kernel (profiling pass, CUDA events per launch)
+    # roofline of the dominant kernel: the transport kernel of the particle type
+    # that takes the most device time (profiling pass, CUDA events around each
+    # launch on the launching stream)
     stp = one(1, 1, profile=1)
-    k = int(np.argmax(stp["step_ms"]))
-    nbytes = (stp["tracks_read"][k] + stp["tracks_written"][k]) * stp["bytes_per_track"]
-    achieved = nbytes / (stp["step_ms"][k] / 1e3) / 1e9
+    k = int(np.argmax(stp["transport_ms"]))
+    launches_k = max(1, stp["step_launches"][k])
+    nbytes = (stp["transport_read"][k] + stp["transport_written"][k]) * stp["bytes_per_track"]
+    achieved = nbytes / (stp["transport_ms"][k] / 1e3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
     except (OSError, ValueError):
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
+    traffic = None
+    tr = os.path.join(REPO, "profiles", "transport_kernel_dram.json")
+    if os.path.exists(tr):
+        # DRAM bytes per track record processed, from one ncu capture of this
+        # kernel on a smaller case, scaled to this run's records per launch
+        per = json.load(open(tr)).get("dram_bytes_per_record", {}).get(str(k))
+        if per:
+            traffic = per * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": None, "kernel": ["gamma step: k_transport<float,0> + k_interact<float,0,*>",
-                                  "e- step: k_transport<float,1> + k_interact<float,1,*>",
-                                  "e+ step: k_transport<float,2> + k_interact<float,2,*>"][k],
+                       "traffic": traffic, "kernel": "k_transport<float,%d> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
-                       "algorithmic_bytes_per_launch": nbytes / max(1, stp["step_launches"][k]),
-                       "avg_launch_ms": stp["step_ms"][k] / max(1, stp["step_launches"][k]),
-                       "share_of_step_kernel_time": stp["step_ms"][k] / max(1e-9, sum(stp["step_ms"]))}
+                       "algorithmic_bytes_per_launch": nbytes / launches_k,
+                       "avg_launch_ms": stp["transport_ms"][k] / launches_k,
+                       "share_of_step_kernel_time": stp["transport_ms"][k] / max(1e-9, sum(stp["step_ms"])),
+                       "records_per_launch": (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k}
 
     if rank == 0:
         v, n, dtc = cpu_baseline(c3_sample(args.electrons, args.photons), args.cpu_seconds, os.cpu_count() or 1)

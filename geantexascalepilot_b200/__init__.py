@@ -10,6 +10,6 @@ from .api import (ANNIHILATION, BETHE_HEITLER, BHABHA, ELECTRON, GAMMA, KLEIN_NI
                   MODE_QUIRK, MOLLER, POSITRON, SAUTER_GAVRILA, SELTZER_BERGER, TABLES, ConstFieldHelixStepper,
                   MRG32k3a, ProxyAnnihilation, ProxyBetheHeitler, ProxyBhabhaScattering, ProxyBremsstrahlung,
                   ProxyCompton, ProxyConversion, ProxyDataManager, ProxyIonization, ProxyKleinNishina,
-                  ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, default_config,
-                  transport, transport_host, transport_noalloc)
-from . import configs  # noqa: F401
+                  ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, autotune,
+                  default_config, transport, transport_host, transport_noalloc)
+from . import configs, sharding  # noqa: F401

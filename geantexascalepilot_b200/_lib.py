@@ -49,7 +49,8 @@ class TransportStats(C.Structure):
     _fields_ = [("steps", LL), ("substeps", LL), ("tracks", LL), ("secondaries", LL * 3), ("n_pair", LL),
                 ("n_annih", LL), ("errors", LL), ("escaped", D), ("iterations", LL), ("peak_in_flight", LL),
                 ("kernel_ms", D), ("step_ms", D * 3), ("step_launches", LL * 3), ("tracks_read", LL * 3),
-                ("tracks_written", LL * 3), ("bytes_per_track", LL)]
+                ("tracks_written", LL * 3), ("bytes_per_track", LL), ("transport_ms", D * 3),
+                ("transport_read", LL * 3), ("transport_written", LL * 3), ("transport_queued", LL * 3)]
 
     def as_dict(self):
         return {"steps": self.steps, "substeps": self.substeps, "tracks": self.tracks,
@@ -59,7 +60,24 @@ class TransportStats(C.Structure):
                 "peak_in_flight": self.peak_in_flight, "kernel_ms": self.kernel_ms,
                 "step_ms": list(self.step_ms), "step_launches": list(self.step_launches),
                 "tracks_read": list(self.tracks_read), "tracks_written": list(self.tracks_written),
-                "bytes_per_track": self.bytes_per_track}
+                "bytes_per_track": self.bytes_per_track, "transport_ms": list(self.transport_ms),
+                "transport_read": list(self.transport_read), "transport_written": list(self.transport_written),
+                "transport_queued": list(self.transport_queued)}
+
+
+AUTOTUNE_MAX_TRIALS = 64
+
+
+class AutotuneReport(C.Structure):
+    _fields_ = [("trials", I), ("best", I), ("block_size", I * AUTOTUNE_MAX_TRIALS),
+                ("blocks_per_sm", I * AUTOTUNE_MAX_TRIALS), ("graph_iters", I * AUTOTUNE_MAX_TRIALS),
+                ("refill_below", LL * AUTOTUNE_MAX_TRIALS), ("wave_energy", D * AUTOTUNE_MAX_TRIALS),
+                ("kernel_ms", D * AUTOTUNE_MAX_TRIALS), ("steps_per_ms", D * AUTOTUNE_MAX_TRIALS)]
+
+    def as_list(self):
+        keys = ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy", "kernel_ms",
+                "steps_per_ms")
+        return [{k: getattr(self, k)[i] for k in keys} for i in range(self.trials)]
 
 
 _SIGS = {
@@ -85,6 +103,8 @@ _SIGS = {
     "gx_transport_run": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P, C.POINTER(TransportStats), P]),
     "gx_transport_run_host": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P,
                                   C.POINTER(TransportStats)]),
+    "gx_transport_autotune": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, I, I, C.POINTER(AutotuneReport),
+                                  P]),
     "gx_transport_run_noalloc": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I,
                                      C.POINTER(TransportStats), P]),
 }

@@ -12,7 +12,7 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import GxError, ModelParams, TransportConfig, TransportStats, check, lib
+from ._lib import AutotuneReport, GxError, ModelParams, TransportConfig, TransportStats, check, lib
 
 # physics-table ids (ProxyPhysicsTableIndex.hpp:23-45)
 TABLES = ["DEDX.eBrem.e-", "DEDX.eBrem.e+", "DEDX.eIoni.e-", "DEDX.eIoni.e+", "InverseRange.eIoni.e-",
@@ -292,6 +292,24 @@ def transport(dm, cfg, types, E, pos, direction, events=None, nvol=None, primary
     check(lib.gx_transport_run(dm.handle, C.byref(cfg), n, _ptr(t), _ptr(E), _ptr(p), _ptr(d), _ptr(ev), _ptr(edep),
                                nvol, _ptr(ps), C.byref(st), _stream()))
     return edep, st.as_dict(), ps
+
+
+def autotune(dm, cfg, types, E, pos, direction, events=None, nvol=None, repeats=2):
+    """gx_transport_autotune: sweep the batched engine's launch settings on
+    these primaries (the workload, or a representative subset), write the
+    fastest into cfg and return the list of trials (best first)."""
+    t = _dev(types, torch.int32)
+    E = _dev(E, torch.float64)
+    p = _dev(pos, torch.float64).reshape(-1, 3)
+    d = _dev(direction, torch.float64).reshape(-1, 3)
+    ev = _dev(events, torch.int32) if events is not None else None
+    if nvol is None:
+        nvol = 2 * cfg.nlayers if cfg.geometry == 1 else 1
+    rep = AutotuneReport()
+    check(lib.gx_transport_autotune(dm.handle, C.byref(cfg), t.numel(), _ptr(t), _ptr(E), _ptr(p), _ptr(d), _ptr(ev),
+                                    nvol, repeats, C.byref(rep), _stream()))
+    trials = rep.as_list()
+    return [trials[rep.best]] + [x for i, x in enumerate(trials) if i != rep.best]
 
 
 def transport_host(dm, cfg, types, E, pos, direction, events=None, nvol=None):

@@ -1,0 +1,139 @@
+// gx_autotune.cu -- launch-setting sweep for the batched transport engine.
+//
+// The step kernels are register-heavy (110-130 registers per thread), so the
+// useful block sizes are 64-256 threads (a 512- or 1024-thread block would
+// need at most 128 or 64 registers per thread and spill); the grid is a
+// multiple of the SM count.  The sweep is coordinate descent: block size x
+// resident blocks per SM first, then the number of iterations per CUDA-graph
+// launch, then the refill threshold, then the primary energy per injection
+// wave.  Each candidate transports the caller's primaries completely; its
+// score is track-steps per millisecond of device time, the best of `repeats`
+// runs (the first run of a new launch shape also captures its graph).
+#include "gx_internal.cuh"
+
+#include <cstring>
+#include <vector>
+
+namespace {
+
+struct Trial {
+  int block, bpsm, graph_iters;
+  long long refill_below;
+  double wave_energy;
+};
+
+} // namespace
+
+extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, const int *d_type,
+                                     const double *d_E, const double *d_pos, const double *d_dir,
+                                     const int *d_event, int nvol, int repeats, gx_autotune_report *rep,
+                                     gx_stream_t stream)
+{
+  using namespace gx;
+  if (!ctx || !cfg || nprim <= 0 || !d_type || !d_E || !d_pos || !d_dir || nvol <= 0 || cfg->nevents < 1)
+    return set_error(GX_ERR_ARG, "gx_transport_autotune: bad arguments");
+  if (cfg->engine != 1) return set_error(GX_ERR_ARG, "gx_transport_autotune: tunes the batched engine (engine 1)");
+  if (repeats < 1) repeats = 2;
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  cudaError_t e = cudaSetDevice(C->device);
+  if (e != cudaSuccess) return cuda_error(e, "gx_transport_autotune: cudaSetDevice");
+  cudaStream_t s = stream_of(stream);
+  const size_t nt = (size_t)cfg->nevents * nvol;
+  double *edep = nullptr;
+  if ((e = cudaMalloc((void **)&edep, nt * sizeof(double))) != cudaSuccess)
+    return cuda_error(e, "gx_transport_autotune: tally scratch");
+
+  gx_transport_config base = *cfg;
+  base.profile = 0;
+  const long long cap = base.capacity > 0 ? base.capacity : (1LL << 24);
+  if (rep) std::memset(rep, 0, sizeof(*rep));
+  int ntrials = 0, rc = GX_OK;
+  double best_rate = -1.0;
+  Trial best = {base.block_size > 0 ? base.block_size : default_block(1),
+                base.blocks_per_sm > 0 ? base.blocks_per_sm : kDefaultBlocksPerSM,
+                base.graph_iters > 0 ? base.graph_iters : 16,
+                base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy};
+
+  auto measure = [&](const Trial &t) -> double {
+    gx_transport_config c = base;
+    c.block_size = t.block;
+    c.blocks_per_sm = t.bpsm;
+    c.graph_iters = t.graph_iters;
+    c.refill_below = t.refill_below;
+    c.wave_energy = t.wave_energy;
+    double best_ms = 0.0, rate = 0.0;
+    for (int r = 0; r < repeats; ++r) {
+      cudaMemsetAsync(edep, 0, nt * sizeof(double), s);
+      gx_transport_stats st;
+      int k = gx_transport_run(ctx, &c, nprim, d_type, d_E, d_pos, d_dir, d_event, edep, nvol, nullptr, &st,
+                               stream);
+      if (k == GX_ERR_CUDA) {
+        rc = k; // the device is in trouble: stop the sweep
+        return -1.0;
+      }
+      if (k != GX_OK || st.kernel_ms <= 0.0) return 0.0; // e.g. overflow with this setting: not a candidate
+      if (r == 0 || st.kernel_ms < best_ms) best_ms = st.kernel_ms;
+      rate = (double)st.steps / best_ms;
+    }
+    if (rep && ntrials < GX_AUTOTUNE_MAX_TRIALS) {
+      rep->block_size[ntrials] = t.block;
+      rep->blocks_per_sm[ntrials] = t.bpsm;
+      rep->graph_iters[ntrials] = t.graph_iters;
+      rep->refill_below[ntrials] = t.refill_below;
+      rep->wave_energy[ntrials] = t.wave_energy;
+      rep->kernel_ms[ntrials] = best_ms;
+      rep->steps_per_ms[ntrials] = rate;
+    }
+    ++ntrials;
+    return rate;
+  };
+  auto consider = [&](const Trial &t) {
+    if (rc) return;
+    double r = measure(t);
+    if (r > best_rate) {
+      best_rate = r;
+      best = t;
+      if (rep) rep->best = ntrials - 1;
+    }
+  };
+
+  const int blocks[] = {64, 128, 256};
+  const int bpsms[] = {1, 2, 4, 8};
+  for (int b : blocks)
+    for (int p : bpsms) {
+      Trial t = best;
+      t.block = b;
+      t.bpsm = p;
+      consider(t);
+    }
+  const Trial after_shape = best;
+  for (int g : {4, 8, 32, 64}) {
+    Trial t = after_shape;
+    t.graph_iters = g;
+    consider(t);
+  }
+  const Trial after_graph = best;
+  for (long long r : {cap / 8, cap / 4, (3 * cap) / 4}) {
+    Trial t = after_graph;
+    t.refill_below = r;
+    consider(t);
+  }
+  const Trial after_refill = best;
+  // multiples of the engine's default widen or narrow the injection waves
+  const double wave0 = default_wave_energy(cap, 0.8);
+  for (double m : {0.25, 0.5, 2.0}) {
+    Trial t = after_refill;
+    t.wave_energy = m * wave0;
+    consider(t);
+  }
+  cudaFree(edep);
+  if (rep) rep->trials = ntrials < GX_AUTOTUNE_MAX_TRIALS ? ntrials : GX_AUTOTUNE_MAX_TRIALS;
+  if (rc) return rc;
+  if (best_rate <= 0.0) return set_error(GX_ERR_OVERFLOW, "gx_transport_autotune: no setting completed the sample");
+  cfg->block_size = best.block;
+  cfg->blocks_per_sm = best.bpsm;
+  cfg->graph_iters = best.graph_iters;
+  cfg->refill_below = best.refill_below;
+  cfg->wave_energy = best.wave_energy;
+  return GX_OK;
+}

@@ -28,4 +28,16 @@ void release_engine(Ctx *c);
 
 inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Launch defaults of the transport engines (the sweep of gx_transport_autotune
+// found 128-thread blocks fastest for the batched engine on C3; the plain loop
+// keeps 256).
+inline int default_block(int engine) { return engine == 1 ? 128 : 256; }
+constexpr int kDefaultBlocksPerSM = 4;
+// Primary energy per injection wave for stores of cap slots: a 10 GeV shower
+// peaks near 800 tracks in flight, ~0.08 per MeV of primary energy; waves are
+// sized so that their showers would peak at `fill` x cap if they all peaked
+// together (they do not: waves overlap as showers age).  The batched engine
+// uses fill 0.8 (fastest in the sweep on C3), the plain loop 0.4.
+inline double default_wave_energy(long long cap, double fill) { return fill * (double)cap / 0.08; }
+
 } // namespace gx

@@ -41,9 +41,13 @@ struct Geom {
   double box_half[3], box_centre[3];
 };
 
-constexpr int kNStat = 16;
+constexpr int kNStat = 25;
+// S_READ/S_WRITE: track records read and written by all step kernels of a
+// type; S_TREAD/S_TWRITE: by its transport kernel alone; S_TQUEUE: of those
+// writes, the records put in an interaction buffer.
 enum { S_STEPS, S_SUBSTEPS, S_TRACKS, S_SEC0, S_SEC1, S_SEC2, S_PAIR, S_ANNIH, S_ERR, S_OVERFLOW,
-       S_READ0, S_READ1, S_READ2, S_WRITE0, S_WRITE1, S_WRITE2 };
+       S_READ0, S_READ1, S_READ2, S_WRITE0, S_WRITE1, S_WRITE2, S_TREAD0, S_TREAD1, S_TREAD2,
+       S_TWRITE0, S_TWRITE1, S_TWRITE2, S_TQUEUE0, S_TQUEUE1, S_TQUEUE2 };
 
 struct Ctl {
   int parity;
@@ -59,7 +63,7 @@ struct Ctl {
   const double *cumE; // inclusive prefix sum of the primary energies
   double wave_energy; // primary energy injected per wave, at most
   long long refill_below, stack_cap;
-  long long qcount[3][3]; // interaction queues [particle][process]
+  long long qcount[3][3]; // records in the interaction buffers [particle][process]
 };
 
 struct Prims {
@@ -81,7 +85,9 @@ template <class R> struct Args {
   int *pstep;
   int nstores;
   long long refill_below;
-  int *queue[3][3]; // slot indices of tracks waiting for an interaction (batched engine)
+  // tracks waiting for an interaction, per particle type and process, stored
+  // compactly so the interaction kernels read them coalesced (batched engine)
+  Store<R> ibuf[3][3];
   long long qcap;
 };
 
@@ -701,7 +707,7 @@ __device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *ede
   // event row 0 of the tally lives in shared memory when it fits in 6 KB
   L.sm_bins = (g.nvol <= 768) ? g.nvol : 0;
   for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x) sm_edep[k] = 0.0;
-  if (threadIdx.x < kNStat) sm_stat[threadIdx.x] = 0;
+  for (int k = threadIdx.x; k < kNStat; k += blockDim.x) sm_stat[k] = 0;
   if (threadIdx.x == 0) {
     *sm_esc = 0.0;
     *sm_err = 0;
@@ -724,7 +730,8 @@ __device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, doub
   __syncthreads();
   for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x)
     if (sm_edep[k] != 0.0) atomicAdd(&edep[k], sm_edep[k]);
-  if (threadIdx.x < kNStat && sm_stat[threadIdx.x]) atomicAdd(&ctl->stat[threadIdx.x], sm_stat[threadIdx.x]);
+  for (int k = threadIdx.x; k < kNStat; k += blockDim.x)
+    if (sm_stat[k]) atomicAdd(&ctl->stat[k], sm_stat[k]);
   if (threadIdx.x == 0) {
     if (*sm_esc != 0.0) atomicAdd(&ctl->escaped, *sm_esc);
     if (*sm_err) atomicOr(&ctl->err_flags, *sm_err);
@@ -833,17 +840,19 @@ template <class R, int PT> __device__ __forceinline__ void step_body(const Args<
 }
 
 // Arguments by value (the allocation-free entry point) or from a device copy.
-template <class R, int PT> __global__ void __launch_bounds__(256) k_step(Args<R> a) { step_body<R, PT>(a); }
-template <class R, int PT> __global__ void __launch_bounds__(256) k_step_p(const Args<R> *__restrict__ A)
+// Two resident blocks per SM: the fused step needs ~190 registers per thread
+// unconstrained, which would leave one 256-thread block (8 warps) per SM.
+template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step(Args<R> a) { step_body<R, PT>(a); }
+template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step_p(const Args<R> *__restrict__ A)
 {
   step_body<R, PT>(*A);
 }
 
 // ------------------------------------------------- batched engine: split step
 // Transport part of the step for every track of type PT: survivors without an
-// interaction go to the next store; a track that interacts is written back in
-// place and its slot index is queued for the interaction kernel of its
-// process (warp prefix sums, one atomic per warp and destination).
+// interaction go to the next store, a track that interacts goes to the
+// interaction buffer of its process (slots from warp prefix sums, one atomic
+// per warp and destination, so both writes are contiguous).
 template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
@@ -868,6 +877,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
     if (active) {
       load_track(cur, i, PT, t);
       L.st[S_READ0 + PT]++;
+      L.st[S_TREAD0 + PT]++;
       r = transport_part(d, a.g, t, L, &proc);
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
@@ -882,11 +892,13 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
     if (r == kAlive) {
       put_track(a, PT, slot, t, L);
       L.st[S_WRITE0 + PT]++;
+      L.st[S_TWRITE0 + PT]++;
     } else if (r == kInteract) {
-      store_track(cur, i, t);
-      L.st[S_WRITE0 + PT]++;
       if (q < a.qcap) {
-        a.queue[PT][proc][q] = (int)i;
+        store_track(a.ibuf[PT][proc], q, t);
+        L.st[S_WRITE0 + PT]++;
+        L.st[S_TWRITE0 + PT]++;
+        L.st[S_TQUEUE0 + PT]++;
       } else {
         L.err |= kErrOverflow;
         L.st[S_OVERFLOW]++;
@@ -897,8 +909,8 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
 }
 
-// Post-step interaction of process PROC for the queued tracks of type PT: one
-// model per kernel, so a warp runs one sampling algorithm; survivor and
+// Post-step interaction of process PROC for the buffered tracks of type PT:
+// one model per kernel, so a warp runs one sampling algorithm; survivor and
 // secondaries go to the next stores.
 template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_interact(const Args<R> *__restrict__ A)
 {
@@ -910,10 +922,9 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_in
   const Data &d = *a.d;
   Ctl *ctl = a.ctl;
   const int par = ctl->parity;
-  const Store<R> &cur = a.st[par][PT];
+  const Store<R> &buf = a.ibuf[PT][PROC];
   const long long n = min(ctl->qcount[PT][PROC], a.qcap);
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
-  const int *queue = a.queue[PT][PROC];
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -925,7 +936,7 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_in
     sec.n = 0;
     bool alive = false;
     if (active) {
-      load_track(cur, (long long)queue[j], PT, t);
+      load_track(buf, j, PT, t);
       L.st[S_READ0 + PT]++;
       run_model(d, a.g, t, PROC, sec, L);
       alive = t.E > R(0);
@@ -1229,21 +1240,25 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
   k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
 }
 
-// One particle type's step (transport + its interactions), for the profiling pass.
-template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q)
+// One particle type's step (transport + its interactions), for the profiling
+// pass; `mid` is recorded between the transport kernel and the interactions.
+template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q, cudaEvent_t mid)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
   if (q == 0) {
     k_transport<R, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    cudaEventRecord(mid, s);
     k_interact<R, 0, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 1><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 2><<<L.grid, L.block, L.smem, s>>>(A);
   } else if (q == 1) {
     k_transport<R, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    cudaEventRecord(mid, s);
     k_interact<R, 1, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 1, 1><<<L.grid, L.block, L.smem, s>>>(A);
   } else {
     k_transport<R, 2><<<L.grid, L.block, L.smem, s>>>(A);
+    cudaEventRecord(mid, s);
     k_interact<R, 2, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 2, 1><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 2, 2><<<L.grid, L.block, L.smem, s>>>(A);
@@ -1273,7 +1288,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     for (int b = 0; b < 2; ++b)
       for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, cap, !batched);
     for (int q = 0; q < nstores; ++q) carve<R>(0, bytes, stack_cap, !batched);
-    if (batched) bytes += 9 * (((size_t)cap * sizeof(int) + 255) & ~size_t(255));
+    if (batched) // interaction buffers: gamma 3 processes, e- 2, e+ 3
+      for (int k = 0; k < 8; ++k) carve<R>(0, bytes, cap, false);
     err = cudaMalloc(&E->pool, bytes);
     if (err != cudaSuccess) {
       release_engine(C);
@@ -1305,10 +1321,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   }
   if (batched) {
     for (int q = 0; q < 3; ++q)
-      for (int pr = 0; pr < 3; ++pr) {
-        L.a.queue[q][pr] = (int *)(base + off);
-        off += ((size_t)cap * sizeof(int) + 255) & ~size_t(255);
-      }
+      for (int pr = 0; pr < 3; ++pr)
+        if (q != 1 || pr != 2) L.a.ibuf[q][pr] = carve<R>(base, off, cap, false);
     L.a.qcap = cap;
   }
   if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
@@ -1347,8 +1361,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.a.pstep = d_pstep;
   L.a.nstores = nstores;
   L.a.refill_below = cfg->refill_below > 0 ? std::min(cfg->refill_below, cap) : cap / 2;
-  L.block = cfg->block_size > 0 ? cfg->block_size : 256;
-  int bpsm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : 4;
+  L.block = cfg->block_size > 0 ? cfg->block_size : default_block(cfg->engine);
+  int bpsm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : kDefaultBlocksPerSM;
   L.grid = C->num_sms * bpsm;
   L.smem = 768 * sizeof(double);
 
@@ -1366,8 +1380,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   h.nprim = nprim;
   h.iterations = -1; // the planning launch below is not an iteration
   h.cumE = E->cumE;
-  // a 10 GeV shower peaks near 800 tracks in flight: ~0.08 per MeV of primary energy
-  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, batched ? 0.8 : 0.4);
   h.refill_below = L.a.refill_below;
   h.stack_cap = stack_cap;
   err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
@@ -1386,14 +1399,15 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     return cuda_error(err, "transport arguments");
   if ((err = cudaMemcpyAsync(E->dargs, &L.a, sizeof(Args<R>), cudaMemcpyHostToDevice, s)) != cudaSuccess)
     return cuda_error(err, "transport arguments upload");
-  double step_ms[3] = {0, 0, 0};
+  double step_ms[3] = {0, 0, 0}, transport_ms[3] = {0, 0, 0};
   long long step_launches[3] = {0, 0, 0};
   if (!batched || cfg->profile) {
     // plain loop (and the profiling pass): launch, synchronise, look at the
     // counters, every iteration
-    cudaEvent_t ea[3], eb[3];
+    cudaEvent_t ea[3], em[3], eb[3];
     for (int q = 0; q < 3; ++q) {
       cudaEventCreate(&ea[q]);
+      cudaEventCreate(&em[q]);
       cudaEventCreate(&eb[q]);
     }
     for (;;) {
@@ -1402,10 +1416,12 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
-          if (!batched)
+          if (!batched) {
             k_step_p<R, 3><<<L.grid, L.block, L.smem, s>>>((const Args<R> *)E->dargs);
-          else
-            enqueue_type(L, E, s, q);
+            cudaEventRecord(em[q], s);
+          } else {
+            enqueue_type(L, E, s, q, em[q]);
+          }
           cudaEventRecord(eb[q], s);
         }
         k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
@@ -1416,9 +1432,11 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport iteration");
       if (cfg->profile)
         for (int q = 0; q < nstores; ++q) {
-          float t = 0;
+          float t = 0, tt = 0;
           cudaEventElapsedTime(&t, ea[q], eb[q]);
+          cudaEventElapsedTime(&tt, ea[q], em[q]);
           step_ms[q] += t;
+          transport_ms[q] += tt;
           step_launches[q]++;
         }
       ++iters;
@@ -1427,6 +1445,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
     for (int q = 0; q < 3; ++q) {
       cudaEventDestroy(ea[q]);
+      cudaEventDestroy(em[q]);
       cudaEventDestroy(eb[q]);
     }
   } else {
@@ -1492,6 +1511,10 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       stats->step_launches[q] = step_launches[q];
       stats->tracks_read[q] = (long long)c.stat[S_READ0 + q];
       stats->tracks_written[q] = (long long)c.stat[S_WRITE0 + q];
+      stats->transport_ms[q] = transport_ms[q];
+      stats->transport_read[q] = (long long)c.stat[S_TREAD0 + q];
+      stats->transport_written[q] = (long long)c.stat[S_TWRITE0 + q];
+      stats->transport_queued[q] = (long long)c.stat[S_TQUEUE0 + q];
     }
     stats->bytes_per_track = (long long)(3 * sizeof(double) + 7 * sizeof(R) + 6 * sizeof(uint32_t) +
                                          3 * sizeof(int) + (batched ? 0 : sizeof(int)));

@@ -1,0 +1,64 @@
+"""Command-line transport of one benchmark workload on one GPU.
+
+    python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --precision 1
+    python -m geantexascalepilot_b200.run c5 --nevents 64 --mean 100 --profile
+    python -m geantexascalepilot_b200.run c4 --n 4096 --autotune
+
+Prints one JSON line: the workload, the transport statistics (steps,
+propagation sub-steps, tracks, secondaries, iterations, per-kernel device
+times in profile mode) and the device time of the transport loop.
+"""
+import argparse
+import json
+import sys
+
+
+def main(argv=None):
+    p = argparse.ArgumentParser(prog="python -m geantexascalepilot_b200.run")
+    p.add_argument("workload", choices=["c1", "c2", "c3", "c4", "c5"])
+    p.add_argument("--n", type=int, default=None, help="primaries (c1, c2, c4)")
+    p.add_argument("--electrons", type=int, default=10000, help="c3")
+    p.add_argument("--photons", type=int, default=10000, help="c3")
+    p.add_argument("--nevents", type=int, default=4096, help="c5")
+    p.add_argument("--mean", type=float, default=100.0, help="c5: mean primaries per event")
+    p.add_argument("--precision", type=int, default=1, choices=[0, 1], help="0 FP64, 1 FP32-mixed")
+    p.add_argument("--engine", type=int, default=1, choices=[0, 1], help="0 plain loop, 1 batched")
+    p.add_argument("--profile", action="store_true", help="time each step kernel with CUDA events (no graph)")
+    p.add_argument("--autotune", action="store_true", help="sweep the launch settings first")
+    p.add_argument("--repeat", type=int, default=1, help="transport the workload this many times")
+    p.add_argument("--device", type=int, default=0)
+    a = p.parse_args(argv)
+
+    import torch
+
+    import geantexascalepilot_b200 as gx
+    from geantexascalepilot_b200 import configs
+
+    torch.cuda.set_device(a.device)
+    if a.workload == "c3":
+        cfg, prims, nvol = configs.c3(a.electrons, a.photons)
+    elif a.workload == "c5":
+        cfg, prims, nvol = configs.c5(a.nevents, a.mean)
+    else:
+        fn = getattr(configs, a.workload)
+        cfg, prims, nvol = fn(a.n) if a.n is not None else fn()
+    cfg.precision, cfg.engine, cfg.profile = a.precision, a.engine, int(a.profile)
+    dm = gx.ProxyDataManager(device=a.device)
+    out = {"workload": a.workload, "primaries": int(len(prims[0])), "precision": a.precision, "engine": a.engine}
+    if a.autotune:
+        cfg.profile = 0
+        out["autotune"] = gx.autotune(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)[0]
+        cfg.profile = int(a.profile)
+    for _ in range(a.repeat):
+        edep, st, _ = gx.transport(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)
+    torch.cuda.synchronize()
+    out["stats"] = st
+    out["edep_total"] = float(edep.sum().item())
+    out["track_steps_per_s"] = st["steps"] / (st["kernel_ms"] / 1e3) if st["kernel_ms"] > 0 else None
+    print(json.dumps(out), flush=True)
+    dm.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -185,6 +185,11 @@ typedef struct {
   long long tracks_read[3];    /* track records read */
   long long tracks_written[3]; /* track records written (survivors and secondaries) */
   long long bytes_per_track;   /* size of one track record in the stores */
+  /* the transport kernel of each type alone (batched engine; times in profile mode only): */
+  double transport_ms[3];
+  long long transport_read[3];    /* track records read */
+  long long transport_written[3]; /* records written: survivors and interacting tracks */
+  long long transport_queued[3];  /* of those, records written to the interaction buffers */
 } gx_transport_stats;
 
 void gx_transport_config_default(gx_transport_config *cfg);
@@ -203,6 +208,33 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
 int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *h_type,
                           const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
                           double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats);
+
+/* Launch-setting sweep of the batched engine.  No counterpart in the
+ * reference (its kernels take nblocks / nthreads from the caller,
+ * source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).  Transports the given
+ * primaries (the whole batch, or a representative subset of it) once per
+ * candidate: block size {64, 128, 256} x resident blocks per SM {1, 2, 4, 8},
+ * then iterations per CUDA-graph launch {4, 8, 32, 64}, then the refill
+ * threshold {1/8, 1/4, 3/4 of the capacity}, then the primary energy per
+ * injection wave {1/4, 1/2, 2 x the default}, each coordinate from the best so
+ * far.  Score: track-steps per millisecond of device time, best of `repeats`
+ * runs (at least 1; the first run of a new launch shape includes its graph
+ * capture).  Writes the winner into cfg->block_size, blocks_per_sm,
+ * graph_iters, refill_below and wave_energy; report (optional) lists every
+ * trial.  cfg->engine must be 1; the precision and capacity are kept. */
+#define GX_AUTOTUNE_MAX_TRIALS 64
+typedef struct {
+  int trials, best; /* number of trials listed; index of the winner */
+  int block_size[GX_AUTOTUNE_MAX_TRIALS], blocks_per_sm[GX_AUTOTUNE_MAX_TRIALS];
+  int graph_iters[GX_AUTOTUNE_MAX_TRIALS];
+  long long refill_below[GX_AUTOTUNE_MAX_TRIALS];
+  double wave_energy[GX_AUTOTUNE_MAX_TRIALS];
+  double kernel_ms[GX_AUTOTUNE_MAX_TRIALS];    /* device time, best of the repeats (0: did not complete) */
+  double steps_per_ms[GX_AUTOTUNE_MAX_TRIALS]; /* track-steps per device millisecond */
+} gx_autotune_report;
+int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
+                          const double *d_pos, const double *d_dir, const int *d_event, int nvol, int repeats,
+                          gx_autotune_report *report, gx_stream_t s);
 
 /* gx_transport_run without any device allocation.  No counterpart in the
  * reference.  For callers that must not allocate device memory while they

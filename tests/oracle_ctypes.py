@@ -212,6 +212,21 @@ class Oracle:
         return res
 
 
+def oracle_config(cfg, nthreads=8):
+    """The oracle's transport configuration for a package TransportConfig."""
+    c = Config()
+    for f in ("geometry", "axis", "nlayers", "t_abs", "t_gap", "half_trans", "box_mat", "Bz", "charged_local",
+              "first_substream"):
+        setattr(c, f, getattr(cfg, f))
+    c.box_half[:] = list(cfg.box_half)
+    c.box_centre[:] = list(cfg.box_centre)
+    c.seed[:] = list(cfg.seed)
+    c.max_steps = 10 ** 8
+    c.nthreads = nthreads
+    c.score_events = cfg.nevents
+    return c
+
+
 class Reference:
     """The reference's own code (oracle/_ref/libgxref.so)."""
 

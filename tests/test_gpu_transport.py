@@ -4,6 +4,7 @@ FP64, energy conservation, and the host-buffer entry point."""
 import numpy as np
 import pytest
 import torch
+from oracle_ctypes import oracle_config
 
 pytestmark = pytest.mark.gpu
 
@@ -12,21 +13,6 @@ pytestmark = pytest.mark.gpu
 def dm():
     import geantexascalepilot_b200 as g
     return g.ProxyDataManager()
-
-
-def oracle_config(cfg, nthreads=8):
-    from oracle_ctypes import Config
-    c = Config()
-    for f in ("geometry", "axis", "nlayers", "t_abs", "t_gap", "half_trans", "box_mat", "Bz", "charged_local",
-              "first_substream"):
-        setattr(c, f, getattr(cfg, f))
-    c.box_half[:] = list(cfg.box_half)
-    c.box_centre[:] = list(cfg.box_centre)
-    c.seed[:] = list(cfg.seed)
-    c.max_steps = 10 ** 8
-    c.nthreads = nthreads
-    c.score_events = cfg.nevents
-    return c
 
 
 def run_gpu(dm, cfg, prims, nvol, precision=0, engine=1, primary_steps=False, **kw):
@@ -150,6 +136,60 @@ def test_per_event_tallies_match_oracle(dm, oracle):
     ref = run_oracle(oracle, cfg, prims, nvol)
     assert edep.shape == (12, nvol)
     np.testing.assert_allclose(edep.sum(1), ref["edep"].sum(1), rtol=1e-6)
+
+
+def test_shards_on_global_substreams_sum_to_the_whole(dm):
+    """Three contiguous shards run one after another (as three GPUs would run
+    them), each on the substreams of its global primary indices: the summed
+    tallies and counters equal one run over all primaries."""
+    from geantexascalepilot_b200 import configs, sharding
+    cfg, prims, nvol = configs.c3(6, 6)
+    whole, sw, _ = run_gpu(dm, cfg, prims, nvol)
+    tot = np.zeros_like(whole)
+    steps = tracks = 0
+    for r in range(3):
+        sub, first = sharding.shard(prims, r, 3)
+        cfg.first_substream = first
+        e, st, _ = run_gpu(dm, cfg, sub, nvol)
+        tot += e
+        steps += st["steps"]
+        tracks += st["tracks"]
+    cfg.first_substream = 0
+    assert steps == sw["steps"] and tracks == sw["tracks"]
+    np.testing.assert_allclose(tot, whole, rtol=1e-9, atol=1e-9 * whole.max())
+
+
+def test_autotune_and_launch_settings_leave_results_unchanged(dm):
+    """The sweep returns its trials and writes the winner into the config; any
+    launch setting transports the same tracks (per-primary substreams)."""
+    import geantexascalepilot_b200 as g
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(6, 6)
+    e0, s0, ps0 = run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True)
+    trials = g.autotune(dm, cfg, *prims[:4], nvol=nvol, repeats=1)
+    assert len(trials) >= 20
+    best = trials[0]
+    assert best["steps_per_ms"] == max(t["steps_per_ms"] for t in trials) > 0
+    assert (cfg.block_size, cfg.blocks_per_sm, cfg.graph_iters) == (best["block_size"], best["blocks_per_sm"],
+                                                                     best["graph_iters"])
+    assert cfg.block_size in (64, 128, 256) and cfg.blocks_per_sm in (1, 2, 4, 8)
+    e1, s1, ps1 = run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True)
+    assert s1["steps"] == s0["steps"] and s1["tracks"] == s0["tracks"]
+    assert np.array_equal(ps0, ps1)
+    np.testing.assert_allclose(e1, e0, rtol=1e-5, atol=1e-6 * e0.max())
+    for k in ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy"):
+        setattr(cfg, k, 0)
+
+
+def test_step_count_distributions_fp32_vs_fp64(dm):
+    """Two-sample Kolmogorov-Smirnov test on the primaries' step counts,
+    FP32-mixed against FP64 on the same streams."""
+    from scipy.stats import ks_2samp
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(100, 100)
+    _, _, p64 = run_gpu(dm, cfg, prims, nvol, precision=0, primary_steps=True)
+    _, _, p32 = run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True)
+    assert ks_2samp(p32, p64).pvalue > 0.01
 
 
 def test_small_capacity_uses_the_overflow_stack(dm):
