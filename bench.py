@@ -34,7 +34,7 @@ sys.path.insert(0, REPO)
 
 METRIC = "track-steps/s on 1 B200: FP32-mixed vs FP64 GPU, ≤0.5% per-layer Edep diff"
 UNIT = "track-steps/s"
-LAUNCH_KEYS = ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy")
+LAUNCH_KEYS = ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy")
 
 
 def parse():
@@ -237,7 +237,8 @@ def main():
         trials = gx.autotune(dm, cfg, dev["t"], dev["E"], dev["p"], dev["d"], nvol=nvol, repeats=2)
         tuned = {"best": trials[0], "trials": len(trials),
                  "default": next((t for t in trials if t["block_size"] == 128 and t["blocks_per_sm"] == 4
-                                  and t["graph_iters"] == 16 and t["wave_energy"] == 0), None)}
+                                  and t["steps_per_launch"] == 16 and t["graph_iters"] == 16
+                                  and t["wave_energy"] == 0), None)}
 
     # headline: FP32-mixed, batched engine, primaries resident in HBM
     with ClockSampler(local) as clk:
@@ -256,6 +257,7 @@ def main():
            "track_steps_per_step": n_steps // max(1, args.steps), "primaries_per_s": world * nprim * args.steps / (ms / 1e3),
            "stats": {k: st32[k] for k in ("steps", "substeps", "tracks", "iterations", "peak_in_flight", "errors")},
            "launch": {"block": cfg.block_size or 128, "blocks_per_sm": cfg.blocks_per_sm or 4,
+                      "steps_per_launch": cfg.steps_per_launch or 16,
                       "graph_iters": cfg.graph_iters or 16}}
     if tuned:
         out["autotune"] = tuned

@@ -42,7 +42,7 @@ class TransportConfig(C.Structure):
                 ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I), ("Bz", D), ("charged_local", I),
                 ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
-                ("graph_iters", I), ("profile", I), ("wave_energy", D)]
+                ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I)]
 
 
 class TransportStats(C.Structure):
@@ -70,13 +70,14 @@ AUTOTUNE_MAX_TRIALS = 64
 
 class AutotuneReport(C.Structure):
     _fields_ = [("trials", I), ("best", I), ("block_size", I * AUTOTUNE_MAX_TRIALS),
-                ("blocks_per_sm", I * AUTOTUNE_MAX_TRIALS), ("graph_iters", I * AUTOTUNE_MAX_TRIALS),
+                ("blocks_per_sm", I * AUTOTUNE_MAX_TRIALS), ("steps_per_launch", I * AUTOTUNE_MAX_TRIALS),
+                ("graph_iters", I * AUTOTUNE_MAX_TRIALS),
                 ("refill_below", LL * AUTOTUNE_MAX_TRIALS), ("wave_energy", D * AUTOTUNE_MAX_TRIALS),
                 ("kernel_ms", D * AUTOTUNE_MAX_TRIALS), ("steps_per_ms", D * AUTOTUNE_MAX_TRIALS)]
 
     def as_list(self):
-        keys = ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy", "kernel_ms",
-                "steps_per_ms")
+        keys = ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy",
+                "kernel_ms", "steps_per_ms")
         return [{k: getattr(self, k)[i] for k in keys} for i in range(self.trials)]
 
 

@@ -4,9 +4,9 @@
 // useful block sizes are 64-256 threads (a 512- or 1024-thread block would
 // need at most 128 or 64 registers per thread and spill); the grid is a
 // multiple of the SM count.  The sweep is coordinate descent: block size x
-// resident blocks per SM first, then the number of iterations per CUDA-graph
-// launch, then the refill threshold, then the primary energy per injection
-// wave.  Each candidate transports the caller's primaries completely; its
+// resident blocks per SM first, then the steps a track may take per transport
+// launch, then the number of iterations per CUDA-graph launch, then the refill
+// threshold, then the primary energy per injection wave.  Each candidate transports the caller's primaries completely; its
 // score is track-steps per millisecond of device time, the best of `repeats`
 // runs (the first run of a new launch shape also captures its graph).
 #include "gx_internal.cuh"
@@ -17,7 +17,7 @@
 namespace {
 
 struct Trial {
-  int block, bpsm, graph_iters;
+  int block, bpsm, steps, graph_iters;
   long long refill_below;
   double wave_energy;
 };
@@ -51,6 +51,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   double best_rate = -1.0;
   Trial best = {base.block_size > 0 ? base.block_size : default_block(1),
                 base.blocks_per_sm > 0 ? base.blocks_per_sm : kDefaultBlocksPerSM,
+                base.steps_per_launch > 0 ? base.steps_per_launch : kDefaultStepsPerLaunch,
                 base.graph_iters > 0 ? base.graph_iters : 16,
                 base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy};
 
@@ -58,6 +59,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     gx_transport_config c = base;
     c.block_size = t.block;
     c.blocks_per_sm = t.bpsm;
+    c.steps_per_launch = t.steps;
     c.graph_iters = t.graph_iters;
     c.refill_below = t.refill_below;
     c.wave_energy = t.wave_energy;
@@ -78,6 +80,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     if (rep && ntrials < GX_AUTOTUNE_MAX_TRIALS) {
       rep->block_size[ntrials] = t.block;
       rep->blocks_per_sm[ntrials] = t.bpsm;
+      rep->steps_per_launch[ntrials] = t.steps;
       rep->graph_iters[ntrials] = t.graph_iters;
       rep->refill_below[ntrials] = t.refill_below;
       rep->wave_energy[ntrials] = t.wave_energy;
@@ -107,8 +110,14 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
       consider(t);
     }
   const Trial after_shape = best;
-  for (int g : {4, 8, 32, 64}) {
+  for (int k : {1, 16, 64, 1024}) {
     Trial t = after_shape;
+    t.steps = k;
+    consider(t);
+  }
+  const Trial after_steps = best;
+  for (int g : {4, 8, 32, 64}) {
+    Trial t = after_steps;
     t.graph_iters = g;
     consider(t);
   }
@@ -132,6 +141,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   if (best_rate <= 0.0) return set_error(GX_ERR_OVERFLOW, "gx_transport_autotune: no setting completed the sample");
   cfg->block_size = best.block;
   cfg->blocks_per_sm = best.bpsm;
+  cfg->steps_per_launch = best.steps;
   cfg->graph_iters = best.graph_iters;
   cfg->refill_below = best.refill_below;
   cfg->wave_energy = best.wave_energy;

@@ -33,6 +33,9 @@ inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStrea
 // keeps 256).
 inline int default_block(int engine) { return engine == 1 ? 128 : 256; }
 constexpr int kDefaultBlocksPerSM = 4;
+// Steps of one track per transport-kernel launch in the batched engine, at
+// most (a track is kept in registers while it neither interacts nor dies).
+constexpr int kDefaultStepsPerLaunch = 16;
 // Primary energy per injection wave for stores of cap slots: a 10 GeV shower
 // peaks near 800 tracks in flight, ~0.08 per MeV of primary energy; waves are
 // sized so that their showers would peak at `fill` x cap if they all peaked

@@ -64,6 +64,7 @@ struct Ctl {
   double wave_energy; // primary energy injected per wave, at most
   long long refill_below, stack_cap;
   long long qcount[3][3]; // records in the interaction buffers [particle][process]
+  long long take[3];      // tracks of the current stores handed out to the transport kernels
 };
 
 struct Prims {
@@ -89,6 +90,7 @@ template <class R> struct Args {
   // compactly so the interaction kernels read them coalesced (batched engine)
   Store<R> ibuf[3][3];
   long long qcap;
+  int step_budget; // steps of one track per transport launch, at most
 };
 
 // ---------------------------------------------------------------- geometry
@@ -365,52 +367,84 @@ template <class R> struct Secs {
   }
 };
 
+// One helix sub-step of length s in a uniform field along z: the reference's
+// ConstFieldHelixStepper::DoStep (magneticfield/ConstFieldHelixStepper.hpp:164-239)
+// with B = (0, 0, Bz) substituted, where the field-direction terms vanish.
+// With rn = p / (kB2C q |Bz|) (signed), phi = -s / rn and sB = sign(Bz):
+//   x' = x + rn ((cos phi - 1) dy sB - sin phi dx),   dx' = cos phi dx + sin phi dy sB
+//   y' = y + rn (-(cos phi - 1) dx sB - sin phi dy),  dy' = cos phi dy - sin phi dx sB
+//   z' = z + s dz,                                     dz' = dz
+// (the reference's R v equals rn (dx, dy) since sinVB = |(dx, dy)|), with
+// cos phi - 1 = -2 sin^2(phi / 2), free of cancellation at small bending
+// angles.  The rotation and the transverse displacement are computed in T, the
+// displacement is added to the FP64 position.
+__device__ __forceinline__ void sincos_t(float x, float *s, float *c) { sincosf(x, s, c); }
+__device__ __forceinline__ void sincos_t(double x, double *s, double *c) { ::sincos(x, s, c); }
+
+template <class T>
+__device__ __forceinline__ void helix_bz(T rn, T sB, double s, const double pos[3], const T dir[3], double np[3],
+                                         T nd[3])
+{
+  const T phi = -(T)s / rn;
+  T sh, ch;
+  sincos_t(T(0.5) * phi, &sh, &ch);
+  const T sinp = T(2) * sh * ch, cm1 = T(-2) * sh * sh, cosp = T(1) + cm1;
+  np[0] = pos[0] + (double)(rn * (cm1 * dir[1] * sB - sinp * dir[0]));
+  np[1] = pos[1] + (double)(rn * (-cm1 * dir[0] * sB - sinp * dir[1]));
+  np[2] = pos[2] + s * (double)dir[2];
+  nd[0] = cosp * dir[0] + sinp * dir[1] * sB;
+  nd[1] = cosp * dir[1] - sinp * dir[0] * sB;
+  nd[2] = dir[2];
+}
+
 // Helix sub-steps in Bz (FieldPropagationHandler::Propagate / PropagateInVolume,
-// magneticfield/src/FieldPropagationHandler.cpp:87-360), FP64.
+// magneticfield/src/FieldPropagationHandler.cpp:87-360).  Positions, the
+// geometry and the step bookkeeping are FP64; the direction, the momentum and
+// the sub-step length heuristic are in R (FP32 in the mixed build).
 template <class R>
 __device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool &crossed, int &newvol, Local &L)
 {
-  const double eps = 0.1; // gEpsDeflection = 1e-2 cm
-  double charge = (t.type == 1) ? -1.0 : 1.0;
-  double E = (double)t.E;
-  double p = ::sqrt(E * (E + 2.0 * kEMass));
+  const R eps = R(0.1); // gEpsDeflection = 1e-2 cm
+  const R charge = (t.type == 1) ? R(-1) : R(1);
+  const R p = M<R>::sqrt(t.E * (t.E + R(2.0 * kEMass)));
+  const R absB = (R)fabs(g.Bz), sB = g.Bz >= 0.0 ? R(1) : R(-1);
+  const R rn = p / (R(kB2C_mm) * charge * absB);
+  const R curv_per_pt = R(0.299792458) * absB; // 1 / radius = curv_per_pt / pt
   double pos[3] = {t.pos[0], t.pos[1], t.pos[2]};
-  double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+  R dir[3] = {t.dir[0], t.dir[1], t.dir[2]};
   double remaining = pstep, total = 0.0;
-  const double B[3] = {0.0, 0.0, g.Bz};
   crossed = false;
   newvol = t.vol;
   for (int it = 0; it < 10000; ++it) {
     int plane;
+    double dd[3] = {(double)dir[0], (double)dir[1], (double)dir[2]};
     double saf = safety(g, t.vol, pos);
     double snext = (saf > remaining) ? remaining
-                                     : fmax(2e-9, fmin(dist_to_out(g, t.vol, pos, dir, plane), remaining) + 2e-9);
+                                     : fmax(2e-9, fmin(dist_to_out(g, t.vol, pos, dd, plane), remaining) + 2e-9);
     double step_gp = fmax(fmin(remaining, 1e-4), snext);
-    double pt = p * ::sqrt(fmax(1.0 - dir[2] * dir[2], 0.0));
+    R pt = p * M<R>::sqrt(fmax(R(1) - dir[2] * dir[2], R(0)));
     double step_field = 1.7976931348623157e308;
-    if (pt > 0.0) step_field = fmax(2.0 * ::sqrt(eps / (0.299792458 * fabs(g.Bz) / pt)), saf);
+    if (pt > R(0)) step_field = fmax(2.0 * (double)M<R>::sqrt(eps * pt / curv_per_pt), saf);
     double s = fmin(fmin(step_gp, step_field), remaining);
-    double np[3], nd[3];
-    if (pt > 0.0) {
-      helix_dostep(kB2C_mm, B, pos, dir, charge, p, s, np, nd);
-      double m = ::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
-      nd[0] /= m;
-      nd[1] /= m;
-      nd[2] /= m;
+    double np[3];
+    if (pt > R(0)) {
+      R nd[3];
+      helix_bz<R>(rn, sB, s, pos, dir, np, nd);
+      const R inv = R(1) / M<R>::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+      dir[0] = nd[0] * inv;
+      dir[1] = nd[1] * inv;
+      dir[2] = nd[2] * inv;
     } else {
-      for (int k = 0; k < 3; ++k) {
-        np[k] = pos[k] + s * dir[k];
-        nd[k] = dir[k];
-      }
+      for (int k = 0; k < 3; ++k) np[k] = pos[k] + s * dd[k];
     }
-    for (int k = 0; k < 3; ++k) {
-      pos[k] = np[k];
-      dir[k] = nd[k];
-    }
+    for (int k = 0; k < 3; ++k) pos[k] = np[k];
     total += s;
     remaining -= s;
     L.st[S_SUBSTEPS]++;
-    int v = relocate(g, t.vol, pos, dir);
+    dd[0] = (double)dir[0];
+    dd[1] = (double)dir[1];
+    dd[2] = (double)dir[2];
+    int v = relocate(g, t.vol, pos, dd);
     if (v != t.vol || remaining <= 1e-10) {
       if (v != t.vol) {
         crossed = true;
@@ -418,7 +452,7 @@ __device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool
       }
       for (int k = 0; k < 3; ++k) {
         t.pos[k] = pos[k];
-        t.dir[k] = (R)dir[k];
+        t.dir[k] = dir[k];
       }
       return total;
     }
@@ -429,7 +463,7 @@ __device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool
   newvol = -2;
   for (int k = 0; k < 3; ++k) {
     t.pos[k] = pos[k];
-    t.dir[k] = (R)dir[k];
+    t.dir[k] = dir[k];
   }
   return total;
 }
@@ -849,10 +883,30 @@ template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step_p(co
 }
 
 // ------------------------------------------------- batched engine: split step
-// Transport part of the step for every track of type PT: survivors without an
-// interaction go to the next store, a track that interacts goes to the
-// interaction buffer of its process (slots from warp prefix sums, one atomic
-// per warp and destination, so both writes are contiguous).
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// One slot per flagged lane in counter *ctr (ballot and popcount, one atomic
+// per warp when any lane is flagged); returns this lane's slot, 0 for lanes
+// not flagged.  Every lane of the warp calls it.
+__device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool flag)
+{
+  const unsigned m = __ballot_sync(0xffffffffu, flag);
+  if (!m) return 0;
+  const int leader = __ffs(m) - 1;
+  unsigned long long base = 0;
+  if ((int)lane_id() == leader) base = atomicAdd(ctr, (unsigned long long)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return flag ? (long long)base + __popc(m & lanemask_lt()) : 0;
+}
+
+// Transport of the tracks of type PT: each lane keeps its track in registers
+// and steps it until the track interacts (it then goes to the interaction
+// buffer of its process), dies, leaves the world, or has taken step_budget
+// steps in this launch (it then goes to the next store).  A lane without a
+// track takes the next one of the current store from a work counter shared by
+// the whole grid (one atomic per warp for all its idle lanes), so the lanes
+// of a warp stay busy while their tracks take different numbers of steps.
+// All stores and buffers are written at slots reserved per warp, contiguous.
 template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
@@ -868,32 +922,51 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
-  const long long stride = (long long)gridDim.x * blockDim.x;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
-    long long i = base + threadIdx.x;
-    bool active = i < n;
-    Track<R> t;
+  const int budget = a.step_budget;
+  Track<R> t;
+  bool have = false, more = true; // `more` is warp-uniform: the work counter is not exhausted
+  int nst = 0;
+  for (;;) {
+    const unsigned need = __ballot_sync(0xffffffffu, !have);
+    if (need && more) {
+      const int leader = __ffs(need) - 1;
+      unsigned long long base = 0;
+      if ((int)lane_id() == leader) base = atomicAdd((unsigned long long *)&ctl->take[PT], (unsigned long long)__popc(need));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (!have) {
+        const long long i = (long long)base + __popc(need & lanemask_lt());
+        if (i < n) {
+          load_track(cur, i, PT, t);
+          L.st[S_READ0 + PT]++;
+          L.st[S_TREAD0 + PT]++;
+          have = true;
+          nst = 0;
+        }
+      }
+      if ((long long)base + __popc(need) >= n) more = false;
+    }
+    if (!__any_sync(0xffffffffu, have)) break;
     int r = kDone, proc = -1;
-    if (active) {
-      load_track(cur, i, PT, t);
-      L.st[S_READ0 + PT]++;
-      L.st[S_TREAD0 + PT]++;
+    if (have) {
       r = transport_part(d, a.g, t, L, &proc);
+      ++nst;
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
-    long long slot = warp_reserve((unsigned long long *)&ctl->count[par ^ 1][PT], r == kAlive ? 1 : 0);
+    const bool w_alive = have && r == kAlive && nst >= budget;
+    const bool w_int = have && r == kInteract;
+    const long long slot = warp_take1((unsigned long long *)&ctl->count[par ^ 1][PT], w_alive);
     long long q = 0;
 #pragma unroll
     for (int p = 0; p < 3; ++p) {
       if (PT == 1 && p == 2) continue; // e- has two processes
-      long long v = warp_reserve((unsigned long long *)&ctl->qcount[PT][p], (r == kInteract && proc == p) ? 1 : 0);
+      const long long v = warp_take1((unsigned long long *)&ctl->qcount[PT][p], w_int && proc == p);
       if (p == proc) q = v;
     }
-    if (r == kAlive) {
+    if (w_alive) {
       put_track(a, PT, slot, t, L);
       L.st[S_WRITE0 + PT]++;
       L.st[S_TWRITE0 + PT]++;
-    } else if (r == kInteract) {
+    } else if (w_int) {
       if (q < a.qcap) {
         store_track(a.ibuf[PT][proc], q, t);
         L.st[S_WRITE0 + PT]++;
@@ -905,6 +978,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
         L.deposit(t.event, t.vol, (double)t.E);
       }
     }
+    if (have && (r != kAlive || nst >= budget)) have = false;
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
 }
@@ -953,8 +1027,10 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
   int par = ctl->parity, np = par ^ 1;
   const long long cap[3] = {cap0, cap1, cap2};
   const long long refill_below = ctl->refill_below, stack_cap = ctl->stack_cap;
-  for (int q = 0; q < 3; ++q)
+  for (int q = 0; q < 3; ++q) {
     for (int p = 0; p < 3; ++p) ctl->qcount[q][p] = 0;
+    ctl->take[q] = 0;
+  }
   long long fl = 0;
   for (int q = 0; q < nstores; ++q) {
     // pushes past the end of a full stack were not written (and were counted as errors)
@@ -1325,6 +1401,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         if (q != 1 || pr != 2) L.a.ibuf[q][pr] = carve<R>(base, off, cap, false);
     L.a.qcap = cap;
   }
+  L.a.step_budget = cfg->steps_per_launch > 0 ? cfg->steps_per_launch : kDefaultStepsPerLaunch;
   if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
   L.a.d = C->dev;
   L.a.ctl = E->ctl;

@@ -169,6 +169,8 @@ typedef struct {
   int graph_iters;         /* iterations per CUDA-graph launch between host checks (0: default) */
   int profile;             /* 1: no graph; CUDA events around every step kernel (per-kernel times in stats) */
   double wave_energy;      /* primary energy (MeV) injected per wave, at most (0: from capacity) */
+  int steps_per_launch;    /* batched engine: steps of one track per transport launch, at most; a track
+                              stays in registers between them (0: default 16; 1: one step per iteration) */
 } gx_transport_config;
 
 typedef struct {
@@ -214,19 +216,20 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
  * source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).  Transports the given
  * primaries (the whole batch, or a representative subset of it) once per
  * candidate: block size {64, 128, 256} x resident blocks per SM {1, 2, 4, 8},
- * then iterations per CUDA-graph launch {4, 8, 32, 64}, then the refill
+ * then steps per track and transport launch {1, 16, 64, 1024}, then
+ * iterations per CUDA-graph launch {4, 8, 32, 64}, then the refill
  * threshold {1/8, 1/4, 3/4 of the capacity}, then the primary energy per
  * injection wave {1/4, 1/2, 2 x the default}, each coordinate from the best so
  * far.  Score: track-steps per millisecond of device time, best of `repeats`
  * runs (at least 1; the first run of a new launch shape includes its graph
  * capture).  Writes the winner into cfg->block_size, blocks_per_sm,
- * graph_iters, refill_below and wave_energy; report (optional) lists every
+ * steps_per_launch, graph_iters, refill_below and wave_energy; report (optional) lists every
  * trial.  cfg->engine must be 1; the precision and capacity are kept. */
 #define GX_AUTOTUNE_MAX_TRIALS 64
 typedef struct {
   int trials, best; /* number of trials listed; index of the winner */
   int block_size[GX_AUTOTUNE_MAX_TRIALS], blocks_per_sm[GX_AUTOTUNE_MAX_TRIALS];
-  int graph_iters[GX_AUTOTUNE_MAX_TRIALS];
+  int steps_per_launch[GX_AUTOTUNE_MAX_TRIALS], graph_iters[GX_AUTOTUNE_MAX_TRIALS];
   long long refill_below[GX_AUTOTUNE_MAX_TRIALS];
   double wave_energy[GX_AUTOTUNE_MAX_TRIALS];
   double kernel_ms[GX_AUTOTUNE_MAX_TRIALS];    /* device time, best of the repeats (0: did not complete) */

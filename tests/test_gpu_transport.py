@@ -177,8 +177,23 @@ def test_autotune_and_launch_settings_leave_results_unchanged(dm):
     assert s1["steps"] == s0["steps"] and s1["tracks"] == s0["tracks"]
     assert np.array_equal(ps0, ps1)
     np.testing.assert_allclose(e1, e0, rtol=1e-5, atol=1e-6 * e0.max())
-    for k in ("block_size", "blocks_per_sm", "graph_iters", "refill_below", "wave_energy"):
+    for k in ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy"):
         setattr(cfg, k, 0)
+
+
+def test_steps_per_launch_leaves_results_unchanged(dm):
+    """One step per transport launch (a track goes back to memory after every
+    step) and many steps per launch (it stays in registers) transport the same
+    tracks."""
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(8, 8)
+    runs = [run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True, steps_per_launch=k) for k in (1, 7, 4096)]
+    cfg.steps_per_launch = 0
+    for e, st, ps in runs[1:]:
+        assert st["steps"] == runs[0][1]["steps"] and st["tracks"] == runs[0][1]["tracks"]
+        assert np.array_equal(ps, runs[0][2])
+        np.testing.assert_allclose(e, runs[0][0], rtol=1e-5, atol=1e-6 * runs[0][0].max())
+    assert runs[2][1]["iterations"] < runs[0][1]["iterations"]
 
 
 def test_step_count_distributions_fp32_vs_fp64(dm):
