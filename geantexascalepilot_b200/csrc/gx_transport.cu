@@ -397,77 +397,6 @@ __device__ __forceinline__ void helix_bz(T rn, T sB, double s, const double pos[
   nd[2] = dir[2];
 }
 
-// Helix sub-steps in Bz (FieldPropagationHandler::Propagate / PropagateInVolume,
-// magneticfield/src/FieldPropagationHandler.cpp:87-360).  Positions, the
-// geometry and the step bookkeeping are FP64; the direction, the momentum and
-// the sub-step length heuristic are in R (FP32 in the mixed build).
-template <class R>
-__device__ double field_propagate(const Geom &g, Track<R> &t, double pstep, bool &crossed, int &newvol, Local &L)
-{
-  const R eps = R(0.1); // gEpsDeflection = 1e-2 cm
-  const R charge = (t.type == 1) ? R(-1) : R(1);
-  const R p = M<R>::sqrt(t.E * (t.E + R(2.0 * kEMass)));
-  const R absB = (R)fabs(g.Bz), sB = g.Bz >= 0.0 ? R(1) : R(-1);
-  const R rn = p / (R(kB2C_mm) * charge * absB);
-  const R curv_per_pt = R(0.299792458) * absB; // 1 / radius = curv_per_pt / pt
-  double pos[3] = {t.pos[0], t.pos[1], t.pos[2]};
-  R dir[3] = {t.dir[0], t.dir[1], t.dir[2]};
-  double remaining = pstep, total = 0.0;
-  crossed = false;
-  newvol = t.vol;
-  for (int it = 0; it < 10000; ++it) {
-    int plane;
-    double dd[3] = {(double)dir[0], (double)dir[1], (double)dir[2]};
-    double saf = safety(g, t.vol, pos);
-    double snext = (saf > remaining) ? remaining
-                                     : fmax(2e-9, fmin(dist_to_out(g, t.vol, pos, dd, plane), remaining) + 2e-9);
-    double step_gp = fmax(fmin(remaining, 1e-4), snext);
-    R pt = p * M<R>::sqrt(fmax(R(1) - dir[2] * dir[2], R(0)));
-    double step_field = 1.7976931348623157e308;
-    if (pt > R(0)) step_field = fmax(2.0 * (double)M<R>::sqrt(eps * pt / curv_per_pt), saf);
-    double s = fmin(fmin(step_gp, step_field), remaining);
-    double np[3];
-    if (pt > R(0)) {
-      R nd[3];
-      helix_bz<R>(rn, sB, s, pos, dir, np, nd);
-      const R inv = R(1) / M<R>::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
-      dir[0] = nd[0] * inv;
-      dir[1] = nd[1] * inv;
-      dir[2] = nd[2] * inv;
-    } else {
-      for (int k = 0; k < 3; ++k) np[k] = pos[k] + s * dd[k];
-    }
-    for (int k = 0; k < 3; ++k) pos[k] = np[k];
-    total += s;
-    remaining -= s;
-    L.st[S_SUBSTEPS]++;
-    dd[0] = (double)dir[0];
-    dd[1] = (double)dir[1];
-    dd[2] = (double)dir[2];
-    int v = relocate(g, t.vol, pos, dd);
-    if (v != t.vol || remaining <= 1e-10) {
-      if (v != t.vol) {
-        crossed = true;
-        newvol = v;
-      }
-      for (int k = 0; k < 3; ++k) {
-        t.pos[k] = pos[k];
-        t.dir[k] = dir[k];
-      }
-      return total;
-    }
-  }
-  L.err |= kErrFieldCap;
-  L.st[S_ERR]++;
-  crossed = true;
-  newvol = -2;
-  for (int k = 0; k < 3; ++k) {
-    t.pos[k] = pos[k];
-    t.dir[k] = dir[k];
-  }
-  return total;
-}
-
 template <class R>
 __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R> &t, int proc, Secs<R> &sec,
                                           Local &L)
@@ -533,18 +462,40 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
 enum { kDone = 0, kAlive = 1, kInteract = 2 };
 
 // One OneStep (test_BasicCpuTransport.cpp:408-497 / InnerStep :358-403) in
-// physics mode, up to the choice of the post-step interaction: GPIL, step
-// limit, propagation, NIL update, continuous loss.  Returns kDone (track
-// finished), kAlive (no interaction this step) or kInteract with *proc set
-// (for a stopped e+, proc 2 = annihilation at rest, at E = 0).
-template <class R> __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
-                                                                 int *proc)
+// physics mode, up to the choice of the post-step interaction, in three
+// phases so that a kernel can interleave tracks at different points of their
+// steps: step_begin (GPIL and the step limit; a straight-line move completes
+// here), field_substep (one helix sub-step, repeated until the step ends) and
+// step_end (NIL update, continuous loss, outcome).  The state carried from one
+// phase to the next:
+template <class R> struct StepCtx {
+  // macroscopic cross sections at the start of the step (scalars: an array
+  // member of a structure that lives across loop passes ends up in local
+  // memory)
+  R xs0, xs1, xs2;
+  double remaining; // helix: length of the step still to go
+  double total;     // length travelled in this step
+  int sel;          // process that limits the step (-1: none)
+  int vol0;         // volume at the start of the step
+  int newvol;       // volume entered (-2: sub-step cap hit)
+  int nsub;         // helix sub-steps taken
+  bool crossed;     // the step ended on a boundary
+  __device__ __forceinline__ R xs(int i) const { return i == 0 ? xs0 : (i == 1 ? xs1 : xs2); }
+};
+
+// GPIL and step limit.  Returns true when the step continues with helix
+// sub-steps (a charged track in a field), false when it is complete.
+template <class R>
+__device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c)
 {
-  int mat = vol_material(g, t.vol);
-  int np = (t.type == 1) ? 2 : 3;
-  bool charged = t.type != 0;
+  const int mat = vol_material(g, t.vol);
+  const int np = (t.type == 1) ? 2 : 3;
+  const bool charged = t.type != 0;
   R xs[3];
   cross_sections<R>(d, t.type, mat, t.E, xs);
+  c.xs0 = xs[0];
+  c.xs1 = xs[1];
+  c.xs2 = xs[2];
   // loops over the three process slots are unrolled with the bound as a guard,
   // so xs[] and nil[] are indexed by constants and stay in registers
 #pragma unroll
@@ -568,45 +519,121 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
       sel = -1;
     }
   }
-  int vol0 = t.vol, newvol = t.vol;
-  bool crossed = false;
-  double step;
-  if (!charged || g.Bz == 0.0) {
-    int plane;
-    double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
-    double dd = dist_to_out(g, t.vol, t.pos, dir, plane);
-    double ps = (double)pstep;
-    if (dd < ps) {
-      step = dd;
-      crossed = true;
-      newvol = next_volume(g, t.vol, plane);
-      for (int k = 0; k < 3; ++k) t.pos[k] += step * dir[k];
-      if (plane != 2) {
-        double lo, hi;
-        slab_bounds(g, t.vol, lo, hi);
-        set_comp(t.pos, g.axis, plane > 0 ? hi : lo);
-      }
-    } else {
-      step = ps;
-      for (int k = 0; k < 3; ++k) t.pos[k] += step * dir[k];
+  c.sel = sel;
+  c.vol0 = t.vol;
+  c.newvol = t.vol;
+  c.crossed = false;
+  c.nsub = 0;
+  if (charged && g.Bz != 0.0) {
+    c.remaining = (double)pstep;
+    c.total = 0.0;
+    return true;
+  }
+  int plane;
+  double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+  double dd = dist_to_out(g, t.vol, t.pos, dir, plane);
+  double ps = (double)pstep;
+  if (dd < ps) {
+    c.total = dd;
+    c.crossed = true;
+    c.newvol = next_volume(g, t.vol, plane);
+    for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
+    if (plane != 2) {
+      double lo, hi;
+      slab_bounds(g, t.vol, lo, hi);
+      set_comp(t.pos, g.axis, plane > 0 ? hi : lo);
     }
   } else {
-    step = field_propagate(g, t, (double)pstep, crossed, newvol, L);
+    c.total = ps;
+    for (int k = 0; k < 3; ++k) t.pos[k] += ps * dir[k];
   }
+  return false;
+}
+
+// One helix sub-step in Bz (FieldPropagationHandler::Propagate /
+// PropagateInVolume, magneticfield/src/FieldPropagationHandler.cpp:87-360).
+// Positions, the geometry and the step bookkeeping are FP64; the direction,
+// the momentum and the sub-step length heuristic are in R (FP32 in the mixed
+// build).  Returns true when the step is complete (boundary reached, length
+// used up, or the cap of 10000 sub-steps hit: then newvol = -2).
+template <class R> __device__ __forceinline__ bool field_substep(const Geom &g, Track<R> &t, StepCtx<R> &c, Local &L)
+{
+  const R eps = R(0.1); // gEpsDeflection = 1e-2 cm
+  const R charge = (t.type == 1) ? R(-1) : R(1);
+  const R p = M<R>::sqrt(t.E * (t.E + R(2.0 * kEMass)));
+  const R absB = (R)fabs(g.Bz), sB = g.Bz >= 0.0 ? R(1) : R(-1);
+  const R curv_per_pt = R(0.299792458) * absB; // 1 / radius = curv_per_pt / pt
+  int plane;
+  double dd[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+  const double remaining = c.remaining;
+  double saf = safety(g, t.vol, t.pos);
+  double snext = (saf > remaining) ? remaining
+                                   : fmax(2e-9, fmin(dist_to_out(g, t.vol, t.pos, dd, plane), remaining) + 2e-9);
+  double step_gp = fmax(fmin(remaining, 1e-4), snext);
+  R pt = p * M<R>::sqrt(fmax(R(1) - t.dir[2] * t.dir[2], R(0)));
+  double step_field = 1.7976931348623157e308;
+  if (pt > R(0)) step_field = fmax(2.0 * (double)M<R>::sqrt(eps * pt / curv_per_pt), saf);
+  double s = fmin(fmin(step_gp, step_field), remaining);
+  if (pt > R(0)) {
+    const R rn = p / (R(kB2C_mm) * charge * absB);
+    double np[3];
+    R nd[3];
+    helix_bz<R>(rn, sB, s, t.pos, t.dir, np, nd);
+    const R inv = R(1) / M<R>::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+    for (int k = 0; k < 3; ++k) {
+      t.pos[k] = np[k];
+      t.dir[k] = nd[k] * inv;
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) t.pos[k] += s * dd[k];
+  }
+  c.total += s;
+  c.remaining = remaining - s;
+  L.st[S_SUBSTEPS]++;
+  dd[0] = (double)t.dir[0];
+  dd[1] = (double)t.dir[1];
+  dd[2] = (double)t.dir[2];
+  int v = relocate(g, t.vol, t.pos, dd);
+  if (v != t.vol || c.remaining <= 1e-10) {
+    if (v != t.vol) {
+      c.crossed = true;
+      c.newvol = v;
+    }
+    return true;
+  }
+  if (++c.nsub >= 10000) {
+    L.err |= kErrFieldCap;
+    L.st[S_ERR]++;
+    c.crossed = true;
+    c.newvol = -2;
+    return true;
+  }
+  return false;
+}
+
+// NIL update, continuous loss and the outcome of the step: kDone (track
+// finished), kAlive (no interaction this step) or kInteract with *proc set
+// (for a stopped e+, proc 2 = annihilation at rest, at E = 0).
+template <class R>
+__device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &t, const StepCtx<R> &c, Local &L,
+                                        int *proc)
+{
+  const int np = (t.type == 1) ? 2 : 3;
+  const double step = c.total;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    if (i < np) t.nil[i] -= (R)step * xs[i];
+    if (i < np) t.nil[i] -= (R)step * c.xs(i);
   L.st[S_STEPS]++;
-  if (newvol == -2) {
-    L.deposit(t.event, vol0, (double)t.E);
+  if (c.newvol == -2) {
+    L.deposit(t.event, c.vol0, (double)t.E);
     return kDone;
   }
-  if (charged) {
-    R eloss = along_loss<R>(d, t.type, mat, step, t.E);
-    L.deposit(t.event, vol0, (double)eloss);
+  if (t.type != 0) {
+    R eloss = along_loss<R>(d, t.type, vol_material(g, c.vol0), step, t.E);
+    L.deposit(t.event, c.vol0, (double)eloss);
     if (t.E <= R(0)) {
       if (t.type == 2) {
-        int v = crossed ? newvol : vol0;
+        int v = c.crossed ? c.newvol : c.vol0;
         if (v >= 0) {
           t.vol = v;
           t.E = R(0);
@@ -618,22 +645,33 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
       return kDone;
     }
   }
-  if (crossed) {
-    t.vol = newvol;
-    if (newvol < 0) {
+  if (c.crossed) {
+    t.vol = c.newvol;
+    if (c.newvol < 0) {
       L.escaped += (double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0);
       return kDone;
     }
     return kAlive;
   }
-  if (sel >= 0) {
+  if (c.sel >= 0) {
 #pragma unroll
     for (int i = 0; i < 3; ++i)
-      if (i == sel) t.nil[i] = R(-1);
-    *proc = sel;
+      if (i == c.sel) t.nil[i] = R(-1);
+    *proc = c.sel;
     return kInteract;
   }
   return kAlive;
+}
+
+// The three phases in sequence: one whole step up to the interaction.
+template <class R> __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
+                                                                 int *proc)
+{
+  StepCtx<R> c;
+  if (step_begin(d, g, t, c))
+    while (!field_substep(g, t, c, L)) {
+    }
+  return step_end(d, g, t, c, L, proc);
 }
 
 // The whole OneStep, interaction included (the fused form the plain loop
@@ -906,6 +944,9 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
 // track takes the next one of the current store from a work counter shared by
 // the whole grid (one atomic per warp for all its idle lanes), so the lanes
 // of a warp stay busy while their tracks take different numbers of steps.
+// One pass of the loop advances every lane by one helix sub-step (charged
+// tracks in a field), with the start and the end of a step attached to it, so
+// a lane whose step needs several sub-steps does not hold up the others.
 // All stores and buffers are written at slots reserved per warp, contiguous.
 template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(const Args<R> *__restrict__ A)
 {
@@ -924,7 +965,9 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
   const int budget = a.step_budget;
   Track<R> t;
+  StepCtx<R> c;
   bool have = false, more = true; // `more` is warp-uniform: the work counter is not exhausted
+  bool infield = false;           // in the middle of a step (helix sub-steps)
   int nst = 0;
   for (;;) {
     const unsigned need = __ballot_sync(0xffffffffu, !have);
@@ -940,6 +983,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
           L.st[S_READ0 + PT]++;
           L.st[S_TREAD0 + PT]++;
           have = true;
+          infield = false;
           nst = 0;
         }
       }
@@ -947,13 +991,22 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
     }
     if (!__any_sync(0xffffffffu, have)) break;
     int r = kDone, proc = -1;
-    if (have) {
-      r = transport_part(d, a.g, t, L, &proc);
+    bool done = false; // a step ends in this pass
+    if (have && !infield) {
+      infield = step_begin(d, a.g, t, c);
+      done = !infield;
+    }
+    if (PT != 0 && have && infield && field_substep(a.g, t, c, L)) {
+      infield = false;
+      done = true;
+    }
+    if (done) {
+      r = step_end(d, a.g, t, c, L, &proc);
       ++nst;
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
-    const bool w_alive = have && r == kAlive && nst >= budget;
-    const bool w_int = have && r == kInteract;
+    const bool w_alive = done && r == kAlive && nst >= budget;
+    const bool w_int = done && r == kInteract;
     const long long slot = warp_take1((unsigned long long *)&ctl->count[par ^ 1][PT], w_alive);
     long long q = 0;
 #pragma unroll
@@ -978,7 +1031,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
         L.deposit(t.event, t.vol, (double)t.E);
       }
     }
-    if (have && (r != kAlive || nst >= budget)) have = false;
+    if (done && (r != kAlive || nst >= budget)) have = false;
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
 }
