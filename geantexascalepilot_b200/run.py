@@ -3,6 +3,7 @@
     python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --precision 1
     python -m geantexascalepilot_b200.run c5 --nevents 64 --mean 100 --profile
     python -m geantexascalepilot_b200.run c4 --n 4096 --autotune
+    python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --profile --capacity 2097152
 
 Prints one JSON line: the workload, the transport statistics (steps,
 propagation sub-steps, tracks, secondaries, iterations, per-kernel device
@@ -25,6 +26,8 @@ def main(argv=None):
     p.add_argument("--engine", type=int, default=1, choices=[0, 1], help="0 plain loop, 1 batched")
     p.add_argument("--profile", action="store_true", help="time each step kernel with CUDA events (no graph)")
     p.add_argument("--autotune", action="store_true", help="sweep the launch settings first")
+    p.add_argument("--capacity", type=int, default=0,
+                   help="track slots per particle type and store (0: the engine's default, 2^24)")
     p.add_argument("--repeat", type=int, default=1, help="transport the workload this many times")
     p.add_argument("--device", type=int, default=0)
     a = p.parse_args(argv)
@@ -43,6 +46,7 @@ def main(argv=None):
         fn = getattr(configs, a.workload)
         cfg, prims, nvol = fn(a.n) if a.n is not None else fn()
     cfg.precision, cfg.engine, cfg.profile = a.precision, a.engine, int(a.profile)
+    cfg.capacity = a.capacity
     dm = gx.ProxyDataManager(device=a.device)
     out = {"workload": a.workload, "primaries": int(len(prims[0])), "precision": a.precision, "engine": a.engine}
     if a.autotune:

@@ -217,3 +217,12 @@ def test_small_capacity_uses_the_overflow_stack(dm):
     assert sb["errors"] == 0
     assert sa["steps"] == sb["steps"]
     np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9 * a.max())
+
+
+def test_run_command_line(capsys):
+    import json
+    from geantexascalepilot_b200 import run
+    assert run.main(["c1", "--n", "200", "--precision", "0", "--capacity", "65536"]) == 0
+    out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert out["workload"] == "c1" and out["primaries"] == 200
+    assert out["stats"]["steps"] > 200 and out["stats"]["errors"] == 0
