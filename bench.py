@@ -320,13 +320,17 @@ def main():
         pass
     peak = peaks.get("hbm_gbs", 6650.0)
     traffic = None
-    tr = os.path.join(REPO, "profiles", "transport_kernel_dram.json")
+    tr = os.path.join(REPO, "profiles", "transport_kernel_dram.txt")
     if os.path.exists(tr):
         # DRAM bytes per track record processed, from one ncu capture of this
         # kernel on a smaller case, scaled to this run's records per launch
-        per = json.load(open(tr)).get("dram_bytes_per_record", {}).get(str(k))
-        if per:
-            traffic = per * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
+        per = {}
+        for line in open(tr):
+            f = line.split()
+            if len(f) == 2 and not line.startswith("#"):
+                per[int(f[0])] = float(f[1])
+        if k in per:
+            traffic = per[k] * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "traffic": traffic, "kernel": "k_transport<float,%d> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
