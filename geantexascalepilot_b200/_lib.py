@@ -65,6 +65,12 @@ class TransportStats(C.Structure):
                 "transport_queued": list(self.transport_queued)}
 
 
+class GunParams(C.Structure):
+    _fields_ = [("nevents", I), ("nparticles", I), ("gamma_fraction", D), ("min_p", D), ("max_p", D),
+                ("min_eta", D), ("max_eta", D), ("min_phi", D), ("max_phi", D), ("vertex", D * 3), ("seed", D * 6),
+                ("first_draw", LL), ("first_event", I)]
+
+
 AUTOTUNE_MAX_TRIALS = 64
 
 
@@ -106,6 +112,10 @@ _SIGS = {
                                   C.POINTER(TransportStats)]),
     "gx_transport_autotune": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, I, I, C.POINTER(AutotuneReport),
                                   P]),
+    "gx_egamma_gun": (I, [C.POINTER(GunParams), P, P, P, P, P, P, P]),
+    "gx_pdg_to_type": (I, [I]),
+    "gx_hepevt_read": (I, [C.c_char_p, I, I, I, P, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),
+    "gx_hepevt_load": (I, [C.c_char_p, I, I, PD, I, P, P, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I), P]),
     "gx_transport_run_noalloc": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I,
                                      C.POINTER(TransportStats), P]),
 }

@@ -12,7 +12,7 @@ import ctypes as C
 import torch
 
 from . import _lib
-from ._lib import AutotuneReport, GxError, ModelParams, TransportConfig, TransportStats, check, lib
+from ._lib import AutotuneReport, GunParams, GxError, ModelParams, TransportConfig, TransportStats, check, lib
 
 # physics-table ids (ProxyPhysicsTableIndex.hpp:23-45)
 TABLES = ["DEDX.eBrem.e-", "DEDX.eBrem.e+", "DEDX.eIoni.e-", "DEDX.eIoni.e+", "InverseRange.eIoni.e-",
@@ -353,3 +353,93 @@ def transport_noalloc(dm, cfg, types, E, pos, direction, events=None, nvol=None,
     check(lib.gx_transport_run_noalloc(dm.handle, C.byref(cfg), t.numel(), _ptr(t), _ptr(E), _ptr(p), _ptr(d),
                                        _ptr(ev), _ptr(edep), nvol, C.byref(st), _stream()))
     return edep, st.as_dict()
+
+
+# ------------------------------------------------------- primary generation
+def egamma_gun(nevents, nparticles, gamma_fraction=0.5, momentum=(1.0e3, 1.0e6), eta=(-3.0, 3.0),
+               phi=(0.0, 2.0 * 3.141592653589793), vertex=(0.0, 0.0, 0.0), seed=(12345.0,) * 6, first_draw=0,
+               first_event=0):
+    """ProxyEgammaGun (proxy/ProxyEgammaGun.hpp:35-82) on the device: returns
+    CUDA tensors (types, E, pos, dir, events, pdg) ready for transport().
+    Defaults are the reference's (1 GeV-1 TeV, |eta| < 3, full phi, seed
+    12345 x 6, the stream a fresh ProxyRandom starts at)."""
+    g = GunParams()
+    g.nevents, g.nparticles, g.gamma_fraction = nevents, nparticles, gamma_fraction
+    g.min_p, g.max_p = momentum
+    g.min_eta, g.max_eta = eta
+    g.min_phi, g.max_phi = phi
+    g.vertex[:] = list(vertex)
+    g.seed[:] = list(seed)
+    g.first_draw, g.first_event = first_draw, first_event
+    n = nevents * nparticles
+    t = torch.empty(n, dtype=torch.int32, device="cuda")
+    ev = torch.empty(n, dtype=torch.int32, device="cuda")
+    pdg = torch.empty(n, dtype=torch.int32, device="cuda")
+    E = torch.empty(n, dtype=torch.float64, device="cuda")
+    pos = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    d = torch.empty((n, 3), dtype=torch.float64, device="cuda")
+    check(lib.gx_egamma_gun(C.byref(g), _ptr(t), _ptr(E), _ptr(pos), _ptr(d), _ptr(ev), _ptr(pdg), _stream()))
+    return t, E, pos, d, ev, pdg
+
+
+def set_direction_xyz(x, y, z, mode=MODE_PHYSICS):
+    """ProxyEgammaGun::SetDirectionXYZ (proxy/src/ProxyEgammaGun.cpp:35-41):
+    the (eta, phi) both ranges collapse to.  MODE_QUIRK keeps the reference's
+    theta = atan(rho / z) and phi = atan(y / z) (a beam along z gets an
+    infinite eta, which the gun's range arithmetic turns into NaN, and z < 0
+    a NaN eta);
+    MODE_PHYSICS uses atan2 and keeps eta finite (|eta| <= 700: along the axis
+    to within exp(-700))."""
+    import math
+    rho = math.sqrt(x * x + y * y)
+    if mode == MODE_QUIRK:
+        theta, ph = math.atan(rho / z), math.atan(y / z)
+        t = math.tan(0.5 * theta)  # negative for z < 0: the reference's log gives NaN there
+        return (-math.log(t) if t > 0 else (math.inf if t == 0 else math.nan)), ph
+    theta, ph = math.atan2(rho, z), math.atan2(y, x)
+    t = math.tan(0.5 * theta)
+    eta = -math.log(t) if t > 0 else math.inf
+    return max(-700.0, min(700.0, eta)), ph
+
+
+def pdg_to_type(pdg):
+    return lib.gx_pdg_to_type(int(pdg))
+
+
+def hepevt_read(path, mode=MODE_PHYSICS, max_events=1 << 30):
+    """ProxyHepEvtGenerator (proxy/src/ProxyHepEvtGenerator.cpp:48-132) on the
+    host: dict of numpy arrays event, pdg, ekin (MeV in physics mode), dir,
+    plus nevents and bad (daughter indices outside their event)."""
+    import numpy as np
+    n, nev, bad = C.c_int(), C.c_int(), C.c_int()
+    rc = lib.gx_hepevt_read(path.encode(), mode, max_events, 0, None, None, None, None, C.byref(n), C.byref(nev),
+                            C.byref(bad))
+    if rc not in (_lib.GX_OK, _lib.GX_ERR_OVERFLOW):
+        check(rc)
+    cap = max(n.value, 1)
+    ev, pdg = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+    ek, d = np.zeros(cap), np.zeros((cap, 3))
+    vp = lambda a: C.c_void_p(a.ctypes.data)  # noqa: E731
+    check(lib.gx_hepevt_read(path.encode(), mode, max_events, cap, vp(ev), vp(pdg), vp(ek), vp(d), C.byref(n),
+                             C.byref(nev), C.byref(bad)))
+    k = n.value
+    return {"event": ev[:k], "pdg": pdg[:k], "ekin": ek[:k], "dir": d[:k], "nevents": nev.value, "bad": bad.value}
+
+
+def hepevt_load(path, mode=MODE_PHYSICS, max_events=1 << 30, vertex=(0.0, 0.0, 0.0), cap=None):
+    """gx_hepevt_load: the gamma / e- / e+ primaries of a HEPEVT file in CUDA
+    tensors (types, E, pos, dir, events), plus (nevents, nskipped)."""
+    if cap is None:
+        cap = len(hepevt_read(path, mode, max_events)["pdg"])
+    t = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
+    ev = torch.empty(max(cap, 1), dtype=torch.int32, device="cuda")
+    E = torch.empty(max(cap, 1), dtype=torch.float64, device="cuda")
+    pos = torch.empty((max(cap, 1), 3), dtype=torch.float64, device="cuda")
+    d = torch.empty((max(cap, 1), 3), dtype=torch.float64, device="cuda")
+    vtx = (C.c_double * 3)(*vertex)
+    n, nev, skip = C.c_int(), C.c_int(), C.c_int()
+    check(lib.gx_hepevt_load(path.encode(), mode, max_events, vtx, cap, _ptr(t), _ptr(E), _ptr(pos), _ptr(d), _ptr(ev),
+                             C.byref(n), C.byref(nev), C.byref(skip), _stream()))
+    k = n.value
+    return (t[:k], E[:k], pos[:k], d[:k], ev[:k]), (nev.value, skip.value)
+

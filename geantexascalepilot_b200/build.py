@@ -38,11 +38,11 @@ def system_libstdcxx():
     return None
 
 
-# The per-function batch kernels reproduce the reference's FP64 arithmetic
-# operation by operation: no fused multiply-adds there, so they round like the
-# host code (only the transcendental functions differ).  The transport engine
-# keeps contraction.
-PER_FILE = {"gx_kernels.cu": ["-fmad=false"]}
+# The per-function batch kernels and the particle gun reproduce the reference's
+# FP64 arithmetic operation by operation: no fused multiply-adds there, so they
+# round like the host code (only the transcendental functions differ).  The
+# transport engine keeps contraction.
+PER_FILE = {"gx_kernels.cu": ["-fmad=false"], "gx_events.cu": ["-fmad=false"]}
 
 
 def _compile(src, verbose):

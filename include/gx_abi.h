@@ -211,6 +211,57 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
                           const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
                           double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats);
 
+/* ------------------------------------------------- primary generation */
+/* The e/gamma particle gun of the reference, ProxyEgammaGun
+ * (source/Geant/proxy/ProxyEgammaGun.hpp:35-82, src/ProxyEgammaGun.cpp:43-85),
+ * writing transport primaries straight into device arrays.  Particle
+ * i = event x nparticles + j draws four uniforms from one MRG32k3a stream
+ * (the stream whose state is seed, after first_draw draws), in the
+ * reference's order: type (gamma below gamma_fraction, else e-), momentum
+ * uniform in [min_p, max_p] (MeV), eta, phi uniform in their ranges; kinetic
+ * energy p^2 / (sqrt(p^2 + m^2) + m), direction from eta and phi.  The
+ * output equals the reference's sequential output for the same stream state
+ * (the reference's ProxyRandom starts at the default seed, 12345 x 6).
+ * Position = vertex (the reference leaves it at the origin); d_event[i] =
+ * first_event + event; d_pdg (optional) gets 22 / 11.  Draws consumed:
+ * 4 x nevents x nparticles. */
+typedef struct {
+  int nevents, nparticles;  /* particles per event */
+  double gamma_fraction;    /* reference default 0.5 */
+  double min_p, max_p;      /* MeV; reference default 1 GeV .. 1 TeV */
+  double min_eta, max_eta;  /* reference default -3 .. 3 */
+  double min_phi, max_phi;  /* reference default 0 .. 2 pi */
+  double vertex[3];         /* mm */
+  double seed[6];           /* MRG32k3a stream state */
+  long long first_draw;     /* draws of that stream already used */
+  int first_event;
+} gx_egamma_gun_params;
+int gx_egamma_gun(const gx_egamma_gun_params *p, int *d_type, double *d_E, double *d_pos, double *d_dir,
+                  int *d_event, int *d_pdg, gx_stream_t s);
+/* Particle type of the transport (0 gamma, 1 e-, 2 e+) for a PDG code, -1 for
+ * the particles the EM path does not transport. */
+int gx_pdg_to_type(int pdg);
+/* ProxyHepEvtGenerator::GenerateOneEvent (source/Geant/proxy/src/
+ * ProxyHepEvtGenerator.cpp:48-132) for up to max_events events of a HEPEVT
+ * ASCII file, on the host: per event NHEP, then NHEP lines "ISTHEP IDHEP
+ * JDAHEP1 JDAHEP2 PX PY PZ M" (GeV).  The primaries are the daughters (of an
+ * entry with daughters, status > 0) that have no daughters, in file order;
+ * per primary: event index, PDG code, kinetic energy, unit direction.
+ * GX_MODE_QUIRK reproduces the reference (mass squared, GeV numbers kept as
+ * MeV); GX_MODE_PHYSICS uses the mass as given and converts GeV to MeV.
+ * Daughter indices outside their event are skipped and counted in *bad (the
+ * reference reads out of bounds there).  *n_out = primaries found; if that
+ * exceeds cap, the first cap are stored and GX_ERR_OVERFLOW is returned.
+ * A truncated event ends the read with GX_ERR_DATA. */
+int gx_hepevt_read(const char *path, int mode, int max_events, int cap, int *h_event, int *h_pdg, double *h_E,
+                   double *h_dir, int *n_out, int *nev_out, int *bad_out);
+/* gx_hepevt_read, then the gamma / e- / e+ primaries into device arrays ready
+ * for gx_transport_run (position = vertex, or the origin if null; other
+ * particles are counted in *n_skipped).  Synchronises the stream. */
+int gx_hepevt_load(const char *path, int mode, int max_events, const double vertex[3], int cap, int *d_type,
+                   double *d_E, double *d_pos, double *d_dir, int *d_event, int *n_prim, int *n_events,
+                   int *n_skipped, gx_stream_t s);
+
 /* Launch-setting sweep of the batched engine.  No counterpart in the
  * reference (its kernels take nblocks / nthreads from the caller,
  * source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).  Transports the given

@@ -27,5 +27,7 @@ ${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
   "$SRC/proxy/src/ProxyPhysicsVector.cu" \
   "$SRC/proxy/src/ProxyPhysicsTable.cu" \
   "$SRC/proxy/src/ProxyDataManager.cu" \
+  "$SRC/proxy/src/ProxyEgammaGun.cpp" \
+  "$SRC/proxy/src/ProxyHepEvtGenerator.cpp" \
   -x none "$STDCXX" -lm -o "$OUT/libgxref.so"
 echo "built $OUT/libgxref.so"

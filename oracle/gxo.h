@@ -207,6 +207,16 @@ int gxo_transport_flat(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
                        const int *event, double *edep, int nvol, double *escaped,
                        long long *counters, int *primary_steps);
 
+/* ------------------------------------------------------ event generators */
+/* gxo_events.c: ProxyEgammaGun (proxy/src/ProxyEgammaGun.cpp:35-85) and
+ * ProxyHepEvtGenerator (proxy/src/ProxyHepEvtGenerator.cpp:48-132). */
+int gxo_egamma_gun(gxo_mrg_t *r, int nevents, int nparticles, double gamma_fraction, double minp, double maxp,
+                   double mineta, double maxeta, double minphi, double maxphi, int *pdg, double *p, double *ekin,
+                   double *dir);
+void gxo_egamma_dir(int physics, double x, double y, double z, double *eta, double *phi);
+int gxo_hepevt_read(const char *path, int physics, int max_events, int cap, int *event, int *pdg, double *p,
+                    double *ekin, double *dir, int *nev_read, int *bad);
+
 #ifdef __cplusplus
 }
 #endif

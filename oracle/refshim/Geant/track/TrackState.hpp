@@ -41,6 +41,7 @@ struct TrackPhysicsState {
 };
 struct PhysicsProcessState { double fNumOfInteractLengthLeft = 0; double fPhysicsInteractLength = 0; };
 struct TrackMaterialState { unsigned fMaterialId = 0; Material_t *fMaterial = nullptr; };
+struct TrackSchedulingState { int fGVcode = 0; };
 struct TrackState;
 struct CapturedTrack { long seq; double ekin; double dir[3]; };
 extern thread_local std::vector<CapturedTrack> *gxrefCapture;
@@ -54,6 +55,7 @@ struct TrackState {
   TrackPhysicsState fPhysicsState;
   PhysicsProcessState fPhysicsProcessState[3];
   TrackMaterialState fMaterialState;
+  TrackSchedulingState fSchedulingState;
   TrackState() = default;
   TrackState(const TrackState &) = default;
   TrackState &operator=(const TrackState &) = default;

@@ -21,6 +21,8 @@
 #include "Geant/proxy/ProxySeltzerBerger.hpp"
 #include "Geant/proxy/Proxy2DVector.hpp"
 #include "Geant/random/MRG32k3a.hpp"
+#include "Geant/proxy/ProxyEgammaGun.hpp"
+#include "Geant/proxy/ProxyHepEvtGenerator.hpp"
 
 #include <algorithm>
 #include <cstring>
@@ -261,6 +263,82 @@ void gxref_helix(const double *B, int n, const double *pos, const double *dir, c
     newdir[3 * i + 1] = dy;
     newdir[3 * i + 2] = dz;
   }
+}
+
+} // extern "C"
+
+
+extern "C" {
+
+// ProxyEgammaGun::GenerateOneEvent (proxy/src/ProxyEgammaGun.cpp:43-85), nevents
+// events of nparticles, drawing from the stream state `state` (updated).  Per
+// particle: PDG code, momentum, kinetic energy, direction.
+int gxref_egamma_gun(double *state, int nevents, int nparticles, double gamma_fraction, double minp, double maxp,
+                     double mineta, double maxeta, double minphi, double maxphi, int *pdg, double *p, double *ekin,
+                     double *dir)
+{
+  load_state(state);
+  // the one-argument constructor is ambiguous with the (nevents, nparticles = 1) one
+  ProxyEgammaGun gun(nevents, nparticles);
+  gun.SetGammaFraction(gamma_fraction);
+  gun.SetMomentum(minp, maxp);
+  gun.SetEta(mineta, maxeta);
+  gun.SetPhi(minphi, maxphi);
+  int k = 0;
+  for (int e = 0; e < nevents; ++e) {
+    ProxyEvent *ev = gun.GenerateOneEvent();
+    ProxyVertex *v = (*ev->GetVertexVector())[0];
+    for (int i = 0; i < v->GetNumberOfParticles(); ++i, ++k) {
+      TrackState *t = v->GetParticle(i);
+      t->fCapture = false;
+      pdg[k] = t->fSchedulingState.fGVcode;
+      p[k] = t->fPhysicsState.fMomentum;
+      ekin[k] = t->fPhysicsState.fEkin;
+      for (int j = 0; j < 3; ++j) dir[3 * k + j] = t->fDir.v[j];
+    }
+  }
+  store_state(state);
+  return k;
+}
+
+// ProxyEgammaGun::SetDirectionXYZ (ProxyEgammaGun.cpp:35-41): the direction of
+// a particle generated with the eta and phi it sets (both ranges collapse to
+// one value, so no draw changes it).
+void gxref_egamma_direction(double x, double y, double z, double *dir)
+{
+  ProxyEgammaGun gun(1, 1);
+  gun.SetDirectionXYZ(x, y, z);
+  double st[6] = {12345., 12345., 12345., 12345., 12345., 12345.};
+  load_state(st);
+  ProxyEvent *ev = gun.GenerateOneEvent();
+  TrackState *t = (*ev->GetVertexVector())[0]->GetParticle(0);
+  t->fCapture = false;
+  for (int j = 0; j < 3; ++j) dir[j] = t->fDir.v[j];
+}
+
+// ProxyHepEvtGenerator::GenerateOneEvent (proxy/src/ProxyHepEvtGenerator.cpp:48-132)
+// for max_events events of `path`; per particle: event, PDG code, momentum,
+// kinetic energy, direction.  Returns the number of particles (at most cap).
+int gxref_hepevt(const char *path, int max_events, int cap, int *event, int *pdg, double *p, double *ekin, double *dir)
+{
+  // the path-only constructor leaves the event vector null, which the base
+  // class destructor dereferences; the (nevents, path) one allocates it
+  ProxyHepEvtGenerator gen(max_events, path);
+  int k = 0;
+  for (int e = 0; e < max_events; ++e) {
+    ProxyEvent *ev = gen.GenerateOneEvent();
+    ProxyVertex *v = (*ev->GetVertexVector())[0];
+    for (int i = 0; i < v->GetNumberOfParticles() && k < cap; ++i, ++k) {
+      TrackState *t = v->GetParticle(i);
+      t->fCapture = false;
+      event[k] = e;
+      pdg[k] = t->fSchedulingState.fGVcode;
+      p[k] = t->fPhysicsState.fMomentum;
+      ekin[k] = t->fPhysicsState.fEkin;
+      for (int j = 0; j < 3; ++j) dir[3 * k + j] = t->fDir.v[j];
+    }
+  }
+  return k;
 }
 
 } // extern "C"

@@ -211,6 +211,39 @@ class Oracle:
         res.update(edep=edep, escaped=esc.value, primary_steps=psteps)
         return res
 
+    # ------------------------------------------------------ event generators
+    def egamma_gun(self, state, nevents, nparticles, gamma_fraction, minp, maxp, mineta, maxeta, minphi, maxphi):
+        f = self.lib.gxo_egamma_gun
+        f.restype = I
+        f.argtypes = [C.POINTER(D), I, I] + [D] * 7 + [C.POINTER(I)] + [C.POINTER(D)] * 3
+        st = np.ascontiguousarray(state, dtype=np.float64).copy()
+        n = nevents * nparticles
+        pdg = np.zeros(n, np.int32)
+        p, ek, d = np.zeros(n), np.zeros(n), np.zeros((n, 3))
+        k = f(dp(st), nevents, nparticles, gamma_fraction, minp, maxp, mineta, maxeta, minphi, maxphi, ip(pdg), dp(p),
+              dp(ek), dp(d))
+        assert k == n
+        return pdg, p, ek, d, st
+
+    def egamma_dir(self, physics, x, y, z):
+        f = self.lib.gxo_egamma_dir
+        f.argtypes = [I, D, D, D, C.POINTER(D), C.POINTER(D)]
+        eta, phi = D(), D()
+        f(physics, x, y, z, C.byref(eta), C.byref(phi))
+        return eta.value, phi.value
+
+    def hepevt(self, path, physics, max_events=1 << 30, cap=1 << 20):
+        f = self.lib.gxo_hepevt_read
+        f.restype = I
+        f.argtypes = [C.c_char_p, I, I, I, C.POINTER(I), C.POINTER(I)] + [C.POINTER(D)] * 3 + [C.POINTER(I)] * 2
+        ev, pdg = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        p, ek, d = np.zeros(cap), np.zeros(cap), np.zeros((cap, 3))
+        nev, bad = C.c_int(), C.c_int()
+        k = f(path.encode(), physics, max_events, cap, ip(ev), ip(pdg), dp(p), dp(ek), dp(d), C.byref(nev),
+              C.byref(bad))
+        assert k >= 0
+        return dict(event=ev[:k], pdg=pdg[:k], p=p[:k], ekin=ek[:k], dir=d[:k], nevents=nev.value, bad=bad.value)
+
 
 def oracle_config(cfg, nthreads=8):
     """The oracle's transport configuration for a package TransportConfig."""
@@ -342,3 +375,33 @@ class Reference:
         npos, ndir = np.zeros((n, 3)), np.zeros((n, 3))
         self.lib.gxref_helix(dp(B), n, *[dp(a) for a in args], dp(npos), dp(ndir))
         return npos, ndir
+
+    # ------------------------------------------------------ event generators
+    def egamma_gun(self, state, nevents, nparticles, gamma_fraction, minp, maxp, mineta, maxeta, minphi, maxphi):
+        f = self.lib.gxref_egamma_gun
+        f.restype = I
+        f.argtypes = [C.POINTER(D), I, I] + [D] * 7 + [C.POINTER(I)] + [C.POINTER(D)] * 3
+        st = np.ascontiguousarray(state, dtype=np.float64).copy()
+        n = nevents * nparticles
+        pdg = np.zeros(n, np.int32)
+        p, ek, d = np.zeros(n), np.zeros(n), np.zeros((n, 3))
+        k = f(dp(st), nevents, nparticles, gamma_fraction, minp, maxp, mineta, maxeta, minphi, maxphi, ip(pdg), dp(p),
+              dp(ek), dp(d))
+        assert k == n
+        return pdg, p, ek, d, st
+
+    def egamma_direction(self, x, y, z):
+        f = self.lib.gxref_egamma_direction
+        f.argtypes = [D, D, D, C.POINTER(D)]
+        d = np.zeros(3)
+        f(x, y, z, dp(d))
+        return d
+
+    def hepevt(self, path, max_events, cap=1 << 16):
+        f = self.lib.gxref_hepevt
+        f.restype = I
+        f.argtypes = [C.c_char_p, I, I, C.POINTER(I), C.POINTER(I)] + [C.POINTER(D)] * 3
+        ev, pdg = np.zeros(cap, np.int32), np.zeros(cap, np.int32)
+        p, ek, d = np.zeros(cap), np.zeros(cap), np.zeros((cap, 3))
+        k = f(path.encode(), max_events, cap, ip(ev), ip(pdg), dp(p), dp(ek), dp(d))
+        return dict(event=ev[:k], pdg=pdg[:k], p=p[:k], ekin=ek[:k], dir=d[:k])
