@@ -288,6 +288,14 @@ def main():
         out["primary_step_count_ks_fp32_vs_fp64"] = {"statistic": float(ks.statistic), "pvalue": float(ks.pvalue),
                                                      "mean_fp32": float(p32.mean()), "mean_fp64": float(p64.mean())}
 
+    # the same workload with multiple scattering of e-/e+ switched on
+    # (Urban-type; the reference has none): FP32-mixed batched engine
+    cfg.msc = 1
+    msm, msteps, _, stm = timed(1, 1, 1, 1)
+    cfg.msc = 0
+    out["with_multiple_scattering"] = {"value": msteps / (msm / 1e3), "unit": UNIT, "steps": int(msteps),
+                                       "substeps": int(stm["substeps"]), "ms": msm}
+
     # e2e through the host-buffer entry point (warm-up calls first: the FP64
     # runs above released the FP32 engine's stores)
     cfg.precision, cfg.engine, cfg.profile = 1, 1, 0

@@ -42,7 +42,7 @@ class TransportConfig(C.Structure):
                 ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I), ("Bz", D), ("charged_local", I),
                 ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
-                ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I)]
+                ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I)]
 
 
 class TransportStats(C.Structure):

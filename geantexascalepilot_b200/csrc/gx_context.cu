@@ -176,7 +176,7 @@ static bool read_sandia(const std::string &dir, Data &d, std::vector<double> &bi
 
 // Derived electromagnetic constants, evaluated along the CLHEP definition
 // chain (ProxySystemOfUnits.hpp / ProxyPhysicalConstants.hpp).
-static void em_constants(double *rcl, double *compton_len)
+static void em_constants(double *rcl, double *compton_len, double *alpha)
 {
   const double pi = kPi, eplus = 1., e_SI = 1.602176487e-19;
   const double coulomb = eplus / e_SI, second = 1.e+9, meter = 1000.;
@@ -191,9 +191,31 @@ static void em_constants(double *rcl, double *compton_len)
   const double hbarc = h_Planck / (2 * pi) * c_light;
   *rcl = elm_coupling / kEMass;
   *compton_len = hbarc / kEMass;
+  *alpha = elm_coupling / hbarc;
 }
 
-static void material(Data &d, int m, double Z, double A, double density, double rcl, double lc)
+// Tsai's radiation-length factor of an element (ProxyElementUtils.cu:40-61,
+// its Coulomb correction :24-37), mm^2.
+static double lrad_tsai_factor(double Z, double alpha, double rcl)
+{
+  static const double lrad_light[] = {5.31, 4.79, 4.74, 4.71};
+  static const double lprad_light[] = {6.144, 5.621, 5.805, 5.924};
+  const double logZ3 = std::log(Z) / 3.;
+  double lrad, lprad;
+  const int iz = (int)(Z + 0.5) - 1;
+  if (iz <= 3) {
+    lrad = lrad_light[iz];
+    lprad = lprad_light[iz];
+  } else {
+    lrad = std::log(184.15) - logZ3;
+    lprad = std::log(1194.) - 2 * logZ3;
+  }
+  const double az1 = alpha * Z, az2 = az1 * az1, az4 = az2 * az2;
+  const double fc = (0.0083 * az4 + 0.20206 + 1. / (1. + az2)) * az2 - (0.0020 * az4 + 0.0369) * az4;
+  return 4 * alpha * rcl * rcl * Z * (Z * (lrad - fc) + lprad);
+}
+
+static void material(Data &d, int m, double Z, double A, double density, double rcl, double lc, double alpha)
 {
   const double avogadro = 6.02214179e+23;
   double n_atoms = avogadro * density / A * 1.e-3; // 1/mm3
@@ -201,6 +223,20 @@ static void material(Data &d, int m, double Z, double A, double density, double 
   d.mat_density[m] = density;
   d.mat_nel[m] = Z * n_atoms;
   d.mat_dfactor[m] = d.mat_nel[m] * 4.0 * kPi * rcl * lc * lc; // Migdal constant x n_el
+  // radiation length (ProxyMaterial::ComputeDerivedQuantities, ProxyMaterial.cu:133-150)
+  const double radinv = n_atoms * lrad_tsai_factor(Z, alpha, rcl);
+  // the Urban model's Z-dependent constants: the theta0 correction and the
+  // coefficients of the tail parameter (published with the model)
+  const double z16 = std::exp(std::log(Z) / 6.0), z13 = z16 * z16;
+  const double facz = 0.990395 + z16 * (-0.168386 + z16 * 0.093286);
+  double *c = d.mat_msc[m];
+  c[0] = radinv <= 0.0 ? 1.7976931348623157e308 : 1. / radinv;
+  c[1] = facz * (1.0 - 8.7780e-2 / Z);
+  c[2] = facz * (4.0780e-2 + 1.7315e-4 * Z);
+  c[3] = 2.3785 - z13 * (4.1981e-1 - z13 * 6.3100e-2);
+  c[4] = 4.7526e-1 + z13 * (1.7694 - z13 * 3.3885e-1);
+  c[5] = 2.3683e-1 - z13 * (1.8111 - z13 * 3.2774e-1);
+  c[6] = 1.7888e-2 + z13 * (1.9659e-2 - z13 * 2.6664e-3);
 }
 
 template <class T> static int upload(const std::vector<T> &h, T **d)
@@ -260,12 +296,12 @@ int load_data(const char *datadir, Ctx *ctx)
     return set_error(GX_ERR_DATA, "cannot read Seltzer-Berger tables in %s/brem_SB", datadir);
   std::vector<double> binding, sandia;
   if (!read_sandia(dir, d, binding, sandia)) return set_error(GX_ERR_DATA, "cannot read %s/sandia.dat", datadir);
-  double rcl, lc;
-  em_constants(&rcl, &lc);
+  double rcl, lc, alpha;
+  em_constants(&rcl, &lc, &alpha);
   d.pi_rcl2 = kPi * rcl * rcl;
-  material(d, 0, 1.0, 1.01, 1.e-25, rcl, lc);   // Galactic
-  material(d, 1, 82.0, 207.2, 11.35, rcl, lc);  // G4_Pb
-  material(d, 2, 18.0, 39.95, 1.396, rcl, lc);  // G4_lAr
+  material(d, 0, 1.0, 1.01, 1.e-25, rcl, lc, alpha);   // Galactic
+  material(d, 1, 82.0, 207.2, 11.35, rcl, lc, alpha);  // G4_Pb
+  material(d, 2, 18.0, 39.95, 1.396, rcl, lc, alpha);  // G4_lAr
   double *px, *py, *pd2, *pc64, *pbind, *psandia;
   float *pc32;
   SBTable *psb;

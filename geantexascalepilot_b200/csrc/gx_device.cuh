@@ -155,6 +155,9 @@ struct Data {
   double cut_length[4][kNMat];
   int nshell[101], ishell[101], nint[101], cumint[101];
   double mat_Z[kNMat], mat_density[kNMat], mat_nel[kNMat], mat_dfactor[kNMat];
+  // multiple scattering, per material: radiation length (mm) and the Urban
+  // model's Z-dependent constants {X0, th1, th2, ca, cb, cc, cd}
+  double mat_msc[kNMat][7];
   double pi_rcl2; // pi r_e^2, mm^2
 };
 

@@ -30,6 +30,7 @@ namespace gx {
 template <class R> struct Store {
   double *x, *y, *z;
   R *dx, *dy, *dz, *E, *n0, *n1, *n2;
+  R *r0; // multiple scattering: range scale of the step limit in the current volume (<= 0: unset)
   uint32_t *rng; // 6 planes of cap words
   int *vol, *event, *prim, *type;
   long long cap;
@@ -37,6 +38,7 @@ template <class R> struct Store {
 
 struct Geom {
   int geometry, axis, nlayers, box_mat, charged_local, nvol, nevents;
+  int msc; // multiple scattering of e-/e+
   double t_abs, pitch, x0, total, half_trans, Bz;
   double box_half[3], box_centre[3];
 };
@@ -317,6 +319,7 @@ template <class R> struct Track {
   int type, vol, event, prim;
   double pos[3];
   R dir[3], E, nil[3];
+  R msc_r0; // multiple scattering: range scale of the step limit in this volume (<= 0: unset)
   Mrg rng;
 };
 
@@ -459,6 +462,147 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
   if (io.status == 1) t.E = R(0);
 }
 
+// ------------------------------------------------------- multiple scattering
+// Multiple scattering of e-/e+ (config msc = 1): the Urban model as published
+// (L. Urban, CERN-OPEN-2006-077); the reference has only a placeholder
+// (proxy/ProxyScattering.hpp:53-71) and ships the transport mean free path
+// tables (LambdaMod1.msc: E^2 / lambda1).  The oracle restates the same model
+// in the same order of random draws.
+//   step limit: t <= max(0.04 r0, 0.6 safety, 1e-5 mm), r0 = max(range,
+//     lambda1) at the first step in each volume;
+//   paths: geometric z = lambda1 (1 - exp(-t / lambda1)) from the true length t,
+//     and back when a boundary stops the step;
+//   deflection after the along-step loss: cos(theta) from the model's mixture
+//     of a central exponential part (Highland-type width theta0), a power tail
+//     and a uniform part, weighted so that <cos theta> = exp(-tau); where the
+//     published weights would need a uniform part above 1 it is dropped and
+//     the central / tail split keeps that mean; phi uniform.
+// Not modelled: lateral displacement, the e+ correction of theta0.
+constexpr double kMscFr = 0.04, kMscFs = 0.6, kMscTmin = 1.0e-5;
+constexpr double kMscTauBig = 8.0, kMscTauSmall = 1.0e-16, kMscTauLim = 1.0e-6;
+
+// transport mean free path lambda1 (mm); 0 when the table has nothing
+template <class R> __device__ __forceinline__ R msc_lambda1(const Data &d, int type, int mat, R e)
+{
+  const R v = vec_value_fast<R>(d, d.vec[type == 2 ? GX_LambdaMod1_msc_ep : GX_LambdaMod1_msc_em][mat], e);
+  return v > R(0) ? e * e / v : R(0);
+}
+
+template <class R> __device__ __forceinline__ R msc_expm1(R x);
+template <> __device__ __forceinline__ float msc_expm1(float x) { return expm1f(x); }
+template <> __device__ __forceinline__ double msc_expm1(double x) { return ::expm1(x); }
+template <class R> __device__ __forceinline__ R msc_log1p(R x);
+template <> __device__ __forceinline__ float msc_log1p(float x) { return log1pf(x); }
+template <> __device__ __forceinline__ double msc_log1p(double x) { return ::log1p(x); }
+
+template <class R> __device__ __forceinline__ double msc_true_to_geom(double t, R lam)
+{
+  const R tau = (R)t / lam;
+  return tau < R(kMscTauLim) ? t : -(double)lam * (double)msc_expm1<R>(-tau);
+}
+
+template <class R> __device__ __forceinline__ double msc_geom_to_true(double z, R lam, double tmax)
+{
+  const R x = (R)z / lam;
+  if (x < R(kMscTauLim)) return z;
+  const double t = x < R(1) ? -(double)lam * (double)msc_log1p<R>(-x) : tmax;
+  return t < tmax ? t : tmax;
+}
+
+// the model's two-function form for large angles: exact first and second moments
+template <class R> __device__ __forceinline__ R msc_simple(Mrg &rng, R xm, R x2m)
+{
+  const R a = (R(2) * xm + R(9) * x2m - R(3)) / (R(2) * xm - R(3) * x2m + R(1));
+  const R prob = (a + R(2)) * xm / a;
+  const R r0 = rng.template u<R>(), r1 = rng.template u<R>();
+  if (r0 < prob) return R(-1) + R(2) * M<R>::exp(M<R>::log(r1) / (a + R(1)));
+  return R(-1) + R(2) * r1;
+}
+
+// cos(theta) after a true path t; lam0 / lam1 and e0 / e1 at the start and
+// the end of the step; c = the material's constants {X0, th1, th2, ca..cd}
+template <class R>
+__device__ __forceinline__ R msc_cos_theta(Mrg &rng, const double *c, R t, R lam0, R lam1, R e0, R e1)
+{
+  R tau = t / lam0;
+  if (lam1 > R(0) && fabs(lam1 - lam0) > R(0.01) * lam0) tau = t * M<R>::log(lam0 / lam1) / (lam0 - lam1);
+  if (tau >= R(kMscTauBig)) return R(-1) + R(2) * rng.template u<R>();
+  if (tau < R(kMscTauSmall)) return R(1);
+  R xm, x2m;
+  if (tau < R(0.01)) {
+    xm = R(1) - tau * (R(1) - R(0.5) * tau);
+    x2m = R(1) - tau * (R(5) - R(6.25) * tau) / R(3);
+  } else {
+    xm = M<R>::exp(-tau);
+    x2m = (R(1) + R(2) * M<R>::exp(R(-2.5) * tau)) / R(3);
+  }
+  if (R(1) - e1 / e0 > R(0.5)) return msc_simple<R>(rng, xm, x2m);
+  const R m = R(kEMass);
+  const R inv0 = (e0 + m) / (e0 * (e0 + R(2) * m)), inv1 = (e1 + m) / (e1 * (e1 + R(2) * m));
+  const R X0 = (R)c[0], y = t / X0;
+  const R th0 = R(13.6) * M<R>::sqrt(y) * M<R>::sqrt(inv0 * inv1) * ((R)c[1] + (R)c[2] * M<R>::log(y));
+  const R th2 = th0 * th0;
+  if (th2 < R(kMscTauSmall)) return R(1);
+  if (th0 > R(kPi / 6)) return msc_simple<R>(rng, xm, x2m);
+  R x = th2 * (R(1) - th2 / R(12));
+  if (th2 > R(0.01)) {
+    const R s = R(2) * sin(R(0.5) * th0);
+    x = s * s;
+  }
+  const R u = M<R>::exp(M<R>::log(tau) / R(6));
+  R xsi = (R)c[3] + u * ((R)c[4] + (R)c[5] * u) + (R)c[6] * M<R>::log((t / tau) / X0);
+  if (xsi < R(1.9)) xsi = R(1.9);
+  R cc = xsi;
+  if (fabs(cc - R(3)) < R(0.001))
+    cc = R(3.001);
+  else if (fabs(cc - R(2)) < R(0.001))
+    cc = R(2.001);
+  const R c1 = cc - R(1);
+  const R ea = M<R>::exp(-xsi), eaa = R(1) - ea;
+  const R xmean1 = R(1) - (R(1) - (R(1) + xsi) * ea) * x / eaa;
+  if (xmean1 <= R(0.999) * xm) return msc_simple<R>(rng, xm, x2m);
+  const R x0 = R(1) - xsi * x;
+  const R b = R(1) + (cc - xsi) * x, b1 = b + R(1), bx = cc * x;
+  const R dd = M<R>::exp(c1 * M<R>::log(bx)) / M<R>::exp(c1 * M<R>::log(b1));
+  const R xmean2 = (x0 + dd - (bx - b1 * dd) / (cc - R(2))) / (R(1) - dd);
+  const R f1x0 = ea / eaa, f2x0 = c1 / (cc * (R(1) - dd));
+  R prob = f2x0 / (f1x0 + f2x0);
+  R qprob = xm / (prob * xmean1 + (R(1) - prob) * xmean2);
+  if (qprob > R(1)) {
+    qprob = R(1);
+    prob = (xm - xmean2) / (xmean1 - xmean2);
+  }
+  const R r0 = rng.template u<R>(), r1 = rng.template u<R>();
+  if (r0 < qprob) {
+    if (r1 < prob) return R(1) + M<R>::log(ea + rng.template u<R>() * eaa) * x;
+    R var = (R(1) - dd) * rng.template u<R>();
+    if (var < R(0.01) * dd) {
+      var /= dd * c1;
+      return R(-1) + var * (R(1) - R(0.5) * var * cc) * (R(2) + (cc - xsi) * x);
+    }
+    return R(1) + x * (cc - xsi - cc * M<R>::exp(-M<R>::log(var + dd) / c1));
+  }
+  return R(-1) + R(2) * r1;
+}
+
+// deflect the direction by the sampled angle (no draw for phi when it is 0)
+template <class R>
+__device__ __forceinline__ void msc_deflect(const Data &d, Track<R> &t, int mat, R step, R lam0, R e0)
+{
+  const R lam1 = msc_lambda1<R>(d, t.type, mat, t.E);
+  R ct = msc_cos_theta<R>(t.rng, d.mat_msc[mat], step, lam0, lam1, e0, t.E);
+  if (!(ct < R(1))) return;
+  if (ct < R(-1)) ct = R(-1);
+  const R st = M<R>::sqrt((R(1) - ct) * (R(1) + ct));
+  R sp, cp;
+  M<R>::sincos2pi(t.rng.template u<R>(), &sp, &cp);
+  R u = st * cp, v = st * sp, w = ct;
+  rotate_to_lab(u, v, w, t.dir[0], t.dir[1], t.dir[2]);
+  t.dir[0] = u;
+  t.dir[1] = v;
+  t.dir[2] = w;
+}
+
 enum { kDone = 0, kAlive = 1, kInteract = 2 };
 
 // One OneStep (test_BasicCpuTransport.cpp:408-497 / InnerStep :358-403) in
@@ -480,6 +624,10 @@ template <class R> struct StepCtx {
   int newvol;       // volume entered (-2: sub-step cap hit)
   int nsub;         // helix sub-steps taken
   bool crossed;     // the step ended on a boundary
+  // multiple scattering (lam0 > 0 when it applies to this step): transport
+  // mean free path and energy at the start, the step's true length
+  R lam0, e0;
+  double ttrue;
   __device__ __forceinline__ R xs(int i) const { return i == 0 ? xs0 : (i == 1 ? xs1 : xs2); }
 };
 
@@ -517,6 +665,28 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
     if (slim < pstep) {
       pstep = slim;
       sel = -1;
+    }
+  }
+  // multiple scattering: its step limit, then the true step becomes the
+  // geometric length to move
+  c.lam0 = R(0);
+  c.e0 = t.E;
+  if (charged && g.msc) {
+    const R lam0 = msc_lambda1<R>(d, t.type, mat, t.E);
+    if (t.msc_r0 <= R(0)) {
+      R range = vec_value_fast<R>(d, d.vec[t.type == 2 ? GX_Range_ep : GX_Range_em][mat], t.E);
+      if (t.E < R(kMinE)) range *= t.E / R(kMinE);
+      t.msc_r0 = range > lam0 ? range : lam0;
+    }
+    const double tlim = fmax(fmax(kMscFr * (double)t.msc_r0, kMscFs * safety(g, t.vol, t.pos)), kMscTmin);
+    if (tlim < (double)pstep) {
+      pstep = (R)tlim;
+      sel = -1;
+    }
+    c.ttrue = (double)pstep;
+    if (lam0 > R(0)) {
+      c.lam0 = lam0;
+      pstep = (R)msc_true_to_geom<R>((double)pstep, lam0);
     }
   }
   c.sel = sel;
@@ -619,7 +789,9 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
                                         int *proc)
 {
   const int np = (t.type == 1) ? 2 : 3;
-  const double step = c.total;
+  // the true length of the step: all of it, or back from where a boundary
+  // stopped it
+  const double step = c.lam0 > R(0) ? (c.crossed ? msc_geom_to_true<R>(c.total, c.lam0, c.ttrue) : c.ttrue) : c.total;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
     if (i < np) t.nil[i] -= (R)step * c.xs(i);
@@ -644,8 +816,10 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
       }
       return kDone;
     }
+    if (c.lam0 > R(0)) msc_deflect<R>(d, t, vol_material(g, c.vol0), (R)step, c.lam0, c.e0);
   }
   if (c.crossed) {
+    t.msc_r0 = R(-1); // a new volume: the step limit starts again
     t.vol = c.newvol;
     if (c.newvol < 0) {
       L.escaped += (double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0);
@@ -703,6 +877,7 @@ template <class R> __device__ __forceinline__ void load_track(const Store<R> &s,
   t.nil[0] = s.n0[i];
   t.nil[1] = s.n1[i];
   t.nil[2] = s.n2[i];
+  t.msc_r0 = s.r0[i];
   t.rng.load(s.rng, s.cap, i);
   t.vol = s.vol[i];
   t.event = s.event[i];
@@ -721,6 +896,7 @@ template <class R> __device__ __forceinline__ void store_track(const Store<R> &s
   s.n0[i] = t.nil[0];
   s.n1[i] = t.nil[1];
   s.n2[i] = t.nil[2];
+  s.r0[i] = t.msc_r0;
   t.rng.store(s.rng, s.cap, i);
   s.vol[i] = t.vol;
   s.event[i] = t.event;
@@ -856,6 +1032,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
     c.dir[2] = sec.dir[k][2];
     c.E = sec.E[k];
     c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
+    c.msc_r0 = R(-1);
     t.rng.seed_child(c.rng);
     c.vol = t.vol;
     c.event = t.event;
@@ -1206,6 +1383,7 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
     double dd[3] = {a.p.dir[3 * pi], a.p.dir[3 * pi + 1], a.p.dir[3 * pi + 2]};
     t.vol = locate(a.g, t.pos, dd);
     t.nil[0] = t.nil[1] = t.nil[2] = R(-1);
+    t.msc_r0 = R(-1);
     t.event = a.p.event ? a.p.event[pi] : 0;
     t.prim = (int)pi;
     unsigned long long kk = (unsigned long long)(a.p.first_substream + pi);
@@ -1292,6 +1470,7 @@ template <class R> static Store<R> carve(uintptr_t base, size_t &off, long long 
   s.n0 = (R *)take(cap * sizeof(R));
   s.n1 = (R *)take(cap * sizeof(R));
   s.n2 = (R *)take(cap * sizeof(R));
+  s.r0 = (R *)take(cap * sizeof(R));
   s.rng = (uint32_t *)take(6 * cap * sizeof(uint32_t));
   s.vol = (int *)take(cap * sizeof(int));
   s.event = (int *)take(cap * sizeof(int));
@@ -1472,6 +1651,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   g.total = cfg->nlayers * g.pitch;
   g.half_trans = cfg->half_trans;
   g.Bz = cfg->Bz;
+  g.msc = cfg->msc;
   for (int k = 0; k < 3; ++k) {
     g.box_half[k] = cfg->box_half[k];
     g.box_centre[k] = cfg->box_centre[k];
@@ -1646,7 +1826,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       stats->transport_written[q] = (long long)c.stat[S_TWRITE0 + q];
       stats->transport_queued[q] = (long long)c.stat[S_TQUEUE0 + q];
     }
-    stats->bytes_per_track = (long long)(3 * sizeof(double) + 7 * sizeof(R) + 6 * sizeof(uint32_t) +
+    stats->bytes_per_track = (long long)(3 * sizeof(double) + 8 * sizeof(R) + 6 * sizeof(uint32_t) +
                                          3 * sizeof(int) + (batched ? 0 : sizeof(int)));
   }
   if (c.err_flags & kErrOverflow) return set_error(GX_ERR_OVERFLOW, "transport: track stores and stacks full");
@@ -1775,7 +1955,7 @@ namespace gx {
 
 constexpr long long kNoallocCapacity = 16384;
 constexpr int kNoallocMaxPrimaries = 4096;
-constexpr size_t kNoallocStoreBytes = 120 * (size_t)kNoallocCapacity; // FP64 record with type field
+constexpr size_t kNoallocStoreBytes = 128 * (size_t)kNoallocCapacity; // FP64 record with type field
 constexpr size_t kNoallocCtlBytes = 4096;
 constexpr size_t kNoallocCumEBytes = sizeof(double) * kNoallocMaxPrimaries;
 constexpr size_t kNoallocJumpBytes = sizeof(uint64_t) * 2 * 64 * 9;
@@ -1881,6 +2061,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   g.total = cfg->nlayers * g.pitch;
   g.half_trans = cfg->half_trans;
   g.Bz = cfg->Bz;
+  g.msc = cfg->msc;
   for (int k = 0; k < 3; ++k) {
     g.box_half[k] = cfg->box_half[k];
     g.box_centre[k] = cfg->box_centre[k];
@@ -1948,7 +2129,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
     stats->peak_in_flight = hc.peak;
     stats->tracks_read[0] = (long long)hc.stat[S_READ0];
     stats->tracks_written[0] = (long long)hc.stat[S_WRITE0];
-    stats->bytes_per_track = 120;
+    stats->bytes_per_track = 128;
   }
   if (hc.err_flags & kErrOverflow)
     return set_error(GX_ERR_OVERFLOW, "gx_transport_run_noalloc: more than %lld tracks in flight and deferred",

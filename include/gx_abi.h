@@ -171,6 +171,9 @@ typedef struct {
   double wave_energy;      /* primary energy (MeV) injected per wave, at most (0: from capacity) */
   int steps_per_launch;    /* batched engine: steps of one track per transport launch, at most; a track
                               stays in registers between them (0: default 16; 1: one step per iteration) */
+  int msc;                 /* 1: multiple scattering of e-/e+ (Urban-type: safety-based step limit, true /
+                              geometric path conversion, angular deflection; no lateral displacement);
+                              0: off (the reference has none, proxy/ProxyScattering.hpp:53-71) */
 } gx_transport_config;
 
 typedef struct {
@@ -296,7 +299,7 @@ int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, cons
  * memory, a process held to a fixed memory budget, or a time-critical loop
  * that cannot take the implicit device synchronisation of cudaMalloc /
  * cudaFree.  The plain FP64 loop runs on a static device array owned by the
- * library (about 5.7 MB, held on every device that loads the library until the
+ * library (about 6.3 MB, held on every device that loads the library until the
  * process exits): at most GX_NOALLOC_MAX_PRIMARIES primaries per call, at most
  * GX_NOALLOC_CAPACITY tracks in flight plus as many deferred; larger inputs
  * are rejected with GX_ERR_ARG and a message.  precision must be 0 (FP64);

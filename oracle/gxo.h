@@ -92,6 +92,7 @@ typedef struct {
   double n_atoms;        /* 1/mm3 */
   double n_el;           /* electrons / mm3 */
   double density_factor; /* Migdal constant x electron density (MeV^-2 scale) */
+  double radlen;         /* radiation length, mm (ProxyMaterial.cu:133-150) */
 } gxo_material_t;
 void gxo_material_make(double Z, double A, double density, gxo_material_t *m);
 
@@ -178,6 +179,7 @@ typedef struct {
   long first_substream;    /* substream index of primary 0 */
   int nthreads;
   int score_events;        /* number of event tallies (>=1) */
+  int msc;                 /* 1: multiple scattering of e-/e+ (gxo_transport.c) */
 } gxo_config_t;
 
 typedef struct {
@@ -206,6 +208,13 @@ int gxo_transport_flat(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
                        const int *type, const double *E, const double *pos, const double *dir,
                        const int *event, double *edep, int nvol, double *escaped,
                        long long *counters, int *primary_steps);
+
+/* multiple scattering (gxo_transport.c), test front ends */
+void gxo_msc_cos_batch(double Z, double X0, int n, double *states, double t, double lam0, double lam1, double e0,
+                       double e1, double *out);
+double gxo_msc_lambda1(const gxo_data_t *d, int type, int mat, double e);
+double gxo_msc_true_to_geom(double t, double lam);
+double gxo_msc_geom_to_true(double z, double lam, double tmax);
 
 /* ------------------------------------------------------ event generators */
 /* gxo_events.c: ProxyEgammaGun (proxy/src/ProxyEgammaGun.cpp:35-85) and

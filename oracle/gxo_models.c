@@ -26,7 +26,7 @@
 #define EV 1.e-6
 #define TEV 1.e+6
 #define EMASS 0.510998910
-static double g_rcl = 0, g_twopi_mc2_rcl2 = 0, g_pi_rcl2 = 0, g_compton_len = 0;
+static double g_rcl = 0, g_twopi_mc2_rcl2 = 0, g_pi_rcl2 = 0, g_compton_len = 0, g_alpha = 0;
 static void init_constants(void)
 {
   if (g_rcl != 0) return;
@@ -47,6 +47,28 @@ static void init_constants(void)
   g_twopi_mc2_rcl2 = TWOPI * EMASS * g_rcl * g_rcl;
   g_pi_rcl2 = PI * g_rcl * g_rcl;
   g_compton_len = hbarc / EMASS;
+  g_alpha = elm_coupling / hbarc;
+}
+
+/* Tsai's radiation-length factor of an element (ProxyElementUtils.cu:40-61,
+ * with its Coulomb correction ComputeCoulombFactor, :24-37). */
+static double lrad_tsai_factor(double Z)
+{
+  static const double lrad_light[] = {5.31, 4.79, 4.74, 4.71};
+  static const double lprad_light[] = {6.144, 5.621, 5.805, 5.924};
+  double logZ3 = log(Z) / 3.;
+  double lrad, lprad;
+  int iz = (int)(Z + 0.5) - 1;
+  if (iz <= 3) {
+    lrad = lrad_light[iz];
+    lprad = lprad_light[iz];
+  } else {
+    lrad = log(184.15) - logZ3;
+    lprad = log(1194.) - 2 * logZ3;
+  }
+  double az1 = g_alpha * Z, az2 = az1 * az1, az4 = az2 * az2;
+  double fc = (0.0083 * az4 + 0.20206 + 1. / (1. + az2)) * az2 - (0.0020 * az4 + 0.0369) * az4;
+  return 4 * g_alpha * g_rcl * g_rcl * Z * (Z * (lrad - fc) + lprad);
 }
 
 /* Math::RotateToLabFrame, source/Geant/core/math_wrappers.hpp:194-212 */
@@ -588,6 +610,8 @@ void gxo_material_make(double Z, double A, double density, gxo_material_t *m)
   m->n_el = Z * m->n_atoms;
   double migdal = 4.0 * PI * g_rcl * g_compton_len * g_compton_len;
   m->density_factor = m->n_el * migdal;
+  double radinv = m->n_atoms * lrad_tsai_factor(Z);
+  m->radlen = radinv <= 0.0 ? DBL_MAX : 1. / radinv;
 }
 
 /* ------------------------------------------------------- batch front end */

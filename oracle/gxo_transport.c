@@ -31,6 +31,8 @@
 
 #define EMASS 0.510998910
 #define MINE 1.0e-4 /* 100 eV: the models' low-energy limit used as minE */
+#define PI 3.14159265358979323846
+#define TWOPI (2 * PI)
 
 typedef struct {
   int type;
@@ -39,7 +41,8 @@ typedef struct {
   double nil[3];
   gxo_mrg_t rng;
   int event;
-  int primary; /* index of the primary if this is the primary track, else -1 */
+  int primary;   /* index of the primary if this is the primary track, else -1 */
+  double msc_r0; /* multiple scattering: range scale of the step limit in this volume (<= 0: unset) */
 } track_t;
 
 typedef struct {
@@ -61,6 +64,7 @@ typedef struct {
   const gxo_config_t *c;
   gxo_material_t mat[3];
   double pitch;
+  struct msc_mat { double X0, th1, th2, ca, cb, cc, cd; } msc[3];
 } world_t;
 
 /* ---------------------------------------------------------------- geometry */
@@ -251,6 +255,170 @@ static void cross_sections(const world_t *w, int type, int mat, double e, double
 
 static int nproc(int type) { return type == 1 ? 2 : 3; }
 
+/* ------------------------------------------------------ multiple scattering
+ * Multiple scattering of e-/e+ (physics mode, config msc = 1): the Urban
+ * model as published (L. Urban, CERN-OPEN-2006-077): the reference has only a
+ * placeholder (proxy/ProxyScattering.hpp:53-71); it ships the transport mean
+ * free path tables (LambdaMod1.msc.e-/e+: E^2 / lambda1, MeV^2 / mm).
+ *   step limit: t <= max(MSC_FR r0, MSC_FS safety, MSC_TMIN), r0 = max(range,
+ *     lambda1) taken at the first step in each volume (safety-based stepping);
+ *   path lengths: geometric z = lambda1 (1 - exp(-t / lambda1)) from the true
+ *     length t, and back when a boundary stops the step;
+ *   deflection after the along-step loss: cos(theta) from the model's mixture
+ *     (a central exponential part with the Highland-type width theta0, a power
+ *     tail, a uniform part), normalised so that <cos theta> = exp(-tau),
+ *     tau = t / lambda1 (averaged over the loss); phi uniform.  Where the
+ *     published weights would need a uniform part above 1, the uniform part is
+ *     dropped and the central/tail split set to keep that mean (a choice of
+ *     this restatement).
+ * Not modelled: lateral displacement, the e+ correction of theta0. */
+#define MSC_FR 0.04
+#define MSC_FS 0.6
+#define MSC_TMIN 1.0e-5
+#define MSC_TAUBIG 8.0
+#define MSC_TAUSMALL 1.0e-16
+#define MSC_TAULIM 1.0e-6
+
+/* Z-dependent constants of the model: the theta0 correction and the tail
+ * parameter's coefficients. */
+static void msc_material(double Z, double X0, struct msc_mat *m)
+{
+  double z16 = exp(log(Z) / 6.0), z13 = z16 * z16;
+  double facz = 0.990395 + z16 * (-0.168386 + z16 * 0.093286);
+  m->X0 = X0;
+  m->th1 = facz * (1.0 - 8.7780e-2 / Z);
+  m->th2 = facz * (4.0780e-2 + 1.7315e-4 * Z);
+  m->ca = 2.3785 - z13 * (4.1981e-1 - z13 * 6.3100e-2);
+  m->cb = 4.7526e-1 + z13 * (1.7694 - z13 * 3.3885e-1);
+  m->cc = 2.3683e-1 - z13 * (1.8111 - z13 * 3.2774e-1);
+  m->cd = 1.7888e-2 + z13 * (1.9659e-2 - z13 * 2.6664e-3);
+}
+
+/* transport mean free path lambda1 (mm); 0 when the table has nothing */
+static double msc_lambda1(const world_t *w, int type, int mat, double e)
+{
+  const gxo_pvec_t *v = &w->d->vec[type == 2 ? GXO_LambdaMod1_msc_ep : GXO_LambdaMod1_msc_em][mat];
+  double t = gxo_pvec_value(v, e);
+  return t > 0.0 ? e * e / t : 0.0;
+}
+
+static double msc_range(const world_t *w, int type, int mat, double e)
+{
+  double r = gxo_table_value(w->d, type == 2 ? GXO_Range_ep : GXO_Range_em, mat, e);
+  if (e < MINE) r *= e / MINE;
+  return r;
+}
+
+static double msc_true_to_geom(double t, double lam)
+{
+  double tau = t / lam;
+  return tau < MSC_TAULIM ? t : -lam * expm1(-tau);
+}
+
+static double msc_geom_to_true(double z, double lam, double tmax)
+{
+  double x = z / lam;
+  if (x < MSC_TAULIM) return z;
+  double t = x < 1.0 ? -lam * log1p(-x) : tmax;
+  return t < tmax ? t : tmax;
+}
+
+/* the model's two-function form for large angles: exact first and second moments */
+static double msc_simple(gxo_mrg_t *r, double xm, double x2m)
+{
+  double a = (2 * xm + 9 * x2m - 3) / (2 * xm - 3 * x2m + 1);
+  double prob = (a + 2) * xm / a;
+  double r0 = gxo_mrg_u01(r), r1 = gxo_mrg_u01(r);
+  if (r0 < prob) return -1 + 2 * exp(log(r1) / (a + 1));
+  return -1 + 2 * r1;
+}
+
+/* cos(theta) after a true path t; lam0 / lam1 and e0 / e1 at the start and
+ * the end of the step */
+static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, double lam0, double lam1, double e0,
+                            double e1)
+{
+  double tau = t / lam0;
+  if (lam1 > 0.0 && fabs(lam1 - lam0) > 0.01 * lam0) tau = t * log(lam0 / lam1) / (lam0 - lam1);
+  if (tau >= MSC_TAUBIG) return -1 + 2 * gxo_mrg_u01(r);
+  if (tau < MSC_TAUSMALL) return 1.0;
+  double xm, x2m;
+  if (tau < 0.01) {
+    xm = 1 - tau * (1 - 0.5 * tau);
+    x2m = 1 - tau * (5 - 6.25 * tau) / 3;
+  } else {
+    xm = exp(-tau);
+    x2m = (1 + 2 * exp(-2.5 * tau)) / 3;
+  }
+  if (1.0 - e1 / e0 > 0.5) return msc_simple(r, xm, x2m);
+  /* Highland-type width with the model's Z-dependent correction; 1 / (beta c p)
+   * taken at the geometric mean of the start and end energies */
+  double inv0 = (e0 + EMASS) / (e0 * (e0 + 2 * EMASS)), inv1 = (e1 + EMASS) / (e1 * (e1 + 2 * EMASS));
+  double y = t / m->X0;
+  double th0 = 13.6 * sqrt(y) * sqrt(inv0 * inv1) * (m->th1 + m->th2 * log(y));
+  double th2 = th0 * th0;
+  if (th2 < MSC_TAUSMALL) return 1.0;
+  if (th0 > PI / 6) return msc_simple(r, xm, x2m);
+  double x = th2 * (1 - th2 / 12);
+  if (th2 > 0.01) {
+    double s = 2 * sin(0.5 * th0);
+    x = s * s;
+  }
+  double u = exp(log(tau) / 6);
+  double xsi = m->ca + u * (m->cb + m->cc * u) + m->cd * log((t / tau) / m->X0);
+  if (xsi < 1.9) xsi = 1.9;
+  double c = xsi;
+  if (fabs(c - 3) < 0.001)
+    c = 3.001;
+  else if (fabs(c - 2) < 0.001)
+    c = 2.001;
+  double c1 = c - 1;
+  double ea = exp(-xsi), eaa = 1 - ea;
+  double xmean1 = 1 - (1 - (1 + xsi) * ea) * x / eaa;
+  if (xmean1 <= 0.999 * xm) return msc_simple(r, xm, x2m);
+  double x0 = 1 - xsi * x;
+  double b = 1 + (c - xsi) * x, b1 = b + 1, bx = c * x;
+  double d = exp(c1 * log(bx)) / exp(c1 * log(b1));
+  double xmean2 = (x0 + d - (bx - b1 * d) / (c - 2)) / (1 - d);
+  double f1x0 = ea / eaa, f2x0 = c1 / (c * (1 - d));
+  double prob = f2x0 / (f1x0 + f2x0);
+  double qprob = xm / (prob * xmean1 + (1 - prob) * xmean2);
+  if (qprob > 1.0) {
+    /* the published normalisation would need a negative uniform part: keep
+     * q = 1 and move weight from the tail to the central part so that
+     * <cos theta> = exp(-tau) still holds (xmean2 < xm < xmean1 here) */
+    qprob = 1.0;
+    prob = (xm - xmean2) / (xmean1 - xmean2);
+  }
+  double r0 = gxo_mrg_u01(r), r1 = gxo_mrg_u01(r);
+  if (r0 < qprob) {
+    if (r1 < prob) return 1 + log(ea + gxo_mrg_u01(r) * eaa) * x;
+    double var = (1 - d) * gxo_mrg_u01(r);
+    if (var < 0.01 * d) {
+      var /= d * c1;
+      return -1 + var * (1 - 0.5 * var * c) * (2 + (c - xsi) * x);
+    }
+    return 1 + x * (c - xsi - c * exp(-log(var + d) / c1));
+  }
+  return -1 + 2 * r1;
+}
+
+/* deflect the direction by the sampled angle (no draw for phi when it is 0) */
+static void msc_deflect(const world_t *w, track_t *tr, int mat, double t, double lam0, double e0)
+{
+  double lam1 = msc_lambda1(w, tr->type, mat, tr->E);
+  double ct = msc_cos_theta(&tr->rng, &w->msc[mat], t, lam0, lam1, e0, tr->E);
+  if (ct >= 1.0) return;
+  if (ct < -1.0) ct = -1.0;
+  double st = sqrt((1 - ct) * (1 + ct));
+  double phi = TWOPI * gxo_mrg_u01(&tr->rng);
+  double u = st * cos(phi), v = st * sin(phi), z = ct;
+  gxo_rotate_to_lab(&u, &v, &z, tr->dir[0], tr->dir[1], tr->dir[2]);
+  tr->dir[0] = u;
+  tr->dir[1] = v;
+  tr->dir[2] = z;
+}
+
 /* ---------------------------------------------------------- one track step */
 typedef struct {
   double *edep; /* [events][nvol] */
@@ -282,6 +450,7 @@ static void make_secondary(const world_t *w, track_t *parent, stack_t *st, tally
   }
   s.vol = parent->vol;
   s.nil[0] = s.nil[1] = s.nil[2] = -1.0;
+  s.msc_r0 = -1.0;
   gxo_mrg_seed_child(&parent->rng, &s.rng);
   s.event = parent->event;
   s.primary = -1;
@@ -420,6 +589,21 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
       sel = -1;
     }
   }
+  /* multiple scattering: its step limit, then the true step pstep becomes the
+   * geometric length to move */
+  const int msc = charged && w->c->msc;
+  double lam0 = 0.0, ttrue = 0.0, e0 = tr->E;
+  if (msc) {
+    lam0 = msc_lambda1(w, tr->type, mat, tr->E);
+    if (tr->msc_r0 <= 0.0) tr->msc_r0 = fmax(msc_range(w, tr->type, mat, tr->E), lam0);
+    double tlim = fmax(fmax(MSC_FR * tr->msc_r0, MSC_FS * safety(w, tr->vol, tr->pos)), MSC_TMIN);
+    if (tlim < pstep) {
+      pstep = tlim;
+      sel = -1;
+    }
+    ttrue = pstep;
+    if (lam0 > 0.0) pstep = msc_true_to_geom(pstep, lam0);
+  }
   int vol0 = tr->vol, crossed = 0, newvol = tr->vol;
   double step;
   if (!charged || w->c->Bz == 0.0) {
@@ -442,6 +626,9 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
   } else {
     step = field_propagate(w, tr, pstep, &crossed, &newvol, t);
   }
+  /* the true length of the step: all of it, or back from where a boundary
+   * stopped it */
+  if (msc && lam0 > 0.0) step = crossed ? msc_geom_to_true(step, lam0, ttrue) : ttrue;
   for (int i = 0; i < np; ++i) tr->nil[i] -= step * xs[i];
   t->steps++;
   if (newvol == -2) { /* stuck in field: deposit and stop */
@@ -466,8 +653,10 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
       }
       return 0;
     }
+    if (msc && lam0 > 0.0) msc_deflect(w, tr, mat, step, lam0, e0);
   }
   if (crossed) {
+    tr->msc_r0 = -1.0; /* a new volume: the step limit starts again */
     tr->vol = newvol;
     if (newvol < 0) {
       t->escaped += tr->E;
@@ -483,6 +672,31 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
   }
   return 1;
 }
+
+/* test front ends of the multiple-scattering model */
+void gxo_msc_cos_batch(double Z, double X0, int n, double *states, double t, double lam0, double lam1, double e0,
+                       double e1, double *out)
+{
+  struct msc_mat m;
+  msc_material(Z, X0, &m);
+  for (int i = 0; i < n; ++i) {
+    gxo_mrg_t r;
+    memcpy(r.s, &states[6 * i], sizeof(r.s));
+    out[i] = msc_cos_theta(&r, &m, t, lam0, lam1, e0, e1);
+    memcpy(&states[6 * i], r.s, sizeof(r.s));
+  }
+}
+
+double gxo_msc_lambda1(const gxo_data_t *d, int type, int mat, double e)
+{
+  world_t w;
+  memset(&w, 0, sizeof(w));
+  w.d = d;
+  return msc_lambda1(&w, type, mat, e);
+}
+
+double gxo_msc_true_to_geom(double t, double lam) { return msc_true_to_geom(t, lam); }
+double gxo_msc_geom_to_true(double z, double lam, double tmax) { return msc_geom_to_true(z, lam, tmax); }
 
 /* -------------------------------------------------------------- runner */
 typedef struct {
@@ -509,6 +723,7 @@ static void *worker(void *arg)
     memcpy(tr.dir, pr->dir, sizeof(tr.dir));
     tr.vol = locate(w, tr.pos, tr.dir);
     tr.nil[0] = tr.nil[1] = tr.nil[2] = -1.0;
+    tr.msc_r0 = -1.0;
     gxo_mrg_substreams(w->c->seed, w->c->first_substream + i, 1, tr.rng.s);
     tr.event = pr->event;
     tr.primary = i;
@@ -546,6 +761,7 @@ int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const
   gxo_material_make(1.0, 1.01, 1.e-25, &w.mat[0]);
   gxo_material_make(82.0, 207.2, 11.35, &w.mat[1]);
   gxo_material_make(18.0, 39.95, 1.396, &w.mat[2]);
+  for (int m = 0; m < 3; ++m) msc_material(w.mat[m].Z, w.mat[m].radlen, &w.msc[m]);
   int nt = cfg->nthreads > 0 ? cfg->nthreads : 1;
   int nvol = res->nvol;
   int nev = cfg->score_events > 0 ? cfg->score_events : 1;

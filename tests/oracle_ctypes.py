@@ -45,7 +45,7 @@ class Config(C.Structure):
     _fields_ = [("geometry", I), ("axis", I), ("nlayers", I), ("t_abs", D), ("t_gap", D),
                 ("half_trans", D), ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I),
                 ("Bz", D), ("charged_local", I), ("max_steps", I), ("seed", D * 6),
-                ("first_substream", L), ("nthreads", I), ("score_events", I)]
+                ("first_substream", L), ("nthreads", I), ("score_events", I), ("msc", I)]
 
 
 MODEL_IDS = {"kn": 0, "sg": 1, "bh": 2, "sb": 3, "mb": 4, "bhabha": 5, "annih": 6}
@@ -211,6 +211,36 @@ class Oracle:
         res.update(edep=edep, escaped=esc.value, primary_steps=psteps)
         return res
 
+    # --------------------------------------------------- multiple scattering
+    def material(self, Z, A, density):
+        """gxo_material_t fields (Z, A, density, n_atoms, n_el, density_factor, radlen)"""
+        buf = (D * 7)()
+        self.lib.gxo_material_make.argtypes = [D, D, D, C.c_void_p]
+        self.lib.gxo_material_make(Z, A, density, C.cast(buf, C.c_void_p))
+        return dict(zip(("Z", "A", "density", "n_atoms", "n_el", "density_factor", "radlen"), list(buf)))
+
+    def msc_cos(self, Z, X0, states, t, lam0, lam1, e0, e1):
+        f = self.lib.gxo_msc_cos_batch
+        f.argtypes = [D, D, I, C.POINTER(D)] + [D] * 5 + [C.POINTER(D)]
+        st = np.ascontiguousarray(states, dtype=np.float64).copy()
+        out = np.zeros(len(st))
+        f(Z, X0, len(st), dp(st), t, lam0, lam1, e0, e1, dp(out))
+        return out, st
+
+    def msc_lambda1(self, type_, mat, e):
+        f = self.lib.gxo_msc_lambda1
+        f.restype = D
+        f.argtypes = [P, I, I, D]
+        return f(self.data, type_, mat, e)
+
+    def msc_paths(self, t, lam):
+        f, g = self.lib.gxo_msc_true_to_geom, self.lib.gxo_msc_geom_to_true
+        f.restype = g.restype = D
+        f.argtypes = [D, D]
+        g.argtypes = [D, D, D]
+        z = f(t, lam)
+        return z, g(z, lam, t)
+
     # ------------------------------------------------------ event generators
     def egamma_gun(self, state, nevents, nparticles, gamma_fraction, minp, maxp, mineta, maxeta, minphi, maxphi):
         f = self.lib.gxo_egamma_gun
@@ -257,6 +287,7 @@ def oracle_config(cfg, nthreads=8):
     c.max_steps = 10 ** 8
     c.nthreads = nthreads
     c.score_events = cfg.nevents
+    c.msc = cfg.msc
     return c
 
 

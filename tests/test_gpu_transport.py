@@ -226,3 +226,44 @@ def test_run_command_line(capsys):
     out = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
     assert out["workload"] == "c1" and out["primaries"] == 200
     assert out["stats"]["steps"] > 200 and out["stats"]["errors"] == 0
+
+
+def test_multiple_scattering_fp64_matches_oracle(dm, oracle):
+    """With multiple scattering on, the FP64 engine and the oracle run the
+    same model on the same streams.  Its sampling takes logs, exponentials and
+    sines whose last bits differ between CUDA and glibc, which can flip a
+    rejection and send a track another way: compare the showers
+    statistically (C2, 1 GeV e-, 48 showers)."""
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c2(48)
+    edep, st, _ = run_gpu(dm, cfg, prims, nvol, msc=1)
+    ref = run_oracle(oracle, cfg, prims, nvol)
+    cfg.msc = 0
+    assert st["errors"] == 0 and ref["errors"] == 0
+    assert abs(st["steps"] - ref["steps"]) <= 0.01 * ref["steps"]
+    assert abs(st["tracks"] - ref["tracks"]) <= 0.01 * ref["tracks"]
+    e0 = prims[1].sum()
+    assert abs(edep.sum() + st["escaped"] - e0) <= 1e-9 * e0
+    g = edep.reshape(-1, 2).sum(1)
+    o = ref["edep"].reshape(-1, 2).sum(1)
+    big = o > 0.002 * o.sum()
+    assert np.all(np.abs(g - o)[big] <= 5 * 0.25 / np.sqrt(48) * o[big] + 1e-3 * o.sum())
+
+
+def test_multiple_scattering_fp32_vs_fp64_and_field(dm):
+    """FP32-mixed against FP64 with multiple scattering in 4 T (C3), per layer
+    within 1% plus statistics; energy conserved in both."""
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(40, 40)
+    out = {}
+    for prec in (0, 1):
+        e, st, _ = run_gpu(dm, cfg, prims, nvol, precision=prec, msc=1)
+        e0 = prims[1].sum()
+        assert st["errors"] == 0
+        assert abs(e.sum() + st["escaped"] - e0) <= (1e-9 if prec == 0 else 1e-5) * e0
+        out[prec] = (e.reshape(-1, 2).sum(1), st)
+    cfg.msc = 0
+    a, b = out[0][0], out[1][0]
+    big = a > 0.002 * a.sum()
+    assert np.all(np.abs(a - b)[big] <= 0.01 * a[big] + 5 * 0.2 / np.sqrt(80) * a[big])
+    assert abs(out[0][1]["steps"] - out[1][1]["steps"]) <= 0.02 * out[0][1]["steps"]
