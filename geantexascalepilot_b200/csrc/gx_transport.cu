@@ -1098,6 +1098,11 @@ template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step_p(co
 }
 
 // ------------------------------------------------- batched engine: split step
+// Resident 256-thread blocks per SM the step kernels are compiled for: the FP64
+// kernels would take 160-180 registers unbounded (12 warps per SM); bounded to
+// 128 they keep 16 warps at the cost of a few spills.  The FP32-mixed kernels
+// fit in 128 registers unbounded.
+template <class R> constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 0; // 0: no minimum
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
 // One slot per flagged lane in counter *ctr (ballot and popcount, one atomic
@@ -1125,7 +1130,7 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
 // tracks in a field), with the start and the end of a step attached to it, so
 // a lane whose step needs several sub-steps does not hold up the others.
 // All stores and buffers are written at slots reserved per warp, contiguous.
-template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(const Args<R> *__restrict__ A)
+template <class R, int PT> __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1216,7 +1221,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256) k_transport(co
 // Post-step interaction of process PROC for the buffered tracks of type PT:
 // one model per kernel, so a warp runs one sampling algorithm; survivor and
 // secondaries go to the next stores.
-template <class R, int PT, int PROC> __global__ void __launch_bounds__(256) k_interact(const Args<R> *__restrict__ A)
+template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMinBlocks<R>) k_interact(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
