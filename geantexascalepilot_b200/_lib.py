@@ -100,6 +100,10 @@ _SIGS = {
     "gx_table_invrange": (I, [P, I, I, P, P, I, P]),
     "gx_sb_value": (I, [P, I, P, P, P, I, P]),
     "gx_cut_value": (I, [P, I, I, PD]),
+    "gx_cut_convert": (I, [I, I, PD, PD, D, D, I, PD]),
+    "gx_ctx_compute_cuts": (I, [P, D]),
+    "gx_table_build": (I, [P, I, I, P, P, I, P]),
+    "gx_ctx_rebuild_tables": (I, [P, PD]),
     "gx_interact": (I, [P, I, C.POINTER(ModelParams), I] + [P] * 11 + [P]),
     "gx_xs_per_atom": (I, [I, D, P, P, I, P]),
     "gx_post_step_gpil": (I, [P, I, I, I] + [P] * 6 + [P]),

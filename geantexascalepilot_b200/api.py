@@ -60,6 +60,27 @@ class ProxyDataManager:
         except Exception:
             pass
 
+    def table_build(self, table, mat, E):
+        """A macroscopic cross-section table evaluated from the models
+        (gx_table_build)."""
+        E = _dev(E, torch.float64)
+        out = torch.empty_like(E)
+        check(lib.gx_table_build(self.handle, table, mat, _ptr(E), _ptr(out), E.numel(), _stream()))
+        return out
+
+    def rebuild_tables(self):
+        """Replace the Compton, ionisation and e- brems tables by ones built
+        from the models (gx_ctx_rebuild_tables); returns the largest relative
+        change above 10 keV."""
+        worst = C.c_double()
+        check(lib.gx_ctx_rebuild_tables(self.handle, C.byref(worst)))
+        return worst.value
+
+    def compute_cuts(self, cut_mm=0.7):
+        """Replace the cut table read from cut.dat by one converted from a
+        range cut (gx_ctx_compute_cuts)."""
+        check(lib.gx_ctx_compute_cuts(self.handle, cut_mm))
+
     # ProxyPhysicsTable::Value(index, E) of table `table`
     def table_value(self, table, mat, E):
         E = _dev(E, torch.float64)
@@ -442,4 +463,17 @@ def hepevt_load(path, mode=MODE_PHYSICS, max_events=1 << 30, vertex=(0.0, 0.0, 0
                              C.byref(n), C.byref(nev), C.byref(skip), _stream()))
     k = n.value
     return (t[:k], E[:k], pos[:k], d[:k], ev[:k]), (nev.value, skip.value)
+
+
+def cut_convert(particle, Z, n_atoms, density, cut, from_length=True):
+    """CutConverter::Convert (cuts/src/CutConverter.cpp:107-128) on the host:
+    the energy (MeV) of a range cut (mm) for particle 0 gamma / 1 e- / 2 e+ in
+    a material of elements Z with n_atoms per mm^3 and density g/cm^3, or the
+    length of an energy cut when from_length is False."""
+    Z = [float(z) for z in (Z if hasattr(Z, "__len__") else [Z])]
+    n = [float(a) for a in (n_atoms if hasattr(n_atoms, "__len__") else [n_atoms])]
+    out = C.c_double()
+    check(lib.gx_cut_convert(particle, len(Z), (C.c_double * len(Z))(*Z), (C.c_double * len(n))(*n), density, cut,
+                             1 if from_length else 0, C.byref(out)))
+    return out.value
 

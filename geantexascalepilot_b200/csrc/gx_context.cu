@@ -239,6 +239,51 @@ static void material(Data &d, int m, double Z, double A, double density, double 
   c[6] = 1.7888e-2 + z13 * (1.9659e-2 - z13 * 2.6664e-3);
 }
 
+// Per node of a vector: the cubic of its bin as a polynomial in
+// u = (E - x_i) / delta, {x_i, 1 / delta, c0, c1, c2, c3}, in FP64 and FP32.
+static void append_coeffs(const HostVec &v, std::vector<double> &C64, std::vector<float> &C32)
+{
+  const int n = (int)v.x.size();
+  for (int i = 0; i < n; ++i) {
+    double x1 = v.x[i], x2 = (i + 1 < n) ? v.x[i + 1] : x1 + 1.0;
+    double y1 = v.y[i], y2 = (i + 1 < n) ? v.y[i + 1] : y1;
+    double a1 = v.d2[i], a2 = (i + 1 < n) ? v.d2[i + 1] : a1;
+    double dl = x2 - x1, h = dl * dl / 6.0;
+    double c[6] = {x1, 1.0 / dl, y1, (y2 - y1) - h * (2.0 * a1 + a2), 3.0 * h * a1, h * (a2 - a1)};
+    for (int k = 0; k < 6; ++k) {
+      C64.push_back(c[k]);
+      C32.push_back((float)c[k]);
+    }
+  }
+}
+
+// New node values for vector (table, mat): second derivatives and per-bin
+// coefficients recomputed on the host, all four node arrays updated on the
+// device in place (the node energies stay).
+int refit_vector(Ctx *ctx, int table, int mat, const double *ynew)
+{
+  const Data &d = ctx->host;
+  const VecDesc &vd = d.vec[table][mat];
+  const int n = vd.n;
+  HostVec v;
+  v.x.resize(n);
+  v.y.assign(ynew, ynew + n);
+  cudaError_t e = cudaMemcpy(v.x.data(), d.x + vd.off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_error(e, "refit: node energies");
+  spline_d2(v);
+  std::vector<double> C64;
+  std::vector<float> C32;
+  append_coeffs(v, C64, C32);
+  if ((e = cudaMemcpy(const_cast<double *>(d.y) + vd.off, v.y.data(), n * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(const_cast<double *>(d.d2) + vd.off, v.d2.data(), n * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(const_cast<double *>(d.c64) + 6 * vd.off, C64.data(), C64.size() * sizeof(double),
+                      cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(const_cast<float *>(d.c32) + 6 * vd.off, C32.data(), C32.size() * sizeof(float),
+                      cudaMemcpyHostToDevice)))
+    return cuda_error(e, "refit: upload");
+  return GX_OK;
+}
+
 template <class T> static int upload(const std::vector<T> &h, T **d)
 {
   cudaError_t e = cudaMalloc((void **)d, sizeof(T) * (h.empty() ? 1 : h.size()));
@@ -277,17 +322,8 @@ int load_data(const char *datadir, Ctx *ctx)
         X.push_back(v[m].x[i]);
         Y.push_back(v[m].y[i]);
         D2.push_back(v[m].d2[i]);
-        // bin i: polynomial in u = (E - x_i) / delta of the same cubic
-        double x1 = v[m].x[i], x2 = (i + 1 < n) ? v[m].x[i + 1] : x1 + 1.0;
-        double y1 = v[m].y[i], y2 = (i + 1 < n) ? v[m].y[i + 1] : y1;
-        double a1 = v[m].d2[i], a2 = (i + 1 < n) ? v[m].d2[i + 1] : a1;
-        double dl = x2 - x1, h = dl * dl / 6.0;
-        double c[6] = {x1, 1.0 / dl, y1, (y2 - y1) - h * (2.0 * a1 + a2), 3.0 * h * a1, h * (a2 - a1)};
-        for (int k = 0; k < 6; ++k) {
-          C64.push_back(c[k]);
-          C32.push_back((float)c[k]);
-        }
       }
+      append_coeffs(v[m], C64, C32);
     }
   }
   if (!read_cuts(dir, d)) return set_error(GX_ERR_DATA, "cannot read %s/table/cut.dat", datadir);

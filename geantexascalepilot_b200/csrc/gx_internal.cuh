@@ -25,6 +25,7 @@ void jump_matrix(int comp, long long e, long long c, uint64_t out[9]);
 void mat_mul(const uint64_t A[9], const uint64_t B[9], uint64_t C[9], uint64_t m);
 void mat_vec(const uint64_t A[9], uint64_t v[3], uint64_t m);
 void release_engine(Ctx *c);
+int refit_vector(Ctx *ctx, int table, int mat, const double *ynew);
 
 inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 

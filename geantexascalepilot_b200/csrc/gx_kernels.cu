@@ -201,53 +201,11 @@ __global__ void k_interact(const Data *__restrict__ d, InterArgs a)
   if (err) atomicOr(a.err, err);
 }
 
-// ProxyKleinNishina::CrossSectionPerAtom (ProxyKleinNishina.hpp:62-93); the
-// reference's low-energy threshold is 15 * geantx::units::keV, a GeV-based
-// unit, i.e. 1.5e-5 in this MeV-based arithmetic.
-__device__ double kn_xs_per_atom(double Z, double e)
-{
-  double Z2 = Z * Z;
-  double p1 = 2.7965e-1 + 1.9756e-5 * Z + -3.9178e-7 * Z2;
-  double p2 = -1.8300e-1 + -1.0205e-2 * Z + 6.8241e-5 * Z2;
-  double p3 = 6.7527 + -7.3913e-2 * Z + 6.0480e-5 * Z2;
-  double p4 = -1.9798e+1 + 2.7079e-2 * Z + 3.0274e-4 * Z2;
-  double T0 = (Z < 1.5) ? 40.0 * keV : 15.0 * 1.e-6;
-  double X = fmax(e, T0) / kEMass, X2 = X * X;
-  double xs = p1 * ::log(1. + 2. * X) / X + (p2 + p3 * X + p4 * X2) / (1. + 20. * X + 230. * X2 + 440. * X2 * X);
-  if (e < T0) {
-    const double dT0 = keV;
-    X = (T0 + dT0) / kEMass;
-    X2 = X * X;
-    double sigma = p1 * ::log(1. + 2. * X) / X + (p2 + p3 * X + p4 * X2) / (1. + 20. * X + 230. * X2 + 440. * X2 * X);
-    double c1 = -T0 * (sigma - xs) / (xs * dT0);
-    double c2 = (Z > 1.5) ? 0.375 - 0.0556 * ::log(Z) : 0.150;
-    double y = ::log(e / T0);
-    xs *= ::exp(-y * (c1 + c2 * y));
-  }
-  return Z * xs * (1.e-28 * (1000. * 1000.));
-}
-
-// ProxyMollerScattering::CrossSectionPerAtom (ProxyMollerScattering.hpp:61-89)
-__device__ double mb_xs_per_atom(double Z, double kin, double twopi_mc2_rcl2)
-{
-  const double cutEnergy = 10.0 * eV;
-  double tmax = fmin(100.0 * TeV, 0.5 * kin);
-  if (cutEnergy > tmax) return 0.0;
-  double xmin = cutEnergy / kin, xmax = tmax / kin;
-  double tau = kin / kEMass, gam = tau + 1.0, gamma2 = gam * gam;
-  double beta2 = tau * (tau + 2) / gamma2;
-  double gg = (2.0 * gam - 1.0) / gamma2;
-  double xs = ((xmax - xmin) * (1.0 - gg + 1.0 / (xmin * xmax) + 1.0 / ((1.0 - xmin) * (1.0 - xmax))) -
-               gg * ::log(xmax * (1.0 - xmin) / (xmin * (1.0 - xmax)))) /
-              beta2;
-  return Z * xs * twopi_mc2_rcl2 / kin;
-}
-
 __global__ void k_xs(int model, double Z, double c, const double *__restrict__ E, double *__restrict__ out, int n)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  out[i] = (model == GX_KLEIN_NISHINA) ? kn_xs_per_atom(Z, E[i]) : mb_xs_per_atom(Z, E[i], c);
+  out[i] = (model == GX_KLEIN_NISHINA) ? kn_xs_per_atom(Z, E[i]) : mb_xs_per_atom(Z, E[i], c, 10.0 * eV);
 }
 
 // ------------------------------------------------------------- processes

@@ -1,0 +1,156 @@
+// gx_tables_build.cu -- macroscopic cross-section tables built on the device
+// from the models' cross sections, in place of the Geant4-dumped ASCII tables.
+//
+// The reference builds nothing (its macroscopic cross section is
+// ProxyEmModel::MacroscopicCrossSection, proxy/ProxyEmModel.hpp:57-76, the sum
+// over elements of n_atoms x CrossSectionPerAtom, evaluated per call); its
+// tables come from Geant4.  Here one thread per node energy evaluates:
+//   Lambda.compt / LambdaPrim.compt   n_atoms sigma_KN(Z, E) (x E for Prim):
+//     ProxyKleinNishina::CrossSectionPerAtom (ProxyKleinNishina.hpp:62-93)
+//   Lambda.eIoni.e-   n_atoms sigma_Moller(Z, T, cut_e-): ProxyMollerScattering::
+//     CrossSectionPerAtom (ProxyMollerScattering.hpp:61-89) with the
+//     material's production cut instead of the reference's fixed 10 eV
+//   Lambda.eIoni.e+   n_el sigma_Bhabha(T, cut_e-): the integral from the cut
+//     to T of the differential cross section the Bhabha sampler draws from
+//     (B(x) = 1/(beta^2 x^2) - b1/x + b2 - b3 x + b4 x^2, x = energy fraction)
+//   Lambda.eBrem.e-   n_atoms sigma_SB(Z, T, cut_gamma): the Seltzer-Berger
+//     tables chi(k/T, T) = (beta^2/Z^2) k dsigma/dk integrated in ln k from the
+//     cut to T with the dielectric suppression k^2 / (k^2 + k_p^2),
+//     k_p^2 = (Migdal constant x n_el) E_total^2; 16 x 8-point Gauss-Legendre.
+// gx_ctx_rebuild_tables puts these values on the shipped tables' node
+// energies (materials Pb and LAr; brems up to 1 GeV, where Geant4's table
+// switches from the Seltzer-Berger model to the relativistic one) and refits
+// the splines; the shipped values remain where no model here applies.
+#include "gx_internal.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace gx {
+
+namespace {
+
+// 8-point Gauss-Legendre on [0, 1]: nodes and weights
+__constant__ double kGLx[8] = {0.019855071751231856, 0.10166676129318664, 0.2372337950418355,
+                               0.40828267875217510,  0.59171732124782490, 0.7627662049581645,
+                               0.89833323870681340,  0.98014492824876810};
+__constant__ double kGLw[8] = {0.050614268145188130, 0.11119051722668724, 0.15685332293894363,
+                               0.18134189168918100,  0.18134189168918100, 0.15685332293894363,
+                               0.11119051722668724,  0.050614268145188130};
+
+__device__ double bhabha_xs_per_electron(double kin, double cut, double twopi_mc2_rcl2)
+{
+  if (!(cut < kin)) return 0.0;
+  const double energy = kin + kEMass, gam = energy / kEMass, beta2 = 1.0 - 1.0 / (gam * gam);
+  const double y = 1.0 / (1.0 + gam), y2 = y * y, y12 = 1.0 - 2.0 * y;
+  const double b1 = 2.0 - y2, b2 = y12 * (3.0 + y2), y122 = y12 * y12, b4 = y122 * y12, b3 = b4 + y122;
+  const double x0 = cut / kin;
+  const double I = (1.0 / x0 - 1.0) / beta2 - b1 * ::log(1.0 / x0) + b2 * (1.0 - x0) -
+                   b3 * (1.0 - x0 * x0) / 2.0 + b4 * (1.0 - x0 * x0 * x0) / 3.0;
+  return twopi_mc2_rcl2 / kin * I;
+}
+
+__device__ double sb_xs_per_atom(const SBTable &t, double Z, double kin, double cut, double density_factor)
+{
+  if (!(cut < kin)) return 0.0;
+  const double E = kin + kEMass, beta2 = kin * (kin + 2.0 * kEMass) / (E * E), kp2 = density_factor * E * E;
+  const double v0 = ::log(cut), dv = (::log(kin) - v0) / 16.0, lnT = ::log(kin);
+  double s = 0.0;
+  for (int l = 0; l < 16; ++l)
+    for (int i = 0; i < 8; ++i) {
+      const double k = ::exp(v0 + (l + kGLx[i]) * dv);
+      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k));
+    }
+  return Z * Z / beta2 * s * dv * 1.0e-25; // millibarn -> mm^2
+}
+
+__global__ void k_table_build(const Data *__restrict__ D, int table, int mat, const double *__restrict__ E,
+                              double *__restrict__ out, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Data &d = *D;
+  const double e = E[i], Z = d.mat_Z[mat], n_el = d.mat_nel[mat], n_atoms = n_el / Z;
+  const double twopi_mc2_rcl2 = 2.0 * kEMass * d.pi_rcl2;
+  double v = 0.0;
+  switch (table) {
+  case GX_Lambda_compt: v = fmax(0.0, n_atoms * kn_xs_per_atom(Z, e)); break;
+  case GX_LambdaPrim_compt: v = fmax(0.0, e * n_atoms * kn_xs_per_atom(Z, e)); break;
+  case GX_Lambda_eIoni_em: v = n_atoms * mb_xs_per_atom(Z, e, twopi_mc2_rcl2, d.cut_energy[1][mat]); break;
+  case GX_Lambda_eIoni_ep: v = n_el * bhabha_xs_per_electron(e, d.cut_energy[1][mat], twopi_mc2_rcl2); break;
+  case GX_Lambda_eBrem_em:
+    v = n_atoms * sb_xs_per_atom(d.sb[mat == 1 ? 2 : 1], Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat]);
+    break;
+  default: v = 0.0;
+  }
+  out[i] = v;
+}
+
+bool buildable(int table, int mat)
+{
+  const bool t = table == GX_Lambda_compt || table == GX_LambdaPrim_compt || table == GX_Lambda_eIoni_em ||
+                 table == GX_Lambda_eIoni_ep || table == GX_Lambda_eBrem_em;
+  return t && (mat == 1 || mat == 2); // the SB data cover lead and argon
+}
+
+} // namespace
+
+} // namespace gx
+
+using namespace gx;
+
+extern "C" {
+
+int gx_table_build(gx_ctx *ctx, int table, int mat, const double *d_E, double *d_out, int n, gx_stream_t s)
+{
+  if (!ctx || n < 0 || (n > 0 && (!d_E || !d_out))) return set_error(GX_ERR_ARG, "gx_table_build: bad arguments");
+  if (!buildable(table, mat)) return set_error(GX_ERR_ARG, "gx_table_build: table %d, material %d not built", table, mat);
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (n == 0) return GX_OK;
+  k_table_build<<<(n + 127) / 128, 128, 0, stream_of(s)>>>(c->dev, table, mat, d_E, d_out, n);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "k_table_build");
+}
+
+int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change)
+{
+  if (!ctx) return set_error(GX_ERR_ARG, "gx_ctx_rebuild_tables: null context");
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return cuda_error(e, "gx_ctx_rebuild_tables: cudaSetDevice");
+  const int tables[] = {GX_Lambda_compt, GX_LambdaPrim_compt, GX_Lambda_eIoni_em, GX_Lambda_eIoni_ep,
+                        GX_Lambda_eBrem_em};
+  double *dv = nullptr;
+  int nmax = 0;
+  for (int t : tables)
+    for (int m = 1; m <= 2; ++m) nmax = std::max(nmax, c->host.vec[t][m].n);
+  if ((e = cudaMalloc((void **)&dv, nmax * sizeof(double))) != cudaSuccess)
+    return cuda_error(e, "gx_ctx_rebuild_tables: scratch");
+  double worst = 0.0;
+  int rc = GX_OK;
+  for (int t : tables)
+    for (int m = 1; m <= 2 && rc == GX_OK; ++m) {
+      const VecDesc &vd = c->host.vec[t][m];
+      std::vector<double> x(vd.n), y(vd.n), old(vd.n);
+      k_table_build<<<(vd.n + 127) / 128, 128>>>(c->dev, t, m, c->host.x + vd.off, dv, vd.n);
+      if ((e = cudaMemcpy(y.data(), dv, vd.n * sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess ||
+          (e = cudaMemcpy(x.data(), c->host.x + vd.off, vd.n * sizeof(double), cudaMemcpyDeviceToHost)) ||
+          (e = cudaMemcpy(old.data(), c->host.y + vd.off, vd.n * sizeof(double), cudaMemcpyDeviceToHost))) {
+        rc = cuda_error(e, "gx_ctx_rebuild_tables: download");
+        break;
+      }
+      for (int i = 0; i < vd.n; ++i) {
+        // brems: the Seltzer-Berger range only (Geant4 changes model at 1 GeV)
+        if (t == GX_Lambda_eBrem_em && x[i] > 1.0e3) y[i] = old[i];
+        if (old[i] > 0.0 && y[i] > 0.0 && x[i] > 0.01) // above 10 keV (below it the shipped low-energy tails differ)
+          worst = std::max(worst, std::fabs(y[i] / old[i] - 1.0));
+      }
+      rc = refit_vector(c, t, m, y.data());
+    }
+  cudaFree(dv);
+  if (rc) return rc;
+  if (max_rel_change) *max_rel_change = worst;
+  return GX_OK;
+}
+
+} // extern "C"

@@ -93,6 +93,35 @@ int gx_sb_value(gx_ctx *ctx, int which, const double *d_x, const double *d_y, do
                 gx_stream_t s);
 /* ProxyDataManager::GetCutValue(index, ipart) (ProxyDataManager.cuh:52-54), host. */
 int gx_cut_value(gx_ctx *ctx, int index, int ipart, double *out);
+/* The production-cut converter of the reference, CutConverter::Convert
+ * (source/Geant/cuts/src/CutConverter.cpp:107-128, with
+ * CutConverterForGamma/Electron/Positron and Spline; 301 energies from 990 eV
+ * to 10 GeV as MaterialCuts.cpp:88-93 sets it), on the host: particle 0 gamma,
+ * 1 e-, 2 e+; a material of nelem elements Z with n_atoms per mm^3 and
+ * density in g/cm^3; from_length 1: *out = energy (MeV) of a cut given as a
+ * length (mm); 0: the length (mm) of a cut given as an energy (MeV). */
+int gx_cut_convert(int particle, int nelem, const double *Z, const double *n_atoms, double density, double cut,
+                   int from_length, double *out);
+/* Replaces the context's cut table (read from cut.dat, the Geant4 dump) by one
+ * computed with gx_cut_convert for a range cut of cut_mm in every material
+ * (protons: 100 keV per mm, Geant4's rule; the reference has no proton
+ * converter), and uploads it: the models' thresholds follow from then on. */
+int gx_ctx_compute_cuts(gx_ctx *ctx, double cut_mm);
+
+/* Macroscopic cross sections built on the device from the models' cross
+ * sections instead of read from the Geant4 tables (the reference evaluates
+ * ProxyEmModel::MacroscopicCrossSection, proxy/ProxyEmModel.hpp:57-76, and
+ * ships the tables): d_out[i] for table id `table` of material mat (1 Pb,
+ * 2 LAr) at energies d_E[i]: GX_Lambda_compt and GX_LambdaPrim_compt (Klein-
+ * Nishina, ProxyKleinNishina.hpp:62-93), GX_Lambda_eIoni_em (Moller with the
+ * material's e- cut, ProxyMollerScattering.hpp:61-89), GX_Lambda_eIoni_ep
+ * (Bhabha, integrated from the cut), GX_Lambda_eBrem_em (Seltzer-Berger
+ * tables integrated from the gamma cut, with dielectric suppression). */
+int gx_table_build(gx_ctx *ctx, int table, int mat, const double *d_E, double *d_out, int n, gx_stream_t s);
+/* Replaces the node values of those tables (brems up to 1 GeV) with the built
+ * ones and refits their splines; *max_rel_change (optional) receives the
+ * largest relative change above 10 keV.  Synchronous. */
+int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change);
 
 /* ------------------------------------------------------------- models */
 typedef struct {

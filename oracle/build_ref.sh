@@ -30,4 +30,14 @@ ${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
   "$SRC/proxy/src/ProxyEgammaGun.cpp" \
   "$SRC/proxy/src/ProxyHepEvtGenerator.cpp" \
   -x none "$STDCXX" -lm -o "$OUT/libgxref.so"
-echo "built $OUT/libgxref.so"
+# the production-cut converter, with its own material shims (oracle/refshim_cuts)
+${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
+  -I"$HERE/refshim_cuts" -I"$HERE/refshim" -I"$REF/source" \
+  "$HERE/refshim_cuts/cut_capi.cpp" \
+  "$SRC/cuts/src/CutConverter.cpp" \
+  "$SRC/cuts/src/CutConverterForGamma.cpp" \
+  "$SRC/cuts/src/CutConverterForElectron.cpp" \
+  "$SRC/cuts/src/CutConverterForPositron.cpp" \
+  "$SRC/cuts/src/Spline.cpp" \
+  -x none "$STDCXX" -lm -o "$OUT/libgxref_cuts.so"
+echo "built $OUT/libgxref.so $OUT/libgxref_cuts.so"

@@ -216,6 +216,10 @@ double gxo_msc_lambda1(const gxo_data_t *d, int type, int mat, double e);
 double gxo_msc_true_to_geom(double t, double lam);
 double gxo_msc_geom_to_true(double z, double lam, double tmax);
 
+/* production-cut conversion (gxo_cuts.c): CutConverter, cuts/src/CutConverter*.cpp */
+double gxo_cut_convert(int particle, int nelem, const double *Z, const double *n_atoms, double density, double cut,
+                       int from_length);
+
 /* ------------------------------------------------------ event generators */
 /* gxo_events.c: ProxyEgammaGun (proxy/src/ProxyEgammaGun.cpp:35-85) and
  * ProxyHepEvtGenerator (proxy/src/ProxyHepEvtGenerator.cpp:48-132). */
