@@ -42,7 +42,8 @@ class TransportConfig(C.Structure):
                 ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I), ("Bz", D), ("charged_local", I),
                 ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
-                ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I)]
+                ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I),
+                ("field_map", I)]
 
 
 class TransportStats(C.Structure):
@@ -102,6 +103,8 @@ _SIGS = {
     "gx_cut_value": (I, [P, I, I, PD]),
     "gx_cut_convert": (I, [I, I, PD, PD, D, D, I, PD]),
     "gx_ctx_compute_cuts": (I, [P, D]),
+    "gx_ctx_load_field_map": (I, [P, C.c_char_p]),
+    "gx_field_value": (I, [P, I, P, P, P]),
     "gx_table_build": (I, [P, I, I, P, P, I, P]),
     "gx_ctx_rebuild_tables": (I, [P, PD]),
     "gx_interact": (I, [P, I, C.POINTER(ModelParams), I] + [P] * 11 + [P]),

@@ -76,6 +76,20 @@ class ProxyDataManager:
         check(lib.gx_ctx_rebuild_tables(self.handle, C.byref(worst)))
         return worst.value
 
+    def load_field_map(self, path=None):
+        """Load a field map in the reference's CMS format (gx_ctx_load_field_map);
+        default: the CMS map shipped with the package."""
+        import os
+        path = path or os.path.join(_lib.DATA_DIR, "field", "cmsmagfield2015.txt")
+        check(lib.gx_ctx_load_field_map(self.handle, path.encode()))
+
+    def field_value(self, pos):
+        """The loaded map's field (tesla) at positions (mm), shape (n, 3)."""
+        p = _dev(pos, torch.float64).reshape(-1, 3).contiguous()
+        B = torch.empty_like(p)
+        check(lib.gx_field_value(self.handle, p.shape[0], _ptr(p), _ptr(B), _stream()))
+        return B
+
     def compute_cuts(self, cut_mm=0.7):
         """Replace the cut table read from cut.dat by one converted from a
         range cut (gx_ctx_compute_cuts)."""

@@ -458,6 +458,50 @@ int gx_ctx_create(const char *datadir, int device, gx_ctx **out)
   return GX_OK;
 }
 
+int gx_ctx_load_field_map(gx_ctx *ctx, const char *path)
+{
+  if (!ctx || !path) return set_error(GX_ERR_ARG, "gx_ctx_load_field_map: null argument");
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  FILE *f = std::fopen(path, "r");
+  if (!f) return set_error(GX_ERR_DATA, "gx_ctx_load_field_map: cannot open %s", path);
+  // ScalarCMSmagField::ReadVectorData (ScalarCMSmagField.h:162-199): one
+  // lattice point per line, r outer and z inner, values read as float and
+  // stored times 1 / (dr dz) in float
+  const float kAInverse = (float)(1.0 / (50.0f * 200.0f));
+  std::vector<float4> h((size_t)kFmapNr * kFmapNz);
+  int ind = 0;
+  char line[512];
+  while (std::fgets(line, sizeof(line), f)) {
+    float r, phi, z, bz, br, bphi;
+    if (std::sscanf(line, "R(mm)= %f phi(deg)= %f Z(mm)= %f Bz(tesla)= %f Br(tesla)= %f Bphi(tesla)= %f", &r, &phi,
+                    &z, &bz, &br, &bphi) != 6)
+      continue;
+    const int ir = ind / kFmapNz, iz = ind % kFmapNz;
+    if (ind >= kFmapNr * kFmapNz || std::fabs(r - 50.0f * ir) > 1e-3f || std::fabs(z - (-16000.0f + 200.0f * iz)) > 1e-3f) {
+      std::fclose(f);
+      return set_error(GX_ERR_DATA, "gx_ctx_load_field_map: %s: point %d is not on the 181 x 161 (r, z) lattice", path,
+                       ind);
+    }
+    h[ind] = make_float4(br * kAInverse, bphi * kAInverse, bz * kAInverse, 0.0f);
+    ++ind;
+  }
+  std::fclose(f);
+  if (ind != kFmapNr * kFmapNz)
+    return set_error(GX_ERR_DATA, "gx_ctx_load_field_map: %s: %d lattice points, expected %d", path, ind,
+                     kFmapNr * kFmapNz);
+  cudaError_t e = cudaSetDevice(c->device);
+  float4 *d = const_cast<float4 *>(c->host.fmap);
+  if (e == cudaSuccess && !d) {
+    e = cudaMalloc((void **)&d, h.size() * sizeof(float4));
+    if (e == cudaSuccess) c->owned.push_back(d);
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(d, h.data(), h.size() * sizeof(float4), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_error(e, "gx_ctx_load_field_map: upload");
+  c->host.fmap = d;
+  e = cudaMemcpy(c->dev, &c->host, sizeof(Data), cudaMemcpyHostToDevice);
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "gx_ctx_load_field_map: context upload");
+}
+
 int gx_ctx_destroy(gx_ctx *ctx)
 {
   if (!ctx) return GX_OK;

@@ -159,7 +159,49 @@ struct Data {
   // model's Z-dependent constants {X0, th1, th2, ca, cb, cc, cd}
   double mat_msc[kNMat][7];
   double pi_rcl2; // pi r_e^2, mm^2
+  // field map (optional, gx_ctx_load_field_map): (Br, Bphi, Bz) on an r-z
+  // lattice, r outer, each premultiplied by 1 / (dr dz) as the reference's
+  // reader stores them; null when no map is loaded
+  const float4 *fmap;
 };
+
+// Field of the map at pos (tesla): ScalarCMSmagField::GetFieldValue /
+// GetFieldValueRZ (examples/magneticfield/simplifiedCMS/inc/Geant/
+// ScalarCMSmagField.h:207-331) restated: r and z clamped to the lattice,
+// bilinear weights from the areas to the four corners (the stored values
+// carry the 1 / (dr dz)), the cell found with the reference's single-
+// precision inverse spacings; (Br, Bphi) rotated by the azimuth.  181 x 161
+// points, dr = 50 mm up to 9 m, dz = 200 mm over +-16 m.
+constexpr int kFmapNr = 181, kFmapNz = 161;
+__device__ __forceinline__ void field_map_value(const float4 *__restrict__ fmap, const double pos[3], double B[3])
+{
+  const float kRDiff = 9000.0f / (kFmapNr - 1), kZDiff = 2 * 16000.0f / (kFmapNz - 1);
+  const float kRDiffInv = 1.0f / kRDiff, kZDiffInv = 1.0f / kZDiff;
+  const double r0 = ::sqrt(pos[0] * pos[0] + pos[1] * pos[1]);
+  const double radius = fmin(r0, 9000.0), z = fmax(fmin(pos[2], 16000.0), -16000.0);
+  double rFloor = floor(radius * kRDiffInv), zInd = floor((z - (-16000.0)) * kZDiffInv);
+  rFloor = fmin(rFloor, (double)(kFmapNr - 2)); // the reference relies on rounding to stay inside
+  zInd = fmin(zInd, (double)(kFmapNz - 2));
+  const int i1 = (int)(rFloor * kFmapNz + zInd), i2 = i1 + 1;
+  const double zLow = (zInd - (kFmapNz - 1) / 2) * kZDiff, zHigh = zLow + kZDiff;
+  const double rLow = rFloor * kRDiff, rHigh = rLow + kRDiff;
+  const double a1 = (rHigh - radius) * (zHigh - z), a2 = (rHigh - radius) * (z - zLow);
+  const double a3 = (radius - rLow) * (zHigh - z), a4 = (radius - rLow) * (z - zLow);
+  const float4 b1 = __ldg(&fmap[i1]), b3 = __ldg(&fmap[i1 + kFmapNz]);
+  const float4 b2 = __ldg(&fmap[i2]), b4 = __ldg(&fmap[i2 + kFmapNz]);
+  const double br = b1.x * a1 + b2.x * a2 + b3.x * a3 + b4.x * a4;
+  const double bphi = b1.y * a1 + b2.y * a2 + b3.y * a3 + b4.y * a4;
+  const double bz = b1.z * a1 + b2.z * a2 + b3.z * a3 + b4.z * a4;
+  double s = 0.0, c = 1.0;
+  if (r0 != 0.0) {
+    const float rinv = (float)(1.0 / r0); // a float member in the reference
+    s = pos[1] * rinv;
+    c = pos[0] * rinv;
+  }
+  B[0] = br * c - bphi * s;
+  B[1] = br * s + bphi * c;
+  B[2] = bz;
+}
 
 // ProxyPhysicsVector::Value (ProxyPhysicsVector.cu:469-483) with the reference's
 // bin search (:388-394) and spline (:396-429); bin kept inside the vector.

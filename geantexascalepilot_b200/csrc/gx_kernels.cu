@@ -201,6 +201,18 @@ __global__ void k_interact(const Data *__restrict__ d, InterArgs a)
   if (err) atomicOr(a.err, err);
 }
 
+__global__ void k_field_value(const Data *__restrict__ d, int n, const double *__restrict__ pos,
+                              double *__restrict__ B)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  double p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]}, b[3];
+  field_map_value(d->fmap, p, b);
+  B[3 * i] = b[0];
+  B[3 * i + 1] = b[1];
+  B[3 * i + 2] = b[2];
+}
+
 __global__ void k_xs(int model, double Z, double c, const double *__restrict__ E, double *__restrict__ out, int n)
 {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -401,6 +413,17 @@ int gx_interact(gx_ctx *ctx, int model, const gx_model_params *p, int n, uint32_
   if (e != cudaSuccess) return cuda_error(e, "gx_interact");
   if (herr) return set_error(GX_ERR_ITERCAP, "gx_interact: a rejection loop hit its iteration cap");
   return GX_OK;
+}
+
+int gx_field_value(gx_ctx *ctx, int n, const double *d_pos, double *d_B, gx_stream_t s)
+{
+  if (!ctx || n < 0 || (n > 0 && (!d_pos || !d_B))) return set_error(GX_ERR_ARG, "gx_field_value: bad arguments");
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->host.fmap) return set_error(GX_ERR_ARG, "gx_field_value: no field map loaded (gx_ctx_load_field_map)");
+  if (n == 0) return GX_OK;
+  k_field_value<<<grid_for(n), kBlock, 0, stream_of(s)>>>(c->dev, n, d_pos, d_B);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "k_field_value");
 }
 
 int gx_xs_per_atom(int model, double Z, const double *d_E, double *d_out, int n, gx_stream_t s)

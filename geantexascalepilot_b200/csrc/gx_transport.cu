@@ -38,7 +38,8 @@ template <class R> struct Store {
 
 struct Geom {
   int geometry, axis, nlayers, box_mat, charged_local, nvol, nevents;
-  int msc; // multiple scattering of e-/e+
+  int msc;       // multiple scattering of e-/e+
+  int field_map; // 1: the context's field map with Runge-Kutta sub-steps, 0: uniform Bz
   double t_abs, pitch, x0, total, half_trans, Bz;
   double box_half[3], box_centre[3];
 };
@@ -694,7 +695,7 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
   c.newvol = t.vol;
   c.crossed = false;
   c.nsub = 0;
-  if (charged && g.Bz != 0.0) {
+  if (charged && (g.Bz != 0.0 || g.field_map)) {
     c.remaining = (double)pstep;
     c.total = 0.0;
     return true;
@@ -726,7 +727,79 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
 // the momentum and the sub-step length heuristic are in R (FP32 in the mixed
 // build).  Returns true when the step is complete (boundary reached, length
 // used up, or the cap of 10000 sub-steps hit: then newvol = -2).
-template <class R> __device__ __forceinline__ bool field_substep(const Geom &g, Track<R> &t, StepCtx<R> &c, Local &L)
+// One classical fourth-order Runge-Kutta step of length s through the field
+// map (FP64): position x and unit direction u with du/ds = k u x B(x),
+// k = 0.299792458 q / p (MeV, T, mm); four map lookups, direction renormalised.
+__device__ __forceinline__ void rk4_map_step(const float4 *__restrict__ fmap, double k, double s, double x[3],
+                                             double u[3], const double B0[3])
+{
+  double xs[3], us[3], B[3], kx[4][3], ku[4][3];
+  const double h[3] = {0.5 * s, 0.5 * s, s};
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    kx[0][j] = u[j];
+  }
+  ku[0][0] = k * (u[1] * B0[2] - u[2] * B0[1]);
+  ku[0][1] = k * (u[2] * B0[0] - u[0] * B0[2]);
+  ku[0][2] = k * (u[0] * B0[1] - u[1] * B0[0]);
+#pragma unroll
+  for (int st = 1; st < 4; ++st) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      xs[j] = x[j] + h[st - 1] * kx[st - 1][j];
+      us[j] = u[j] + h[st - 1] * ku[st - 1][j];
+    }
+    field_map_value(fmap, xs, B);
+#pragma unroll
+    for (int j = 0; j < 3; ++j) kx[st][j] = us[j];
+    ku[st][0] = k * (us[1] * B[2] - us[2] * B[1]);
+    ku[st][1] = k * (us[2] * B[0] - us[0] * B[2]);
+    ku[st][2] = k * (us[0] * B[1] - us[1] * B[0]);
+  }
+  double m = 0.0;
+#pragma unroll
+  for (int j = 0; j < 3; ++j) {
+    x[j] += s / 6.0 * (kx[0][j] + 2.0 * kx[1][j] + 2.0 * kx[2][j] + kx[3][j]);
+    u[j] += s / 6.0 * (ku[0][j] + 2.0 * ku[1][j] + 2.0 * ku[2][j] + ku[3][j]);
+    m += u[j] * u[j];
+  }
+  m = 1.0 / ::sqrt(m);
+  u[0] *= m;
+  u[1] *= m;
+  u[2] *= m;
+}
+
+// One sub-step through the field map: the sub-step length from the same
+// geometry and sagitta limits as the helix (with the field at the start
+// point), then a Runge-Kutta step.  Returns the length moved.
+template <class R>
+__device__ __forceinline__ double field_map_substep(const Data &d, const Geom &g, Track<R> &t, double remaining,
+                                                    double saf, double snext)
+{
+  const double eps = 0.1, charge = (t.type == 1) ? -1.0 : 1.0;
+  const double E = (double)t.E, p = ::sqrt(E * (E + 2.0 * kEMass));
+  double B0[3], u[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
+  field_map_value(d.fmap, t.pos, B0);
+  const double cx = u[1] * B0[2] - u[2] * B0[1], cy = u[2] * B0[0] - u[0] * B0[2], cz = u[0] * B0[1] - u[1] * B0[0];
+  const double bperp = ::sqrt(cx * cx + cy * cy + cz * cz); // |u x B|
+  double step_field = 1.7976931348623157e308;
+  if (bperp > 0.0) step_field = fmax(2.0 * ::sqrt(eps * p / (0.299792458 * bperp)), saf);
+  const double step_gp = fmax(fmin(remaining, 1e-4), snext);
+  const double s = fmin(fmin(step_gp, step_field), remaining);
+  if (bperp > 0.0) {
+    rk4_map_step(d.fmap, 0.299792458 * charge / p, s, t.pos, u, B0);
+    for (int k = 0; k < 3; ++k) t.dir[k] = (R)u[k];
+  } else {
+    for (int k = 0; k < 3; ++k) t.pos[k] += s * u[k];
+  }
+  return s;
+}
+
+// FM: 1 when the transport follows the field map (Runge-Kutta), 0 for the
+// uniform field (helix); a template parameter so that the uniform-field
+// kernels carry no Runge-Kutta code (registers).
+template <class R, int FM>
+__device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c, Local &L)
 {
   const R eps = R(0.1); // gEpsDeflection = 1e-2 cm
   const R charge = (t.type == 1) ? R(-1) : R(1);
@@ -739,11 +812,15 @@ template <class R> __device__ __forceinline__ bool field_substep(const Geom &g, 
   double saf = safety(g, t.vol, t.pos);
   double snext = (saf > remaining) ? remaining
                                    : fmax(2e-9, fmin(dist_to_out(g, t.vol, t.pos, dd, plane), remaining) + 2e-9);
+  double s;
+  if constexpr (FM == 1) {
+    s = field_map_substep<R>(d, g, t, remaining, saf, snext);
+  } else {
   double step_gp = fmax(fmin(remaining, 1e-4), snext);
   R pt = p * M<R>::sqrt(fmax(R(1) - t.dir[2] * t.dir[2], R(0)));
   double step_field = 1.7976931348623157e308;
   if (pt > R(0)) step_field = fmax(2.0 * (double)M<R>::sqrt(eps * pt / curv_per_pt), saf);
-  double s = fmin(fmin(step_gp, step_field), remaining);
+  s = fmin(fmin(step_gp, step_field), remaining);
   if (pt > R(0)) {
     const R rn = p / (R(kB2C_mm) * charge * absB);
     double np[3];
@@ -756,6 +833,7 @@ template <class R> __device__ __forceinline__ bool field_substep(const Geom &g, 
     }
   } else {
     for (int k = 0; k < 3; ++k) t.pos[k] += s * dd[k];
+  }
   }
   c.total += s;
   c.remaining = remaining - s;
@@ -838,12 +916,13 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
 }
 
 // The three phases in sequence: one whole step up to the interaction.
-template <class R> __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
+template <class R, int FM>
+__device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
                                                                  int *proc)
 {
   StepCtx<R> c;
   if (step_begin(d, g, t, c))
-    while (!field_substep(g, t, c, L)) {
+    while (!field_substep<R, FM>(d, g, t, c, L)) {
     }
   return step_end(d, g, t, c, L, proc);
 }
@@ -851,11 +930,12 @@ template <class R> __device__ __forceinline__ int transport_part(const Data &d, 
 // The whole OneStep, interaction included (the fused form the plain loop
 // runs); the oracle's one_step is the same algorithm in the same order of
 // random draws.  Returns false when the track is finished.
-template <class R> __device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
+template <class R, int FM>
+__device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
 {
   sec.n = 0;
   int proc = -1;
-  int r = transport_part(d, g, t, L, &proc);
+  int r = transport_part<R, FM>(d, g, t, L, &proc);
   if (r == kInteract) {
     run_model(d, g, t, proc, sec, L);
     return t.E > R(0);
@@ -1055,7 +1135,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
 
 // PT: particle type of the store (0, 1, 2), or 3 for the single mixed store.
 // The fused step (transport and interaction in one kernel) of the plain loop.
-template <class R, int PT> __device__ __forceinline__ void step_body(const Args<R> &a)
+template <class R, int PT, int FM> __device__ __forceinline__ void step_body(const Args<R> &a)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1080,7 +1160,7 @@ template <class R, int PT> __device__ __forceinline__ void step_body(const Args<
     if (active) {
       load_track(cur, i, PT, t);
       L.st[S_READ0 + SRC]++;
-      alive = one_step(d, a.g, t, sec, L);
+      alive = one_step<R, FM>(d, a.g, t, sec, L);
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
     emit_tracks<R, SRC>(a, ctl, par, active, alive, t, sec, L);
@@ -1091,10 +1171,13 @@ template <class R, int PT> __device__ __forceinline__ void step_body(const Args<
 // Arguments by value (the allocation-free entry point) or from a device copy.
 // Two resident blocks per SM: the fused step needs ~190 registers per thread
 // unconstrained, which would leave one 256-thread block (8 warps) per SM.
-template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step(Args<R> a) { step_body<R, PT>(a); }
-template <class R, int PT> __global__ void __launch_bounds__(256, 2) k_step_p(const Args<R> *__restrict__ A)
+template <class R, int PT, int FM> __global__ void __launch_bounds__(256, 2) k_step(Args<R> a)
 {
-  step_body<R, PT>(*A);
+  step_body<R, PT, FM>(a);
+}
+template <class R, int PT, int FM> __global__ void __launch_bounds__(256, 2) k_step_p(const Args<R> *__restrict__ A)
+{
+  step_body<R, PT, FM>(*A);
 }
 
 // ------------------------------------------------- batched engine: split step
@@ -1130,7 +1213,8 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
 // tracks in a field), with the start and the end of a step attached to it, so
 // a lane whose step needs several sub-steps does not hold up the others.
 // All stores and buffers are written at slots reserved per warp, contiguous.
-template <class R, int PT> __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
+template <class R, int PT, int FM>
+__global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1178,7 +1262,7 @@ template <class R, int PT> __global__ void __launch_bounds__(256, kMinBlocks<R>)
       infield = step_begin(d, a.g, t, c);
       done = !infield;
     }
-    if (PT != 0 && have && infield && field_substep(a.g, t, c, L)) {
+    if (PT != 0 && have && infield && field_substep<R, FM>(d, a.g, t, c, L)) {
       infield = false;
       done = true;
     }
@@ -1518,7 +1602,7 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     // plain loop: one fused step kernel over the mixed store
     k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
     k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
-    k_step_p<R, 3><<<L.grid, L.block, L.smem, s>>>(A);
+    (L.a.g.field_map ? k_step_p<R, 3, 1> : k_step_p<R, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
     k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
     return;
   }
@@ -1533,14 +1617,15 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     se = e->s1;
     sp = e->s2;
   }
-  k_transport<R, 0><<<L.grid, L.block, L.smem, sg>>>(A);
+  const bool fm = L.a.g.field_map != 0;
+  (fm ? k_transport<R, 0, 1> : k_transport<R, 0, 0>)<<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 0><<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 1><<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 2><<<L.grid, L.block, L.smem, sg>>>(A);
-  k_transport<R, 1><<<L.grid, L.block, L.smem, se>>>(A);
+  (fm ? k_transport<R, 1, 1> : k_transport<R, 1, 0>)<<<L.grid, L.block, L.smem, se>>>(A);
   k_interact<R, 1, 0><<<L.grid, L.block, L.smem, se>>>(A);
   k_interact<R, 1, 1><<<L.grid, L.block, L.smem, se>>>(A);
-  k_transport<R, 2><<<L.grid, L.block, L.smem, sp>>>(A);
+  (fm ? k_transport<R, 2, 1> : k_transport<R, 2, 0>)<<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 0><<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 1><<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 2><<<L.grid, L.block, L.smem, sp>>>(A);
@@ -1558,19 +1643,20 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
 template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q, cudaEvent_t mid)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
+  const bool fm = L.a.g.field_map != 0;
   if (q == 0) {
-    k_transport<R, 0><<<L.grid, L.block, L.smem, s>>>(A);
+    (fm ? k_transport<R, 0, 1> : k_transport<R, 0, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 0, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 1><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 2><<<L.grid, L.block, L.smem, s>>>(A);
   } else if (q == 1) {
-    k_transport<R, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    (fm ? k_transport<R, 1, 1> : k_transport<R, 1, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 1, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 1, 1><<<L.grid, L.block, L.smem, s>>>(A);
   } else {
-    k_transport<R, 2><<<L.grid, L.block, L.smem, s>>>(A);
+    (fm ? k_transport<R, 2, 1> : k_transport<R, 2, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 2, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 2, 1><<<L.grid, L.block, L.smem, s>>>(A);
@@ -1657,6 +1743,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   g.half_trans = cfg->half_trans;
   g.Bz = cfg->Bz;
   g.msc = cfg->msc;
+  g.field_map = cfg->field_map;
   for (int k = 0; k < 3; ++k) {
     g.box_half[k] = cfg->box_half[k];
     g.box_centre[k] = cfg->box_centre[k];
@@ -1732,7 +1819,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
           if (!batched) {
-            k_step_p<R, 3><<<L.grid, L.block, L.smem, s>>>((const Args<R> *)E->dargs);
+            (L.a.g.field_map ? k_step_p<R, 3, 1> : k_step_p<R, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(
+                (const Args<R> *)E->dargs);
             cudaEventRecord(em[q], s);
           } else {
             enqueue_type(L, E, s, q, em[q]);
@@ -1879,6 +1967,8 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
   if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
     return set_error(GX_ERR_ARG, "gx_transport_run: block_size must be a multiple of 32, at most 256");
   Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  if (cfg->field_map && !C->host.fmap)
+    return set_error(GX_ERR_ARG, "gx_transport_run: field_map = 1 without a field map (gx_ctx_load_field_map)");
   cudaSetDevice(C->device);
   if (cfg->precision == 1)
     return run<float>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
@@ -2026,6 +2116,8 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
     return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: block_size must be a multiple of 32, at most 256");
   Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  if (cfg->field_map && !C->host.fmap)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: field_map = 1 without a field map");
   cudaError_t err = cudaSetDevice(C->device);
   if (err != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: cudaSetDevice");
   unsigned char *base = nullptr;
@@ -2067,6 +2159,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   g.half_trans = cfg->half_trans;
   g.Bz = cfg->Bz;
   g.msc = cfg->msc;
+  g.field_map = cfg->field_map;
   for (int k = 0; k < 3; ++k) {
     g.box_half[k] = cfg->box_half[k];
     g.box_centre[k] = cfg->box_centre[k];
@@ -2106,7 +2199,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   for (;;) {
     k_refill<double><<<L.grid, L.block, 0, s>>>(L.a);
     k_refill_done<<<1, 1, 0, s>>>(ctl);
-    k_step<double, 3><<<L.grid, L.block, L.smem, s>>>(L.a);
+    (cfg->field_map ? k_step<double, 3, 1> : k_step<double, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(L.a);
     k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
     if ((err = cudaGetLastError()) != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: launch");
     if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

@@ -1,8 +1,9 @@
 #!/usr/bin/env python3
 """Import the physics data that the reference ships with its EM transport path.
 
-The reference reads its Geant4-format ASCII physics tables, cut table and
-Seltzer-Berger bremsstrahlung tables at run time from
+The reference reads its Geant4-format ASCII physics tables, cut table,
+Seltzer-Berger bremsstrahlung tables and (in its field example) the CMS
+field map at run time from
 ``source/Geant/proxy/test/BasicCpuTransport/data/`` (see
 ``source/Geant/proxy/src/ProxyDataManager.cu:49-122`` and
 ``source/Geant/proxy/ProxySeltzerBerger.hpp:134-152``).  This script copies
@@ -72,6 +73,12 @@ def main(ref_root):
         shutil.copyfile(os.path.join(data, "table", t), os.path.join(HERE, "table", t))
     for z in SB_Z:
         shutil.copyfile(os.path.join(data, "brem_SB", "br%d" % z), os.path.join(HERE, "brem_SB", "br%d" % z))
+    # the CMS solenoid field map of the reference's field example (181 x 161
+    # (r, z) points, read by examples/magneticfield/simplifiedCMS/inc/Geant/
+    # ScalarCMSmagField.h)
+    os.makedirs(os.path.join(HERE, "field"), exist_ok=True)
+    shutil.copyfile(os.path.join(ref_root, "examples/magneticfield/simplifiedCMS/cmsmagfield2015.txt"),
+                    os.path.join(HERE, "field", "cmsmagfield2015.txt"))
 
     src = open(os.path.join(ref_root, "source/Geant/proxy/ProxySandiaData.hpp")).read()
     nshell = [int(v) for v in _numbers(_array_body(src, "fNumberOfShells"))]

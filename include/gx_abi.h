@@ -91,6 +91,16 @@ int gx_table_invrange(gx_ctx *ctx, int table, int mat, const double *d_r, double
  * which: 0 = br11 (the reference's hard-coded slot 10), 1 = br18, 2 = br82. */
 int gx_sb_value(gx_ctx *ctx, int which, const double *d_x, const double *d_y, double *d_out, int n,
                 gx_stream_t s);
+/* Loads a field map in the format of the reference's CMS map
+ * (examples/magneticfield/simplifiedCMS/cmsmagfield2015.txt: lines
+ * "R(mm)= r phi(deg)= p Z(mm)= z Bz(tesla)= . Br(tesla)= . Bphi(tesla)= .",
+ * 181 x 161 (r, z) points, r outer, dr = 50 mm, dz = 200 mm, |z| <= 16 m) as
+ * ScalarCMSmagField::ReadVectorData reads it (ScalarCMSmagField.h:162-199);
+ * other lattices are rejected.  Used by transports with cfg.field_map = 1. */
+int gx_ctx_load_field_map(gx_ctx *ctx, const char *path);
+/* The map's field (tesla) at n points (mm, xyz interleaved):
+ * ScalarCMSmagField::GetFieldValue (ScalarCMSmagField.h:207-331). */
+int gx_field_value(gx_ctx *ctx, int n, const double *d_pos, double *d_B, gx_stream_t s);
 /* ProxyDataManager::GetCutValue(index, ipart) (ProxyDataManager.cuh:52-54), host. */
 int gx_cut_value(gx_ctx *ctx, int index, int ipart, double *out);
 /* The production-cut converter of the reference, CutConverter::Convert
@@ -203,6 +213,8 @@ typedef struct {
   int msc;                 /* 1: multiple scattering of e-/e+ (Urban-type: safety-based step limit, true /
                               geometric path conversion, angular deflection; no lateral displacement);
                               0: off (the reference has none, proxy/ProxyScattering.hpp:53-71) */
+  int field_map;           /* 1: the context's field map (gx_ctx_load_field_map) with fourth-order
+                              Runge-Kutta sub-steps, Bz ignored; 0: uniform Bz with the helix */
 } gx_transport_config;
 
 typedef struct {

@@ -40,4 +40,9 @@ ${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
   "$SRC/cuts/src/CutConverterForPositron.cpp" \
   "$SRC/cuts/src/Spline.cpp" \
   -x none "$STDCXX" -lm -o "$OUT/libgxref_cuts.so"
-echo "built $OUT/libgxref.so $OUT/libgxref_cuts.so"
+# the CMS field-map reader of the reference's field example, with its own shims
+${CXX:-g++} -std=c++14 -O2 -fPIC -shared -w -x c++ \
+  -I"$HERE/refshim_field" -I"$REF/examples/magneticfield/simplifiedCMS/inc" \
+  "$HERE/refshim_field/field_capi.cpp" \
+  -x none "$STDCXX" -lm -o "$OUT/libgxref_field.so"
+echo "built $OUT/libgxref.so $OUT/libgxref_cuts.so $OUT/libgxref_field.so"

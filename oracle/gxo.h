@@ -180,6 +180,7 @@ typedef struct {
   int nthreads;
   int score_events;        /* number of event tallies (>=1) */
   int msc;                 /* 1: multiple scattering of e-/e+ (gxo_transport.c) */
+  const float *field_map;  /* non-null: follow this field map (gxo_field_map_load) with RK4, Bz ignored */
 } gxo_config_t;
 
 typedef struct {
@@ -215,6 +216,15 @@ void gxo_msc_cos_batch(double Z, double X0, int n, double *states, double t, dou
 double gxo_msc_lambda1(const gxo_data_t *d, int type, int mat, double e);
 double gxo_msc_true_to_geom(double t, double lam);
 double gxo_msc_geom_to_true(double z, double lam, double tmax);
+
+/* field map in the reference's CMS format (gxo_field.c): ScalarCMSmagField,
+ * examples/magneticfield/simplifiedCMS/inc/Geant/ScalarCMSmagField.h:162-331.
+ * load: 181 x 161 x 4 floats (Br, Bphi, Bz premultiplied by 1/(dr dz), pad),
+ * NULL on error; value: tesla at pos (mm). */
+float *gxo_field_map_load(const char *path);
+void gxo_field_map_free(float *map);
+void gxo_field_map_value(const float *map, const double pos[3], double B[3]);
+void gxo_field_map_batch(const float *map, int n, const double *pos, double *B);
 
 /* production-cut conversion (gxo_cuts.c): CutConverter, cuts/src/CutConverter*.cpp */
 double gxo_cut_convert(int particle, int nelem, const double *Z, const double *n_atoms, double density, double cut,

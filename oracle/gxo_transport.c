@@ -458,6 +458,39 @@ static void make_secondary(const world_t *w, track_t *parent, stack_t *st, tally
   push(st, &s);
 }
 
+/* One classical fourth-order Runge-Kutta step of length s through the field
+ * map: du/ds = k u x B(x), k = 0.299792458 q / p; direction renormalised.
+ * (The reference has no stepper for non-uniform fields; this is the textbook
+ * method, the same operations as the CUDA engine's.) */
+static void rk4_map_step(const float *map, double k, double s, double x[3], double u[3], const double B0[3])
+{
+  double xs[3], us[3], B[3], kx[4][3], ku[4][3];
+  const double h[3] = {0.5 * s, 0.5 * s, s};
+  for (int j = 0; j < 3; ++j) kx[0][j] = u[j];
+  ku[0][0] = k * (u[1] * B0[2] - u[2] * B0[1]);
+  ku[0][1] = k * (u[2] * B0[0] - u[0] * B0[2]);
+  ku[0][2] = k * (u[0] * B0[1] - u[1] * B0[0]);
+  for (int st = 1; st < 4; ++st) {
+    for (int j = 0; j < 3; ++j) {
+      xs[j] = x[j] + h[st - 1] * kx[st - 1][j];
+      us[j] = u[j] + h[st - 1] * ku[st - 1][j];
+    }
+    gxo_field_map_value(map, xs, B);
+    for (int j = 0; j < 3; ++j) kx[st][j] = us[j];
+    ku[st][0] = k * (us[1] * B[2] - us[2] * B[1]);
+    ku[st][1] = k * (us[2] * B[0] - us[0] * B[2]);
+    ku[st][2] = k * (us[0] * B[1] - us[1] * B[0]);
+  }
+  double m = 0.0;
+  for (int j = 0; j < 3; ++j) {
+    x[j] += s / 6.0 * (kx[0][j] + 2.0 * kx[1][j] + 2.0 * kx[2][j] + kx[3][j]);
+    u[j] += s / 6.0 * (ku[0][j] + 2.0 * ku[1][j] + 2.0 * ku[2][j] + ku[3][j]);
+    m += u[j] * u[j];
+  }
+  m = 1.0 / sqrt(m);
+  for (int j = 0; j < 3; ++j) u[j] *= m;
+}
+
 /* Helix sub-steps in Bz (FieldPropagationHandler::Propagate/PropagateInVolume).
  * Returns the path length; *crossed and *newvol report a boundary crossing. */
 static double field_propagate(const world_t *w, track_t *tr, double pstep, int *crossed, int *newvol,
@@ -479,14 +512,34 @@ static double field_propagate(const world_t *w, track_t *tr, double pstep, int *
     else
       snext = fmax(2e-9, fmin(dist_to_out(w, tr->vol, tr->pos, tr->dir, &plane), remaining) + 2e-9);
     double step_gp = fmax(fmin(remaining, 1e-4), snext);
+    double np[3], nd[3], s;
+    if (w->c->field_map) {
+      /* the field map: the sub-step length from the field at the start
+       * point, then a Runge-Kutta step */
+      double B0[3];
+      gxo_field_map_value(w->c->field_map, tr->pos, B0);
+      const double *u = tr->dir;
+      double cx = u[1] * B0[2] - u[2] * B0[1], cy = u[2] * B0[0] - u[0] * B0[2], cz = u[0] * B0[1] - u[1] * B0[0];
+      double bperp = sqrt(cx * cx + cy * cy + cz * cz);
+      double step_field = DBL_MAX;
+      if (bperp > 0.0) step_field = fmax(2.0 * sqrt(eps * p / (0.299792458 * bperp)), saf);
+      s = fmin(fmin(step_gp, step_field), remaining);
+      for (int k = 0; k < 3; ++k) {
+        np[k] = tr->pos[k];
+        nd[k] = tr->dir[k];
+      }
+      if (bperp > 0.0)
+        rk4_map_step(w->c->field_map, 0.299792458 * charge / p, s, np, nd, B0);
+      else
+        for (int k = 0; k < 3; ++k) np[k] += s * nd[k];
+    } else {
     double pt = p * sqrt(fmax(1.0 - tr->dir[2] * tr->dir[2], 0.0));
     double step_field = DBL_MAX;
     if (pt > 0.0) {
       double curv = 0.299792458 * fabs(Bz) / pt;
       step_field = fmax(2.0 * sqrt(eps / curv), saf);
     }
-    double s = fmin(fmin(step_gp, step_field), remaining);
-    double np[3], nd[3];
+    s = fmin(fmin(step_gp, step_field), remaining);
     if (pt > 0.0) {
       gxo_helix_dostep_mm(Bz, tr->pos, tr->dir, charge, p, s, np, nd);
       double m = sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
@@ -498,6 +551,7 @@ static double field_propagate(const world_t *w, track_t *tr, double pstep, int *
         np[k] = tr->pos[k] + s * tr->dir[k];
         nd[k] = tr->dir[k];
       }
+    }
     }
     for (int k = 0; k < 3; ++k) {
       tr->pos[k] = np[k];
@@ -606,7 +660,7 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
   }
   int vol0 = tr->vol, crossed = 0, newvol = tr->vol;
   double step;
-  if (!charged || w->c->Bz == 0.0) {
+  if (!charged || (w->c->Bz == 0.0 && !w->c->field_map)) {
     int plane;
     double d = dist_to_out(w, tr->vol, tr->pos, tr->dir, &plane);
     if (d < pstep) {

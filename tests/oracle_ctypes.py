@@ -45,7 +45,8 @@ class Config(C.Structure):
     _fields_ = [("geometry", I), ("axis", I), ("nlayers", I), ("t_abs", D), ("t_gap", D),
                 ("half_trans", D), ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I),
                 ("Bz", D), ("charged_local", I), ("max_steps", I), ("seed", D * 6),
-                ("first_substream", L), ("nthreads", I), ("score_events", I), ("msc", I)]
+                ("first_substream", L), ("nthreads", I), ("score_events", I), ("msc", I),
+                ("field_map", C.c_void_p)]
 
 
 MODEL_IDS = {"kn": 0, "sg": 1, "bh": 2, "sb": 3, "mb": 4, "bhabha": 5, "annih": 6}
@@ -210,6 +211,25 @@ class Oracle:
         res = dict(zip(names, [int(c) for c in counters]))
         res.update(edep=edep, escaped=esc.value, primary_steps=psteps)
         return res
+
+    # ------------------------------------------------------------ field map
+    def field_map_load(self, path):
+        """load a map in the reference's CMS format; the handle goes into
+        Config.field_map"""
+        f = self.lib.gxo_field_map_load
+        f.restype = C.c_void_p
+        f.argtypes = [C.c_char_p]
+        h = f(path.encode())
+        assert h, path
+        return h
+
+    def field_map_value(self, handle, pos):
+        f = self.lib.gxo_field_map_batch
+        f.argtypes = [C.c_void_p, I, C.POINTER(D), C.POINTER(D)]
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        B = np.zeros_like(pos)
+        f(handle, len(pos), dp(pos), dp(B))
+        return B
 
     # --------------------------------------------------- multiple scattering
     def material(self, Z, A, density):
