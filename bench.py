@@ -296,6 +296,30 @@ def main():
     out["with_multiple_scattering"] = {"value": msteps / (msm / 1e3), "unit": UNIT, "steps": int(msteps),
                                        "substeps": int(stm["substeps"]), "ms": msm}
 
+    # the other two throughput workloads on the same engine (FP32-mixed):
+    # C4, 2^16 mixed e-/e+/gamma, log-uniform 10 MeV - 100 GeV, 4 T along z;
+    # C5, events of Poisson(100) 10 GeV electrons scored per event (256 of the
+    # 4096 events, to keep the run short)
+    extra = {}
+    for name, fn in (("c4", lambda: configs.c4(65536)), ("c5", lambda: configs.c5(256, 100))):
+        c, pr, nv = fn()
+        c.precision, c.engine, c.first_substream = 1, 1, rank * len(pr[0])
+        tens = [torch.as_tensor(x, device="cuda") if x is not None else None for x in pr]
+        gx.transport(dm, c, *tens[:4], events=tens[4], nvol=nv)  # warm-up
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _, stx, _ = gx.transport(dm, c, *tens[:4], events=tens[4], nvol=nv)
+        e1.record()
+        barrier()
+        msx = e0.elapsed_time(e1)
+        extra[name] = {"track_steps_per_s": stx["steps"] / (msx / 1e3), "primaries_per_s": len(pr[0]) / (msx / 1e3),
+                       "primaries": len(pr[0]), "steps": stx["steps"], "ms": msx}
+        if name == "c5":
+            extra[name]["events"] = int(c.nevents)
+            extra[name]["events_per_s"] = c.nevents / (msx / 1e3)
+    out["other_workloads"] = extra
+
     # e2e through the host-buffer entry point (warm-up calls first: the FP64
     # runs above released the FP32 engine's stores)
     cfg.precision, cfg.engine, cfg.profile = 1, 1, 0

@@ -37,11 +37,12 @@ constexpr int kDefaultBlocksPerSM = 4;
 // Steps of one track per transport-kernel launch in the batched engine, at
 // most (a track is kept in registers while it neither interacts nor dies).
 constexpr int kDefaultStepsPerLaunch = 16;
-// Primary energy per injection wave for stores of cap slots: a 10 GeV shower
-// peaks near 800 tracks in flight, ~0.08 per MeV of primary energy; waves are
-// sized so that their showers would peak at `fill` x cap if they all peaked
-// together (they do not: waves overlap as showers age).  The batched engine
-// uses fill 0.8 (fastest in the sweep on C3), the plain loop 0.4.
-inline double default_wave_energy(long long cap, double fill) { return fill * (double)cap / 0.08; }
+// Live energy (injected primary energy not yet deposited or escaped) allowed
+// before more primaries are injected, for stores of cap slots: showers started
+// together in the Pb/LAr calorimeter peak at 0.052-0.062 tracks in flight per
+// MeV (all types together; 10 MeV-100 GeV primaries, 4 T), so at 0.064 per MeV
+// the population stays below `fill` x cap.  The batched engine uses fill 0.8,
+// the plain loop 0.4.
+inline double default_wave_energy(long long cap, double fill) { return fill * (double)cap / 0.064; }
 
 } // namespace gx

@@ -63,8 +63,9 @@ struct Ctl {
   long long in_flight, pending, peak, iterations;
   unsigned long long stat[kNStat];
   double escaped;
+  double retired;     // energy deposited or escaped so far (the rest is still carried by tracks)
   const double *cumE; // inclusive prefix sum of the primary energies
-  double wave_energy; // primary energy injected per wave, at most
+  double wave_energy; // energy carried by live tracks before more primaries are injected, at most
   long long refill_below, stack_cap;
   long long qcount[3][3]; // records in the interaction buffers [particle][process]
   long long take[3];      // tracks of the current stores handed out to the transport kernels
@@ -328,12 +329,19 @@ struct Local {
   // deposits go to a shared-memory tally when it fits, else to global memory
   double *sm_edep;
   double *g_edep;
+  double *sm_esc; // this block's [escaped, retired] energy sums (shared memory)
   int nvol, nevents, sm_bins;
-  double escaped;
+  double retired; // energy this thread took out of the live tracks (deposited or escaped)
   unsigned int st[kNStat];
   int err;
+  __device__ __forceinline__ void escape(double e)
+  {
+    retired += e;
+    atomicAdd(sm_esc, e);
+  }
   __device__ __forceinline__ void deposit(int event, int vol, double e)
   {
+    retired += e;
     if (vol < 0 || vol >= nvol || e == 0.0) return;
     if (event < 0 || event >= nevents) { // a primary with an event index outside the tally
       err |= kErrOverflow;
@@ -632,16 +640,47 @@ template <class R> struct StepCtx {
   __device__ __forceinline__ R xs(int i) const { return i == 0 ? xs0 : (i == 1 ? xs1 : xs2); }
 };
 
+// A photon's cross sections in the two calorimeter materials while its energy
+// does not change (it stays in a transport kernel until it interacts):
+// computed at its first step in each material, reused after.
+template <class R> struct GammaXs {
+  R pb0, pb1, pb2, ar0, ar1, ar2;
+  int have; // bit 0: lead (material 1), bit 1: argon (material 2)
+};
+
 // GPIL and step limit.  Returns true when the step continues with helix
-// sub-steps (a charged track in a field), false when it is complete.
+// sub-steps (a charged track in a field), false when it is complete.  gx,
+// when given, caches a photon's cross sections per material.
 template <class R>
-__device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c)
+__device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c,
+                                           GammaXs<R> *gx = nullptr)
 {
   const int mat = vol_material(g, t.vol);
   const int np = (t.type == 1) ? 2 : 3;
   const bool charged = t.type != 0;
   R xs[3];
-  cross_sections<R>(d, t.type, mat, t.E, xs);
+  if (gx && mat == 1 && (gx->have & 1)) {
+    xs[0] = gx->pb0;
+    xs[1] = gx->pb1;
+    xs[2] = gx->pb2;
+  } else if (gx && mat == 2 && (gx->have & 2)) {
+    xs[0] = gx->ar0;
+    xs[1] = gx->ar1;
+    xs[2] = gx->ar2;
+  } else {
+    cross_sections<R>(d, t.type, mat, t.E, xs);
+    if (gx && mat == 1) {
+      gx->pb0 = xs[0];
+      gx->pb1 = xs[1];
+      gx->pb2 = xs[2];
+      gx->have |= 1;
+    } else if (gx && mat == 2) {
+      gx->ar0 = xs[0];
+      gx->ar1 = xs[1];
+      gx->ar2 = xs[2];
+      gx->have |= 2;
+    }
+  }
   c.xs0 = xs[0];
   c.xs1 = xs[1];
   c.xs2 = xs[2];
@@ -890,7 +929,7 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
           *proc = 2;
           return kInteract;
         }
-        L.escaped += 2.0 * kEMass;
+        L.escape(2.0 * kEMass);
       }
       return kDone;
     }
@@ -900,7 +939,7 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
     t.msc_r0 = R(-1); // a new volume: the step limit starts again
     t.vol = c.newvol;
     if (c.newvol < 0) {
-      L.escaped += (double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0);
+      L.escape((double)t.E + ((t.type == 2) ? 2.0 * kEMass : 0.0));
       return kDone;
     }
     return kAlive;
@@ -1032,16 +1071,17 @@ __device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *ede
   L.nevents = g.nevents;
   L.g_edep = edep;
   L.sm_edep = sm_edep;
+  L.sm_esc = sm_esc;
   // event row 0 of the tally lives in shared memory when it fits in 6 KB
   L.sm_bins = (g.nvol <= 768) ? g.nvol : 0;
   for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x) sm_edep[k] = 0.0;
   for (int k = threadIdx.x; k < kNStat; k += blockDim.x) sm_stat[k] = 0;
   if (threadIdx.x == 0) {
-    *sm_esc = 0.0;
+    sm_esc[0] = sm_esc[1] = 0.0;
     *sm_err = 0;
   }
   __syncthreads();
-  L.escaped = 0.0;
+  L.retired = 0.0;
   L.err = 0;
 #pragma unroll
   for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
@@ -1053,7 +1093,7 @@ __device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, doub
 #pragma unroll
   for (int k = 0; k < kNStat; ++k)
     if (L.st[k]) atomicAdd(&sm_stat[k], (unsigned long long)L.st[k]);
-  if (L.escaped != 0.0) atomicAdd(sm_esc, L.escaped);
+  if (L.retired != 0.0) atomicAdd(&sm_esc[1], L.retired);
   if (L.err) atomicOr(sm_err, L.err);
   __syncthreads();
   for (int k = threadIdx.x; k < L.sm_bins; k += blockDim.x)
@@ -1061,7 +1101,8 @@ __device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, doub
   for (int k = threadIdx.x; k < kNStat; k += blockDim.x)
     if (sm_stat[k]) atomicAdd(&ctl->stat[k], sm_stat[k]);
   if (threadIdx.x == 0) {
-    if (*sm_esc != 0.0) atomicAdd(&ctl->escaped, *sm_esc);
+    if (sm_esc[0] != 0.0) atomicAdd(&ctl->escaped, sm_esc[0]);
+    if (sm_esc[1] != 0.0) atomicAdd(&ctl->retired, sm_esc[1]);
     if (*sm_err) atomicOr(&ctl->err_flags, *sm_err);
   }
 }
@@ -1139,7 +1180,7 @@ template <class R, int PT, int FM> __device__ __forceinline__ void step_body(con
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
-  __shared__ double sm_esc;
+  __shared__ double sm_esc[2];
   __shared__ int sm_err;
   const Data &d = *a.d;
   Ctl *ctl = a.ctl;
@@ -1148,7 +1189,7 @@ template <class R, int PT, int FM> __device__ __forceinline__ void step_body(con
   const Store<R> &cur = a.st[par][SRC];
   const long long n = min(ctl->count[par][SRC], cur.cap);
   Local L;
-  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
     long long i = base + threadIdx.x;
@@ -1165,7 +1206,7 @@ template <class R, int PT, int FM> __device__ __forceinline__ void step_body(con
     }
     emit_tracks<R, SRC>(a, ctl, par, active, alive, t, sec, L);
   }
-  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
 }
 
 // Arguments by value (the allocation-free entry point) or from a device copy.
@@ -1218,7 +1259,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
-  __shared__ double sm_esc;
+  __shared__ double sm_esc[2];
   __shared__ int sm_err;
   const Args<R> &a = *A;
   const Data &d = *a.d;
@@ -1228,10 +1269,12 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
   const long long n = min(ctl->count[par][PT], cur.cap);
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
   Local L;
-  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
   const int budget = a.step_budget;
   Track<R> t;
   StepCtx<R> c;
+  GammaXs<R> gxs;
+  gxs.have = 0;
   bool have = false, more = true; // `more` is warp-uniform: the work counter is not exhausted
   bool infield = false;           // in the middle of a step (helix sub-steps)
   int nst = 0;
@@ -1251,6 +1294,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
           have = true;
           infield = false;
           nst = 0;
+          gxs.have = 0; // a new photon energy
         }
       }
       if ((long long)base + __popc(need) >= n) more = false;
@@ -1259,7 +1303,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
     int r = kDone, proc = -1;
     bool done = false; // a step ends in this pass
     if (have && !infield) {
-      infield = step_begin(d, a.g, t, c);
+      infield = step_begin(d, a.g, t, c, PT == 0 ? &gxs : nullptr);
       done = !infield;
     }
     if (PT != 0 && have && infield && field_substep<R, FM>(d, a.g, t, c, L)) {
@@ -1299,7 +1343,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
     }
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
-  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
 }
 
 // Post-step interaction of process PROC for the buffered tracks of type PT:
@@ -1309,7 +1353,7 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMin
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
-  __shared__ double sm_esc;
+  __shared__ double sm_esc[2];
   __shared__ int sm_err;
   const Args<R> &a = *A;
   const Data &d = *a.d;
@@ -1319,7 +1363,7 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMin
   const long long n = min(ctl->qcount[PT][PROC], a.qcap);
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
   Local L;
-  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
   const long long stride = (long long)gridDim.x * blockDim.x;
   for (long long base = (long long)blockIdx.x * blockDim.x; base < n; base += stride) {
     long long j = base + threadIdx.x;
@@ -1336,7 +1380,7 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMin
     }
     emit_tracks<R, PT>(a, ctl, par, active, alive, t, sec, L);
   }
-  tally_end(L, ctl, a.edep, sm_edep, sm_stat, &sm_esc, &sm_err);
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
 }
 
 // End of an iteration: the next stores become current, the refill plan for
@@ -1377,21 +1421,27 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
     budget -= take;
     pend += ctl->stack_count[q];
   }
-  // primaries: a wave carries at most wave_energy (a shower's population peaks
-  // in proportion to its energy, long after the wave is injected)
+  // primaries: a shower's population peaks in proportion to its energy, long
+  // after it is injected, so primaries are injected only while the energy the
+  // live tracks carry (injected minus deposited or escaped) stays within
+  // wave_energy; one primary at least once nothing is left in flight
   long long tp = 0;
   if (budget > 0 && ctl->prim_next < ctl->nprim) {
     long long lo = ctl->prim_next, hi = min(ctl->nprim, ctl->prim_next + budget);
     double e0 = lo > 0 ? ctl->cumE[lo - 1] : 0.0;
-    // largest k in (lo, hi] with cumE[k - 1] - e0 <= wave_energy; at least one primary
-    long long a = lo + 1, b = hi;
+    const double room = ctl->wave_energy - (e0 - ctl->retired);
+    // largest k in [lo, hi] with cumE[k - 1] - e0 <= room
+    long long a = lo, b = hi;
     while (a < b) {
       long long m = (a + b + 1) / 2;
-      if (ctl->cumE[m - 1] - e0 <= ctl->wave_energy)
+      if (ctl->cumE[m - 1] - e0 <= room)
         a = m;
       else
         b = m - 1;
     }
+    long long live = 0;
+    for (int q = 0; q < nstores; ++q) live += ctl->count[np][q] + ctl->stack_count[q];
+    if (a == lo && live == 0) a = lo + 1;
     tp = a - lo;
   }
   ctl->take_prim = tp;
@@ -1490,6 +1540,7 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
     atomicAdd(&ctl->stat[S_TRACKS], 1ULL);
     if (t.vol < 0) {
       atomicAdd(&ctl->escaped, (double)t.E);
+      atomicAdd(&ctl->retired, (double)t.E);
       continue;
     }
     int qs = (a.nstores == 1) ? 0 : t.type;
@@ -2186,7 +2237,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   h.nprim = nprim;
   h.iterations = -1;
   h.cumE = cumE;
-  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : 0.4 * (double)cap / 0.08;
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, 0.4);
   h.refill_below = L.a.refill_below;
   h.stack_cap = cap;
   if ((err = cudaMemcpyAsync(ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||

@@ -207,7 +207,8 @@ typedef struct {
   long long refill_below;  /* inject / refill when fewer tracks than this are in flight (0: default) */
   int graph_iters;         /* iterations per CUDA-graph launch between host checks (0: default) */
   int profile;             /* 1: no graph; CUDA events around every step kernel (per-kernel times in stats) */
-  double wave_energy;      /* primary energy (MeV) injected per wave, at most (0: from capacity) */
+  double wave_energy;      /* energy (MeV) carried by live tracks before more primaries are injected,
+                              at most (0: from capacity) */
   int steps_per_launch;    /* batched engine: steps of one track per transport launch, at most; a track
                               stays in registers between them (0: default 16; 1: one step per iteration) */
   int msc;                 /* 1: multiple scattering of e-/e+ (Urban-type: safety-based step limit, true /
