@@ -171,7 +171,7 @@ def main():
     import torch.distributed as dist
 
     import geantexascalepilot_b200 as gx
-    from geantexascalepilot_b200 import configs
+    from geantexascalepilot_b200 import configs, geometry
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -300,10 +300,16 @@ def main():
     # C4, 2^16 mixed e-/e+/gamma, log-uniform 10 MeV - 100 GeV, 4 T along z;
     # C5, events of Poisson(100) 10 GeV electrons scored per event (256 of the
     # 4096 events, to keep the run short)
+    # and C3 itself through the CSG volume tree (the calorimeter built from
+    # placed boxes, as the reference's detector construction does)
     extra = {}
-    for name, fn in (("c4", lambda: configs.c4(65536)), ("c5", lambda: configs.c5(256, 100))):
+    for name, fn in (("c4", lambda: configs.c4(65536)), ("c5", lambda: configs.c5(256, 100)),
+                     ("c3_csg_tree", lambda: configs.c3())):
         c, pr, nv = fn()
         c.precision, c.engine, c.first_substream = 1, 1, rank * len(pr[0])
+        if name == "c3_csg_tree":
+            dm.load_geometry(geometry.calorimeter(axis=c.axis))
+            c.geometry = 2
         tens = [torch.as_tensor(x, device="cuda") if x is not None else None for x in pr]
         gx.transport(dm, c, *tens[:4], events=tens[4], nvol=nv)  # warm-up
         barrier()

@@ -13,4 +13,4 @@ from .api import (ANNIHILATION, BETHE_HEITLER, BHABHA, ELECTRON, GAMMA, KLEIN_NI
                   ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, autotune,
                   cut_convert, default_config, egamma_gun, hepevt_load, hepevt_read, pdg_to_type, set_direction_xyz, transport,
                   transport_host, transport_noalloc)
-from . import configs, sharding  # noqa: F401
+from . import configs, geometry, sharding  # noqa: F401

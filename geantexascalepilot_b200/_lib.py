@@ -125,6 +125,17 @@ _SIGS = {
     "gx_hepevt_load": (I, [C.c_char_p, I, I, PD, I, P, P, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I), P]),
     "gx_transport_run_noalloc": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I,
                                      C.POINTER(TransportStats), P]),
+    "gx_geom_create": (I, [C.POINTER(P)]),
+    "gx_geom_destroy": (None, [P]),
+    "gx_geom_box": (I, [P, D, D, D, C.POINTER(I)]),
+    "gx_geom_tube": (I, [P, D, D, D, C.POINTER(I)]),
+    "gx_geom_sphere": (I, [P, D, D, C.POINTER(I)]),
+    "gx_geom_logical_volume": (I, [P, I, I, I, C.POINTER(I)]),
+    "gx_geom_place_daughter": (I, [P, I, I, PD, PD, C.POINTER(I)]),
+    "gx_geom_close": (I, [P, I, C.POINTER(I), C.POINTER(I)]),
+    "gx_geom_touchable": (I, [P, I, C.POINTER(I), C.POINTER(I), C.POINTER(I), PD, PD]),
+    "gx_ctx_load_geometry": (I, [P, P]),
+    "gx_geom_probe": (I, [P, I, P, P, P, P, P, P, P, P]),
 }
 for _name, (_res, _args) in _SIGS.items():
     _f = getattr(lib, _name)

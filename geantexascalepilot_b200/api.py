@@ -83,6 +83,12 @@ class ProxyDataManager:
         path = path or os.path.join(_lib.DATA_DIR, "field", "cmsmagfield2015.txt")
         check(lib.gx_ctx_load_field_map(self.handle, path.encode()))
 
+    def load_geometry(self, tree):
+        """Upload a closed CSG volume tree (geometry.CsgGeometry, from
+        GeoManager.CloseGeometry) for transport geometry 2
+        (gx_ctx_load_geometry); returns its number of tally columns (nvol)."""
+        return tree.load(self)
+
     def field_value(self, pos):
         """The loaded map's field (tesla) at positions (mm), shape (n, 3)."""
         p = _dev(pos, torch.float64).reshape(-1, 3).contiguous()

@@ -1,0 +1,395 @@
+// gx_csg.cuh -- CSG geometry on the device: a volume tree of placed solids,
+// flattened into touchables (transport geometry 2).
+//
+// The reference's navigation is VecGeom's (NavigationInterface::
+// FindNextBoundary, source/Geant/geometry/NavigationInterface.hpp:63-98:
+// FindNextBoundaryAndStepAndSafety, then the snext / safety / boundary
+// bookkeeping; IsSameLocation :43-60 relocates after a step), over a tree
+// built from unplaced solids, logical volumes and placed daughters
+// (source/Geant/proxy/test/BasicCpuTransport/ProxyDetectorConstruction.cpp:
+// 241-324).  VecGeom is not part of the reference sources; this is a
+// restatement of the standard ray/solid algorithms for the solids that
+// calorimeters are built from:
+//   - each touchable (one placed instance; the whole tree unrolled, as
+//     VecGeom's navigation-state index does) carries its global transform
+//     x_global = R x_local + t, its solid, material, parent and a contiguous
+//     run of children; a track's volume is one int, like the layered
+//     navigator's;
+//   - step: the distance to leave the current solid, and to enter each child
+//     whose padded bounding box the ray meets before that (and before the
+//     physics step);
+//   - after a crossing: into the child that was hit, then down into the child
+//     containing the point; or up through the parents until one contains it,
+//     then down;
+//   - on a surface (within a tolerance) "contains" is decided by the
+//     direction: a point on a face it moves out through is outside;
+//   - safety: to the current solid's surface and, for each child, the larger
+//     of the distance to its bounding box and the solid's own lower bound.
+// Solids: box (half lengths), tube (rmin, rmax, half length; full phi),
+// sphere (rmin, rmax).  Quadratic roots in the cancellation-free form.
+// Products and sums are rounded separately (__dmul_rn / __dadd_rn), so that
+// the results do not depend on FMA contraction.
+#pragma once
+
+#include <cstdint>
+
+namespace gx {
+
+enum { kCsgBox = 0, kCsgTube = 1, kCsgSphere = 2 };
+constexpr double kCsgTol = 1e-9;    // surface tolerance (mm)
+constexpr double kCsgPad = 1e-6;    // bounding-box padding (mm)
+constexpr int kCsgMaxDepth = 64;    // tree depth, at most
+constexpr int kCsgMaxNodes = 1 << 22;
+constexpr double kCsgInf = 1.7976931348623157e308;
+
+struct CsgNode {
+  double t[3];         // global translation
+  double r[9];         // global rotation, row-major (x_global = R x_local + t)
+  double lo[3], hi[3]; // global bounding box, padded
+  double a, b, c;      // box: half lengths; tube: rmin, rmax, half length in z; sphere: rmin, rmax
+  int kind, rot;       // rot 0: R is the identity
+  int mat, parent, kid0, nkid;
+};
+
+struct CsgView {
+  const CsgNode *node; // node 0 is the world
+  const int *kids;
+};
+
+__device__ __forceinline__ double cmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double cadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double csub(double a, double b) { return __dsub_rn(a, b); }
+
+__device__ __forceinline__ void csg_local(const CsgNode &n, const double *p, const double *d, double *q, double *e)
+{
+  const double x0 = p[0] - n.t[0], x1 = p[1] - n.t[1], x2 = p[2] - n.t[2];
+  if (!n.rot) {
+    q[0] = x0;
+    q[1] = x1;
+    q[2] = x2;
+    e[0] = d[0];
+    e[1] = d[1];
+    e[2] = d[2];
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) { // R^T
+    q[k] = cadd(cadd(cmul(n.r[k], x0), cmul(n.r[3 + k], x1)), cmul(n.r[6 + k], x2));
+    e[k] = cadd(cadd(cmul(n.r[k], d[0]), cmul(n.r[3 + k], d[1])), cmul(n.r[6 + k], d[2]));
+  }
+}
+__device__ __forceinline__ void csg_local_point(const CsgNode &n, const double *p, double *q)
+{
+  const double x0 = p[0] - n.t[0], x1 = p[1] - n.t[1], x2 = p[2] - n.t[2];
+  if (!n.rot) {
+    q[0] = x0;
+    q[1] = x1;
+    q[2] = x2;
+    return;
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) q[k] = cadd(cadd(cmul(n.r[k], x0), cmul(n.r[3 + k], x1)), cmul(n.r[6 + k], x2));
+}
+
+__device__ __forceinline__ double dot2(const double *a, const double *b) { return cadd(cmul(a[0], b[0]), cmul(a[1], b[1])); }
+__device__ __forceinline__ double dot3(const double *a, const double *b)
+{
+  return cadd(cadd(cmul(a[0], b[0]), cmul(a[1], b[1])), cmul(a[2], b[2]));
+}
+
+// inside, or on the surface and not moving out through it
+__device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const double *q, const double *e, double tol)
+{
+  if (n.kind == kCsgBox) {
+    const double h0 = n.a, h1 = n.b, h2 = n.c;
+    const double a0 = fabs(q[0]), a1 = fabs(q[1]), a2 = fabs(q[2]);
+    if (a0 > h0 + tol || a1 > h1 + tol || a2 > h2 + tol) return false;
+    if (a0 >= h0 - tol && cmul(q[0], e[0]) > 0.0) return false;
+    if (a1 >= h1 - tol && cmul(q[1], e[1]) > 0.0) return false;
+    if (a2 >= h2 - tol && cmul(q[2], e[2]) > 0.0) return false;
+    return true;
+  }
+  double r, out;
+  if (n.kind == kCsgTube) {
+    const double az = fabs(q[2]);
+    if (az > n.c + tol) return false;
+    if (az >= n.c - tol && cmul(q[2], e[2]) > 0.0) return false;
+    r = sqrt(dot2(q, q));
+    out = dot2(q, e);
+  } else {
+    r = sqrt(dot3(q, q));
+    out = dot3(q, e);
+  }
+  if (r > n.b + tol) return false;
+  if (r >= n.b - tol && out > 0.0) return false;
+  if (n.a > 0.0) {
+    if (r < n.a - tol) return false;
+    if (r <= n.a + tol && out < 0.0) return false;
+  }
+  return true;
+}
+
+// roots of a t^2 + 2 b t + c = 0 with sq = sqrt(b^2 - a c)
+__device__ __forceinline__ double far_root(double a, double b, double c, double sq)
+{
+  return b > 0.0 ? -c / cadd(b, sq) : csub(sq, b) / a;
+}
+__device__ __forceinline__ double near_root(double a, double b, double c, double sq)
+{
+  return b < 0.0 ? c / csub(sq, b) : -cadd(b, sq) / a;
+}
+
+// distance to leave the solid from a point inside it (or on its surface)
+__device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const double *q, const double *e)
+{
+  double s = kCsgInf;
+  if (n.kind == kCsgBox) {
+    const double h[3] = {n.a, n.b, n.c};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double t = kCsgInf;
+      if (e[k] > 0.0)
+        t = (h[k] - q[k]) / e[k];
+      else if (e[k] < 0.0)
+        t = (-h[k] - q[k]) / e[k];
+      s = fmin(s, t);
+    }
+    return s < 0.0 ? 0.0 : s;
+  }
+  double a, b, r2;
+  if (n.kind == kCsgTube) {
+    if (e[2] > 0.0)
+      s = (n.c - q[2]) / e[2];
+    else if (e[2] < 0.0)
+      s = (-n.c - q[2]) / e[2];
+    a = dot2(e, e);
+    b = dot2(q, e);
+    r2 = dot2(q, q);
+  } else {
+    a = dot3(e, e);
+    b = dot3(q, e);
+    r2 = dot3(q, q);
+  }
+  if (a > 0.0) {
+    const double c = csub(r2, cmul(n.b, n.b)), D = csub(cmul(b, b), cmul(a, c));
+    s = fmin(s, far_root(a, b, c, sqrt(D > 0.0 ? D : 0.0)));
+    if (n.a > 0.0 && b < 0.0) {
+      const double c2 = csub(r2, cmul(n.a, n.a)), D2 = csub(cmul(b, b), cmul(a, c2));
+      if (D2 >= 0.0) s = fmin(s, near_root(a, b, c2, sqrt(D2)));
+    }
+  }
+  return s < 0.0 ? 0.0 : s;
+}
+
+// distance to enter the solid from a point outside it; kCsgInf if missed
+__device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const double *q, const double *e)
+{
+  const double tol = kCsgTol;
+  if (n.kind == kCsgBox) {
+    const double h[3] = {n.a, n.b, n.c};
+    double tmin = -kCsgInf, tmax = kCsgInf;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (e[k] == 0.0) {
+        if (fabs(q[k]) > h[k]) return kCsgInf;
+        continue;
+      }
+      double t0 = (-h[k] - q[k]) / e[k], t1 = (h[k] - q[k]) / e[k];
+      if (t0 > t1) {
+        const double x = t0;
+        t0 = t1;
+        t1 = x;
+      }
+      tmin = fmax(tmin, t0);
+      tmax = fmin(tmax, t1);
+    }
+    if (!(tmax > tmin) || tmax <= tol) return kCsgInf;
+    return tmin < 0.0 ? 0.0 : tmin;
+  }
+  double s = kCsgInf;
+  const double rmin = n.a, rmax = n.b;
+  double a, b, r2;
+  if (n.kind == kCsgTube) {
+    const double dz = n.c;
+    double tz = -1.0;
+    if (q[2] >= dz && e[2] < 0.0)
+      tz = (dz - q[2]) / e[2];
+    else if (q[2] <= -dz && e[2] > 0.0)
+      tz = (-dz - q[2]) / e[2];
+    if (tz >= 0.0) {
+      const double x = cadd(q[0], cmul(tz, e[0])), y = cadd(q[1], cmul(tz, e[1]));
+      const double r = sqrt(cadd(cmul(x, x), cmul(y, y)));
+      if (r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol)) s = tz;
+    }
+    a = dot2(e, e);
+    b = dot2(q, e);
+    r2 = dot2(q, q);
+    if (a > 0.0) {
+      const double c = csub(r2, cmul(rmax, rmax)), D = csub(cmul(b, b), cmul(a, c));
+      if (c >= 0.0 && b < 0.0 && D >= 0.0) { // the outer surface from outside
+        const double t = near_root(a, b, c, sqrt(D));
+        if (t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol) s = t;
+      }
+      if (rmin > 0.0) { // the inner surface from the bore
+        const double c2 = csub(r2, cmul(rmin, rmin)), D2 = csub(cmul(b, b), cmul(a, c2));
+        if (D2 >= 0.0) {
+          const double t = far_root(a, b, c2, sqrt(D2));
+          if (t >= 0.0 && t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol) s = t;
+        }
+      }
+    }
+    return s;
+  }
+  a = dot3(e, e);
+  b = dot3(q, e);
+  r2 = dot3(q, q);
+  const double c = csub(r2, cmul(rmax, rmax)), D = csub(cmul(b, b), cmul(a, c));
+  if (c >= 0.0 && b < 0.0 && D >= 0.0) s = near_root(a, b, c, sqrt(D));
+  if (rmin > 0.0) {
+    const double c2 = csub(r2, cmul(rmin, rmin)), D2 = csub(cmul(b, b), cmul(a, c2));
+    if (D2 >= 0.0) {
+      const double t = far_root(a, b, c2, sqrt(D2));
+      if (t >= 0.0 && t < s) s = t;
+    }
+  }
+  return s;
+}
+
+__device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const double *q)
+{
+  if (n.kind == kCsgBox) return fmin(fmin(n.a - fabs(q[0]), n.b - fabs(q[1])), n.c - fabs(q[2]));
+  if (n.kind == kCsgTube) {
+    const double r = sqrt(dot2(q, q)), s = fmin(n.c - fabs(q[2]), n.b - r);
+    return n.a > 0.0 ? fmin(s, r - n.a) : s;
+  }
+  const double r = sqrt(dot3(q, q));
+  return n.a > 0.0 ? fmin(n.b - r, r - n.a) : n.b - r;
+}
+
+// a lower bound of the distance to the solid from a point outside it
+__device__ __forceinline__ double csg_safety_in_local(const CsgNode &n, const double *q)
+{
+  if (n.kind == kCsgBox) return fmax(fmax(fabs(q[0]) - n.a, fabs(q[1]) - n.b), fabs(q[2]) - n.c);
+  if (n.kind == kCsgTube) {
+    const double r = sqrt(dot2(q, q));
+    return fmax(fmax(fabs(q[2]) - n.c, r - n.b), n.a - r);
+  }
+  const double r = sqrt(dot3(q, q));
+  return fmax(r - n.b, n.a - r);
+}
+
+__device__ __forceinline__ double csg_bbox_gap(const CsgNode &n, const double *p)
+{
+  double g = -kCsgInf;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) g = fmax(g, fmax(n.lo[k] - p[k], p[k] - n.hi[k]));
+  return g;
+}
+
+// entry distance of the ray into the bounding box, kCsgInf if missed
+__device__ __forceinline__ double csg_bbox_ray(const CsgNode &n, const double *p, const double *d)
+{
+  double tmin = 0.0, tmax = kCsgInf;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    if (d[k] == 0.0) {
+      if (p[k] < n.lo[k] || p[k] > n.hi[k]) return kCsgInf;
+      continue;
+    }
+    double t0 = (n.lo[k] - p[k]) / d[k], t1 = (n.hi[k] - p[k]) / d[k];
+    if (t0 > t1) {
+      const double x = t0;
+      t0 = t1;
+      t1 = x;
+    }
+    tmin = fmax(tmin, t0);
+    tmax = fmin(tmax, t1);
+  }
+  return tmax < tmin ? kCsgInf : tmin;
+}
+
+__device__ __forceinline__ bool csg_contains(const CsgView &g, int v, const double *p, const double *d, double tol)
+{
+  const CsgNode &n = g.node[v];
+  if (csg_bbox_gap(n, p) > 0.0) return false;
+  double q[3], e[3];
+  csg_local(n, p, d, q, e);
+  return csg_contains_local(n, q, e, tol);
+}
+
+// the deepest touchable at or below v (which contains p) that contains p
+__device__ __forceinline__ int csg_descend(const CsgView &g, int v, const double *p, const double *d, double tol)
+{
+  for (int depth = 0; depth < kCsgMaxDepth; ++depth) {
+    const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
+    int next = -1;
+    for (int k = 0; k < nk && next < 0; ++k) {
+      const int c = g.kids[k0 + k];
+      if (csg_contains(g, c, p, d, tol)) next = c;
+    }
+    if (next < 0) return v;
+    v = next;
+  }
+  return v;
+}
+
+// from touchable v up until one contains p, then down; -1 outside the world
+__device__ __forceinline__ int csg_locate(const CsgView &g, int v, const double *p, const double *d, double tol)
+{
+  if (v < 0) v = 0;
+  for (int depth = 0; v >= 0 && depth <= kCsgMaxDepth; ++depth) {
+    if (csg_contains(g, v, p, d, tol)) return csg_descend(g, v, p, d, tol);
+    v = g.node[v].parent;
+  }
+  return -1;
+}
+
+// distance to the next boundary from p in v; children whose bounding box the
+// ray reaches only beyond `limit` are skipped (the result is then >= limit);
+// hit = the child entered, -1 when leaving v
+__device__ __forceinline__ double csg_step(const CsgView &g, int v, const double *p, const double *d, double limit,
+                                           int &hit)
+{
+  double q[3], e[3];
+  csg_local(g.node[v], p, d, q, e);
+  double s = csg_dist_out_local(g.node[v], q, e);
+  hit = -1;
+  const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
+  for (int k = 0; k < nk; ++k) {
+    const int c = g.kids[k0 + k];
+    const double tb = csg_bbox_ray(g.node[c], p, d);
+    if (!(tb < s && tb < limit)) continue;
+    csg_local(g.node[c], p, d, q, e);
+    const double t = csg_dist_in_local(g.node[c], q, e);
+    if (t < s) {
+      s = t;
+      hit = c;
+    }
+  }
+  return s;
+}
+
+__device__ __forceinline__ double csg_safety(const CsgView &g, int v, const double *p)
+{
+  double q[3];
+  csg_local_point(g.node[v], p, q);
+  double s = csg_safety_out_local(g.node[v], q);
+  const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
+  for (int k = 0; k < nk; ++k) {
+    const CsgNode &m = g.node[g.kids[k0 + k]];
+    const double gap = csg_bbox_gap(m, p);
+    if (gap >= s) continue;
+    csg_local_point(m, p, q);
+    s = fmin(s, fmax(gap, csg_safety_in_local(m, q)));
+  }
+  return s < 0.0 ? 0.0 : s;
+}
+
+// the touchable entered at p after csg_step's crossing out of v
+__device__ __forceinline__ int csg_cross(const CsgView &g, int v, int hit, const double *p, const double *d)
+{
+  if (hit >= 0) return csg_descend(g, hit, p, d, kCsgTol);
+  return csg_locate(g, g.node[v].parent, p, d, kCsgTol);
+}
+
+} // namespace gx

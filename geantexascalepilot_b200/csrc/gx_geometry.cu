@@ -1,0 +1,343 @@
+// gx_geometry.cu -- the CSG volume tree (transport geometry 2): the host
+// builder behind gx_geom_*, its upload into a context and the navigation
+// probe kernel.
+//
+// The builder takes the calls a VecGeom detector construction makes
+// (UnplacedBox / LogicalVolume / PlaceDaughter with a Transformation3D /
+// SetWorld / CloseGeometry, as in the reference's
+// source/Geant/proxy/test/BasicCpuTransport/ProxyDetectorConstruction.cpp:
+// 241-324), plus a material and a scoring flag per logical volume.  Closing
+// unrolls the tree depth-first into touchables (one per placed instance) with
+// global transforms and padded bounding boxes; scored touchables get
+// consecutive tally columns in that order.  Navigation itself is in gx_csg.cuh.
+#include "gx_csg.cuh"
+#include "gx_internal.cuh"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+struct gx_geom {
+  struct Solid {
+    int kind;
+    double p[3];
+  };
+  struct Lv {
+    int solid, mat, scored;
+  };
+  struct Pv {
+    int mother, lv;
+    double t[3], r[9];
+  };
+  std::vector<Solid> solids;
+  std::vector<Lv> lvs;
+  std::vector<Pv> pvs;
+  // after gx_geom_close
+  int world = -1, nscore = 0;
+  std::vector<gx::CsgNode> nodes;
+  std::vector<int> kids, score, lv_of;
+};
+
+namespace gx {
+
+namespace {
+
+struct Flattener {
+  gx_geom &g;
+  std::vector<std::vector<int>> daughters; // placements per logical volume, in placement order
+  int kcur = 0;
+  bool err = false;
+
+  void bbox_half(const CsgNode &n, double h[3])
+  {
+    if (n.kind == kCsgBox) {
+      h[0] = n.a;
+      h[1] = n.b;
+      h[2] = n.c;
+    } else if (n.kind == kCsgTube) {
+      h[0] = h[1] = n.b;
+      h[2] = n.c;
+    } else {
+      h[0] = h[1] = h[2] = n.b;
+    }
+  }
+
+  long count(int lv, int depth)
+  {
+    if (depth > kCsgMaxDepth) return -1;
+    long n = 1;
+    for (int p : daughters[lv]) {
+      long k = count(g.pvs[p].lv, depth + 1);
+      if (k < 0) return -1;
+      n += k;
+      if (n > kCsgMaxNodes) return -1;
+    }
+    return n;
+  }
+
+  int visit(int lv, int parent, const double R[9], const double t[3], int depth)
+  {
+    const int id = (int)g.nodes.size();
+    g.nodes.emplace_back();
+    g.score.push_back(-1);
+    g.lv_of.push_back(lv);
+    {
+      CsgNode &n = g.nodes[id];
+      const gx_geom::Solid &s = g.solids[g.lvs[lv].solid];
+      n.kind = s.kind;
+      n.a = s.p[0];
+      n.b = s.p[1];
+      n.c = s.p[2];
+      std::memcpy(n.t, t, sizeof(n.t));
+      std::memcpy(n.r, R, sizeof(n.r));
+      n.rot = !(R[0] == 1.0 && R[1] == 0.0 && R[2] == 0.0 && R[3] == 0.0 && R[4] == 1.0 && R[5] == 0.0 &&
+                R[6] == 0.0 && R[7] == 0.0 && R[8] == 1.0);
+      n.mat = g.lvs[lv].mat;
+      n.parent = parent;
+      if (g.lvs[lv].scored) g.score[id] = g.nscore++;
+      double h[3];
+      bbox_half(n, h);
+      for (int k = 0; k < 3; ++k) {
+        n.lo[k] = kCsgInf;
+        n.hi[k] = -kCsgInf;
+      }
+      for (int corner = 0; corner < 8; ++corner) {
+        const double x[3] = {(corner & 1) ? h[0] : -h[0], (corner & 2) ? h[1] : -h[1], (corner & 4) ? h[2] : -h[2]};
+        for (int k = 0; k < 3; ++k) {
+          const double y = R[3 * k] * x[0] + R[3 * k + 1] * x[1] + R[3 * k + 2] * x[2] + t[k];
+          n.lo[k] = std::min(n.lo[k], y);
+          n.hi[k] = std::max(n.hi[k], y);
+        }
+      }
+      for (int k = 0; k < 3; ++k) {
+        n.lo[k] -= kCsgPad;
+        n.hi[k] += kCsgPad;
+      }
+      n.nkid = (int)daughters[lv].size();
+      n.kid0 = kcur; // the children's block, reserved before recursing
+      kcur += n.nkid;
+    }
+    int j = 0;
+    for (int p : daughters[lv]) {
+      const double *Rp = g.pvs[p].r, *tp = g.pvs[p].t;
+      double Rc[9], tc[3];
+      for (int r = 0; r < 3; ++r) {
+        for (int c = 0; c < 3; ++c)
+          Rc[3 * r + c] = R[3 * r] * Rp[c] + R[3 * r + 1] * Rp[3 + c] + R[3 * r + 2] * Rp[6 + c];
+        tc[r] = R[3 * r] * tp[0] + R[3 * r + 1] * tp[1] + R[3 * r + 2] * tp[2] + t[r];
+      }
+      const int kid = visit(g.pvs[p].lv, id, Rc, tc, depth + 1);
+      g.kids[g.nodes[id].kid0 + j++] = kid;
+    }
+    return id;
+  }
+};
+
+bool orthonormal(const double *R)
+{
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      const double d = R[3 * i] * R[3 * j] + R[3 * i + 1] * R[3 * j + 1] + R[3 * i + 2] * R[3 * j + 2];
+      if (std::fabs(d - (i == j ? 1.0 : 0.0)) > 1e-9) return false;
+    }
+  return true;
+}
+
+__global__ void k_geom_probe(CsgView g, int n, const double *__restrict__ pos, const double *__restrict__ dir,
+                             const double *__restrict__ limit, int *__restrict__ vol, double *__restrict__ snext,
+                             int *__restrict__ next, double *__restrict__ safety)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+  const double d[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+  const int v = csg_locate(g, 0, p, d, kCsgTol);
+  vol[i] = v;
+  if (v < 0) {
+    snext[i] = -1.0;
+    next[i] = -1;
+    safety[i] = -1.0;
+    return;
+  }
+  int hit;
+  const double s = csg_step(g, v, p, d, limit[i], hit);
+  snext[i] = s;
+  safety[i] = csg_safety(g, v, p);
+  if (s < limit[i]) {
+    const double x[3] = {cadd(p[0], cmul(s, d[0])), cadd(p[1], cmul(s, d[1])), cadd(p[2], cmul(s, d[2]))};
+    next[i] = csg_cross(g, v, hit, x, d);
+  } else {
+    next[i] = v;
+  }
+}
+
+} // namespace
+
+} // namespace gx
+
+using namespace gx;
+
+extern "C" {
+
+int gx_geom_create(gx_geom **out)
+{
+  if (!out) return set_error(GX_ERR_ARG, "gx_geom_create: null argument");
+  *out = new gx_geom();
+  return GX_OK;
+}
+
+void gx_geom_destroy(gx_geom *g) { delete g; }
+
+static int add_solid(gx_geom *g, int kind, double a, double b, double c, int *solid)
+{
+  if (!g || !solid) return set_error(GX_ERR_ARG, "gx_geom: null argument");
+  if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
+  g->solids.push_back({kind, {a, b, c}});
+  *solid = (int)g->solids.size() - 1;
+  return GX_OK;
+}
+
+int gx_geom_box(gx_geom *g, double hx, double hy, double hz, int *solid)
+{
+  if (!(hx > 0.0 && hy > 0.0 && hz > 0.0)) return set_error(GX_ERR_ARG, "gx_geom_box: half lengths must be > 0");
+  return add_solid(g, kCsgBox, hx, hy, hz, solid);
+}
+
+int gx_geom_tube(gx_geom *g, double rmin, double rmax, double dz, int *solid)
+{
+  if (!(rmin >= 0.0 && rmax > rmin && dz > 0.0))
+    return set_error(GX_ERR_ARG, "gx_geom_tube: need 0 <= rmin < rmax and dz > 0");
+  return add_solid(g, kCsgTube, rmin, rmax, dz, solid);
+}
+
+int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid)
+{
+  if (!(rmin >= 0.0 && rmax > rmin)) return set_error(GX_ERR_ARG, "gx_geom_sphere: need 0 <= rmin < rmax");
+  return add_solid(g, kCsgSphere, rmin, rmax, 0.0, solid);
+}
+
+int gx_geom_logical_volume(gx_geom *g, int solid, int material, int scored, int *lv)
+{
+  if (!g || !lv) return set_error(GX_ERR_ARG, "gx_geom_logical_volume: null argument");
+  if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
+  if (solid < 0 || solid >= (int)g->solids.size()) return set_error(GX_ERR_ARG, "gx_geom_logical_volume: bad solid");
+  if (material < 0 || material >= kNMat) return set_error(GX_ERR_ARG, "gx_geom_logical_volume: bad material");
+  g->lvs.push_back({solid, material, scored ? 1 : 0});
+  *lv = (int)g->lvs.size() - 1;
+  return GX_OK;
+}
+
+int gx_geom_place_daughter(gx_geom *g, int mother, int daughter, const double translation[3],
+                           const double rotation[9], int *pv)
+{
+  if (!g || !translation) return set_error(GX_ERR_ARG, "gx_geom_place_daughter: null argument");
+  if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
+  const int nlv = (int)g->lvs.size();
+  if (mother < 0 || mother >= nlv || daughter < 0 || daughter >= nlv)
+    return set_error(GX_ERR_ARG, "gx_geom_place_daughter: bad logical volume");
+  gx_geom::Pv p;
+  p.mother = mother;
+  p.lv = daughter;
+  std::memcpy(p.t, translation, sizeof(p.t));
+  const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+  std::memcpy(p.r, rotation ? rotation : I, sizeof(p.r));
+  if (!orthonormal(p.r)) return set_error(GX_ERR_ARG, "gx_geom_place_daughter: rotation is not orthonormal");
+  g->pvs.push_back(p);
+  if (pv) *pv = (int)g->pvs.size() - 1;
+  return GX_OK;
+}
+
+int gx_geom_close(gx_geom *g, int world, int *ntouchables, int *nscore)
+{
+  if (!g) return set_error(GX_ERR_ARG, "gx_geom_close: null argument");
+  if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
+  if (world < 0 || world >= (int)g->lvs.size()) return set_error(GX_ERR_ARG, "gx_geom_close: bad world volume");
+  Flattener f{*g, std::vector<std::vector<int>>(g->lvs.size())};
+  for (int p = 0; p < (int)g->pvs.size(); ++p) f.daughters[g->pvs[p].mother].push_back(p);
+  const long total = f.count(world, 0);
+  if (total < 0)
+    return set_error(GX_ERR_ARG, "gx_geom_close: more than %d touchables or deeper than %d levels (a volume placed "
+                                 "inside itself?)",
+                     kCsgMaxNodes, kCsgMaxDepth);
+  g->nodes.clear();
+  g->nodes.reserve(total);
+  g->kids.assign(total, 0);
+  g->nscore = 0;
+  const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, z[3] = {0, 0, 0};
+  f.visit(world, -1, I, z, 0);
+  g->world = world;
+  if (ntouchables) *ntouchables = (int)g->nodes.size();
+  if (nscore) *nscore = g->nscore;
+  return GX_OK;
+}
+
+int gx_geom_touchable(const gx_geom *g, int i, int *lv, int *parent, int *score, double translation[3],
+                      double rotation[9])
+{
+  if (!g || g->world < 0) return set_error(GX_ERR_ARG, "gx_geom_touchable: geometry not closed");
+  if (i < 0 || i >= (int)g->nodes.size()) return set_error(GX_ERR_ARG, "gx_geom_touchable: bad index");
+  const CsgNode &n = g->nodes[i];
+  if (lv) *lv = g->lv_of[i];
+  if (parent) *parent = n.parent;
+  if (score) *score = g->score[i];
+  if (translation) std::memcpy(translation, n.t, sizeof(n.t));
+  if (rotation) std::memcpy(rotation, n.r, sizeof(n.r));
+  return GX_OK;
+}
+
+int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g)
+{
+  if (!ctx || !g) return set_error(GX_ERR_ARG, "gx_ctx_load_geometry: null argument");
+  if (g->world < 0) return set_error(GX_ERR_ARG, "gx_ctx_load_geometry: geometry not closed (gx_geom_close)");
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return cuda_error(e, "gx_ctx_load_geometry: cudaSetDevice");
+  const size_t nn = g->nodes.size(), nk = std::max<size_t>(g->kids.size(), 1);
+  CsgNode *dn = nullptr;
+  int *dk = nullptr, *ds = nullptr;
+  if ((e = cudaMalloc((void **)&dn, nn * sizeof(CsgNode))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&dk, nk * sizeof(int))) != cudaSuccess ||
+      (e = cudaMalloc((void **)&ds, nn * sizeof(int))) != cudaSuccess) {
+    cudaFree(dn);
+    cudaFree(dk);
+    return cuda_error(e, "gx_ctx_load_geometry: allocation");
+  }
+  if ((e = cudaMemcpy(dn, g->nodes.data(), nn * sizeof(CsgNode), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (!g->kids.empty() &&
+       (e = cudaMemcpy(dk, g->kids.data(), g->kids.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) ||
+      (e = cudaMemcpy(ds, g->score.data(), nn * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
+    cudaFree(dn);
+    cudaFree(dk);
+    cudaFree(ds);
+    return cuda_error(e, "gx_ctx_load_geometry: upload");
+  }
+  // the previous tree (if any) stays allocated until the context goes: a
+  // captured transport graph may still refer to it
+  c->owned.push_back(dn);
+  c->owned.push_back(dk);
+  c->owned.push_back(ds);
+  c->csg_node = dn;
+  c->csg_kids = dk;
+  c->csg_score = ds;
+  c->csg_n = (int)nn;
+  c->csg_nscore = g->nscore;
+  return GX_OK;
+}
+
+int gx_geom_probe(gx_ctx *ctx, int n, const double *d_pos, const double *d_dir, const double *d_limit, int *d_vol,
+                  double *d_snext, int *d_next, double *d_safety, gx_stream_t s)
+{
+  if (!ctx || n < 0 || (n > 0 && (!d_pos || !d_dir || !d_limit || !d_vol || !d_snext || !d_next || !d_safety)))
+    return set_error(GX_ERR_ARG, "gx_geom_probe: bad arguments");
+  Ctx *c = reinterpret_cast<Ctx *>(ctx);
+  if (!c->csg_node) return set_error(GX_ERR_ARG, "gx_geom_probe: no geometry loaded (gx_ctx_load_geometry)");
+  if (n == 0) return GX_OK;
+  CsgView v{(const CsgNode *)c->csg_node, c->csg_kids};
+  k_geom_probe<<<(n + 127) / 128, 128, 0, stream_of(s)>>>(v, n, d_pos, d_dir, d_limit, d_vol, d_snext, d_next,
+                                                         d_safety);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "k_geom_probe");
+}
+
+} // extern "C"

@@ -2,6 +2,7 @@
 #pragma once
 
 #include "../../include/gx_abi.h"
+#include "gx_csg.cuh"
 #include "gx_device.cuh"
 
 #include <vector>
@@ -17,6 +18,10 @@ struct Ctx {
   Data *dev = nullptr;  // device copy
   std::vector<void *> owned;
   Engine *engine = nullptr;
+  // the CSG volume tree (gx_ctx_load_geometry): touchables, children, tally column of each
+  CsgNode *csg_node = nullptr;
+  int *csg_kids = nullptr, *csg_score = nullptr;
+  int csg_n = 0, csg_nscore = 0;
 };
 
 int set_error(int code, const char *fmt, ...);

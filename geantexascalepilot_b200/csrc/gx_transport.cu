@@ -42,6 +42,7 @@ struct Geom {
   int field_map; // 1: the context's field map with Runge-Kutta sub-steps, 0: uniform Bz
   double t_abs, pitch, x0, total, half_trans, Bz;
   double box_half[3], box_centre[3];
+  CsgView csg; // geometry 2: the context's volume tree
 };
 
 constexpr int kNStat = 25;
@@ -116,6 +117,7 @@ template <class T> __device__ __forceinline__ void set_comp(T *p, int a, T v)
 // x0 + (k+1) pitch), absorber first.  vol = 2 layer + slab; -1 outside.
 __device__ __forceinline__ int vol_material(const Geom &g, int vol)
 {
+  if (g.geometry == 2) return g.csg.node[vol].mat;
   return g.geometry == 0 ? g.box_mat : ((vol & 1) ? 2 : 1);
 }
 __device__ __forceinline__ void slab_bounds(const Geom &g, int vol, double &lo, double &hi)
@@ -243,6 +245,39 @@ __device__ __forceinline__ int relocate(const Geom &g, int vol, double *p, const
     return next_volume(g, vol, -1);
   }
   return locate(g, p, d);
+}
+
+// Kernel variants, template parameters so that each kernel carries only the
+// code it runs: bit 0 follows the field map (Runge-Kutta sub-steps) instead of
+// the uniform field's helix, bit 1 navigates the CSG tree (gx_csg.cuh) instead
+// of the analytic volumes above.
+enum { kKindFieldMap = 1, kKindCsg = 2 };
+
+template <int K> __device__ __forceinline__ double nav_safety(const Geom &g, int vol, const double *p)
+{
+  if constexpr ((K & kKindCsg) != 0)
+    return csg_safety(g.csg, vol, p);
+  else
+    return safety(g, vol, p);
+}
+// Straight-line distance to the next boundary.  plane: the analytic
+// navigator's face code, or the CSG child entered (-1: leaving the volume);
+// the CSG navigator skips children met only beyond limit.
+template <int K>
+__device__ __forceinline__ double nav_distance(const Geom &g, int vol, const double *p, const double *d, double limit,
+                                               int &plane)
+{
+  if constexpr ((K & kKindCsg) != 0)
+    return csg_step(g.csg, vol, p, d, limit, plane);
+  else
+    return dist_to_out(g, vol, p, d, plane);
+}
+template <int K> __device__ __forceinline__ int nav_relocate(const Geom &g, int vol, double *p, const double *d)
+{
+  if constexpr ((K & kKindCsg) != 0)
+    return csg_locate(g.csg, vol, p, d, kSnap);
+  else
+    return relocate(g, vol, p, d);
 }
 
 // ---------------------------------------------------------- cross sections
@@ -651,7 +686,7 @@ template <class R> struct GammaXs {
 // GPIL and step limit.  Returns true when the step continues with helix
 // sub-steps (a charged track in a field), false when it is complete.  gx,
 // when given, caches a photon's cross sections per material.
-template <class R>
+template <class R, int K>
 __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c,
                                            GammaXs<R> *gx = nullptr)
 {
@@ -718,7 +753,7 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
       if (t.E < R(kMinE)) range *= t.E / R(kMinE);
       t.msc_r0 = range > lam0 ? range : lam0;
     }
-    const double tlim = fmax(fmax(kMscFr * (double)t.msc_r0, kMscFs * safety(g, t.vol, t.pos)), kMscTmin);
+    const double tlim = fmax(fmax(kMscFr * (double)t.msc_r0, kMscFs * nav_safety<K>(g, t.vol, t.pos)), kMscTmin);
     if (tlim < (double)pstep) {
       pstep = (R)tlim;
       sel = -1;
@@ -741,17 +776,22 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
   }
   int plane;
   double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
-  double dd = dist_to_out(g, t.vol, t.pos, dir, plane);
   double ps = (double)pstep;
+  double dd = nav_distance<K>(g, t.vol, t.pos, dir, ps, plane);
   if (dd < ps) {
     c.total = dd;
     c.crossed = true;
-    c.newvol = next_volume(g, t.vol, plane);
-    for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
-    if (plane != 2) {
-      double lo, hi;
-      slab_bounds(g, t.vol, lo, hi);
-      set_comp(t.pos, g.axis, plane > 0 ? hi : lo);
+    if constexpr ((K & kKindCsg) != 0) {
+      for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
+      c.newvol = csg_cross(g.csg, t.vol, plane, t.pos, dir);
+    } else {
+      c.newvol = next_volume(g, t.vol, plane);
+      for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
+      if (plane != 2) {
+        double lo, hi;
+        slab_bounds(g, t.vol, lo, hi);
+        set_comp(t.pos, g.axis, plane > 0 ? hi : lo);
+      }
     }
   } else {
     c.total = ps;
@@ -834,10 +874,8 @@ __device__ __forceinline__ double field_map_substep(const Data &d, const Geom &g
   return s;
 }
 
-// FM: 1 when the transport follows the field map (Runge-Kutta), 0 for the
-// uniform field (helix); a template parameter so that the uniform-field
-// kernels carry no Runge-Kutta code (registers).
-template <class R, int FM>
+// K: the kernel variant (kKindFieldMap, kKindCsg bits).
+template <class R, int K>
 __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c, Local &L)
 {
   const R eps = R(0.1); // gEpsDeflection = 1e-2 cm
@@ -848,11 +886,12 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
   int plane;
   double dd[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
   const double remaining = c.remaining;
-  double saf = safety(g, t.vol, t.pos);
-  double snext = (saf > remaining) ? remaining
-                                   : fmax(2e-9, fmin(dist_to_out(g, t.vol, t.pos, dd, plane), remaining) + 2e-9);
+  double saf = nav_safety<K>(g, t.vol, t.pos);
+  double snext = (saf > remaining)
+                     ? remaining
+                     : fmax(2e-9, fmin(nav_distance<K>(g, t.vol, t.pos, dd, remaining, plane), remaining) + 2e-9);
   double s;
-  if constexpr (FM == 1) {
+  if constexpr ((K & kKindFieldMap) != 0) {
     s = field_map_substep<R>(d, g, t, remaining, saf, snext);
   } else {
   double step_gp = fmax(fmin(remaining, 1e-4), snext);
@@ -880,7 +919,7 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
   dd[0] = (double)t.dir[0];
   dd[1] = (double)t.dir[1];
   dd[2] = (double)t.dir[2];
-  int v = relocate(g, t.vol, t.pos, dd);
+  int v = nav_relocate<K>(g, t.vol, t.pos, dd);
   if (v != t.vol || c.remaining <= 1e-10) {
     if (v != t.vol) {
       c.crossed = true;
@@ -955,13 +994,13 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
 }
 
 // The three phases in sequence: one whole step up to the interaction.
-template <class R, int FM>
+template <class R, int K>
 __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Track<R> &t, Local &L,
                                                                  int *proc)
 {
   StepCtx<R> c;
-  if (step_begin(d, g, t, c))
-    while (!field_substep<R, FM>(d, g, t, c, L)) {
+  if (step_begin<R, K>(d, g, t, c))
+    while (!field_substep<R, K>(d, g, t, c, L)) {
     }
   return step_end(d, g, t, c, L, proc);
 }
@@ -969,12 +1008,12 @@ __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Trac
 // The whole OneStep, interaction included (the fused form the plain loop
 // runs); the oracle's one_step is the same algorithm in the same order of
 // random draws.  Returns false when the track is finished.
-template <class R, int FM>
+template <class R, int K>
 __device__ bool one_step(const Data &d, const Geom &g, Track<R> &t, Secs<R> &sec, Local &L)
 {
   sec.n = 0;
   int proc = -1;
-  int r = transport_part<R, FM>(d, g, t, L, &proc);
+  int r = transport_part<R, K>(d, g, t, L, &proc);
   if (r == kInteract) {
     run_model(d, g, t, proc, sec, L);
     return t.E > R(0);
@@ -1176,7 +1215,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
 
 // PT: particle type of the store (0, 1, 2), or 3 for the single mixed store.
 // The fused step (transport and interaction in one kernel) of the plain loop.
-template <class R, int PT, int FM> __device__ __forceinline__ void step_body(const Args<R> &a)
+template <class R, int PT, int K> __device__ __forceinline__ void step_body(const Args<R> &a)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1201,7 +1240,7 @@ template <class R, int PT, int FM> __device__ __forceinline__ void step_body(con
     if (active) {
       load_track(cur, i, PT, t);
       L.st[S_READ0 + SRC]++;
-      alive = one_step<R, FM>(d, a.g, t, sec, L);
+      alive = one_step<R, K>(d, a.g, t, sec, L);
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
     emit_tracks<R, SRC>(a, ctl, par, active, alive, t, sec, L);
@@ -1212,13 +1251,13 @@ template <class R, int PT, int FM> __device__ __forceinline__ void step_body(con
 // Arguments by value (the allocation-free entry point) or from a device copy.
 // Two resident blocks per SM: the fused step needs ~190 registers per thread
 // unconstrained, which would leave one 256-thread block (8 warps) per SM.
-template <class R, int PT, int FM> __global__ void __launch_bounds__(256, 2) k_step(Args<R> a)
+template <class R, int PT, int K> __global__ void __launch_bounds__(256, 2) k_step(Args<R> a)
 {
-  step_body<R, PT, FM>(a);
+  step_body<R, PT, K>(a);
 }
-template <class R, int PT, int FM> __global__ void __launch_bounds__(256, 2) k_step_p(const Args<R> *__restrict__ A)
+template <class R, int PT, int K> __global__ void __launch_bounds__(256, 2) k_step_p(const Args<R> *__restrict__ A)
 {
-  step_body<R, PT, FM>(*A);
+  step_body<R, PT, K>(*A);
 }
 
 // ------------------------------------------------- batched engine: split step
@@ -1254,7 +1293,7 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
 // tracks in a field), with the start and the end of a step attached to it, so
 // a lane whose step needs several sub-steps does not hold up the others.
 // All stores and buffers are written at slots reserved per warp, contiguous.
-template <class R, int PT, int FM>
+template <class R, int PT, int K>
 __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
@@ -1303,10 +1342,10 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
     int r = kDone, proc = -1;
     bool done = false; // a step ends in this pass
     if (have && !infield) {
-      infield = step_begin(d, a.g, t, c, PT == 0 ? &gxs : nullptr);
+      infield = step_begin<R, K>(d, a.g, t, c, PT == 0 ? &gxs : nullptr);
       done = !infield;
     }
-    if (PT != 0 && have && infield && field_substep<R, FM>(d, a.g, t, c, L)) {
+    if (PT != 0 && have && infield && field_substep<R, K>(d, a.g, t, c, L)) {
       infield = false;
       done = true;
     }
@@ -1520,7 +1559,7 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
       t.dir[k] = (R)a.p.dir[3 * pi + k];
     }
     double dd[3] = {a.p.dir[3 * pi], a.p.dir[3 * pi + 1], a.p.dir[3 * pi + 2]};
-    t.vol = locate(a.g, t.pos, dd);
+    t.vol = a.g.geometry == 2 ? csg_locate(a.g.csg, 0, t.pos, dd, kCsgTol) : locate(a.g, t.pos, dd);
     t.nil[0] = t.nil[1] = t.nil[2] = R(-1);
     t.msc_r0 = R(-1);
     t.event = a.p.event ? a.p.event[pi] : 0;
@@ -1584,6 +1623,8 @@ struct Engine {
   std::vector<char> graph_args; // launch arguments the graph was captured with
   double *cumE = nullptr;
   long long cumE_cap = 0;
+  double *vtally = nullptr; // geometry 2: deposits per (event, touchable), folded into the caller's columns
+  long long vtally_cap = 0;
   void *dargs = nullptr; // device copy of the launch arguments (batched engine)
   cudaStream_t s1 = nullptr, s2 = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_j1 = nullptr, ev_j2 = nullptr;
@@ -1627,6 +1668,7 @@ void release_engine(Ctx *c)
   if (e->pool) cudaFree(e->pool);
   if (e->ctl) cudaFree(e->ctl);
   if (e->cumE) cudaFree(e->cumE);
+  if (e->vtally) cudaFree(e->vtally);
   if (e->dargs) cudaFree(e->dargs);
   if (e->h_ctl) cudaFreeHost(e->h_ctl);
   if (e->s1) cudaStreamDestroy(e->s1);
@@ -1646,6 +1688,40 @@ template <class R> struct Launch {
   int block, grid, smem;
 };
 
+// Geometry 2: the deposits per (event, touchable) added to the caller's
+// tally columns (touchables without a column are dropped).
+__global__ void k_fold_touchables(const double *__restrict__ vt, const int *__restrict__ score, int ntouch,
+                                  int nscore, long long n, double *__restrict__ edep)
+{
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double e = vt[i];
+    const long long ev = i / ntouch;
+    const int c = score[i - ev * ntouch];
+    if (e != 0.0 && c >= 0) edep[ev * nscore + c] += e;
+  }
+}
+
+// The variant of the step kernels for a geometry and field (kKind* bits).
+static int kernel_kind(const Geom &g) { return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0); }
+template <class R, int PT> static void (*transport_kernel(int kind))(const Args<R> *)
+{
+  switch (kind) {
+  case 1: return k_transport<R, PT, 1>;
+  case 2: return k_transport<R, PT, 2>;
+  case 3: return k_transport<R, PT, 3>;
+  default: return k_transport<R, PT, 0>;
+  }
+}
+template <class R> static void (*step_kernel_p(int kind))(const Args<R> *)
+{
+  switch (kind) {
+  case 1: return k_step_p<R, 3, 1>;
+  case 2: return k_step_p<R, 3, 2>;
+  case 3: return k_step_p<R, 3, 3>;
+  default: return k_step_p<R, 3, 0>;
+  }
+}
+
 template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
@@ -1653,7 +1729,7 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     // plain loop: one fused step kernel over the mixed store
     k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
     k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
-    (L.a.g.field_map ? k_step_p<R, 3, 1> : k_step_p<R, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
+    step_kernel_p<R>(kernel_kind(L.a.g))<<<L.grid, L.block, L.smem, s>>>(A);
     k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
     return;
   }
@@ -1668,15 +1744,15 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     se = e->s1;
     sp = e->s2;
   }
-  const bool fm = L.a.g.field_map != 0;
-  (fm ? k_transport<R, 0, 1> : k_transport<R, 0, 0>)<<<L.grid, L.block, L.smem, sg>>>(A);
+  const int kind = kernel_kind(L.a.g);
+  transport_kernel<R, 0>(kind)<<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 0><<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 1><<<L.grid, L.block, L.smem, sg>>>(A);
   k_interact<R, 0, 2><<<L.grid, L.block, L.smem, sg>>>(A);
-  (fm ? k_transport<R, 1, 1> : k_transport<R, 1, 0>)<<<L.grid, L.block, L.smem, se>>>(A);
+  transport_kernel<R, 1>(kind)<<<L.grid, L.block, L.smem, se>>>(A);
   k_interact<R, 1, 0><<<L.grid, L.block, L.smem, se>>>(A);
   k_interact<R, 1, 1><<<L.grid, L.block, L.smem, se>>>(A);
-  (fm ? k_transport<R, 2, 1> : k_transport<R, 2, 0>)<<<L.grid, L.block, L.smem, sp>>>(A);
+  transport_kernel<R, 2>(kind)<<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 0><<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 1><<<L.grid, L.block, L.smem, sp>>>(A);
   k_interact<R, 2, 2><<<L.grid, L.block, L.smem, sp>>>(A);
@@ -1694,20 +1770,20 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
 template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q, cudaEvent_t mid)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
-  const bool fm = L.a.g.field_map != 0;
+  const int kind = kernel_kind(L.a.g);
   if (q == 0) {
-    (fm ? k_transport<R, 0, 1> : k_transport<R, 0, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_kernel<R, 0>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 0, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 1><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 0, 2><<<L.grid, L.block, L.smem, s>>>(A);
   } else if (q == 1) {
-    (fm ? k_transport<R, 1, 1> : k_transport<R, 1, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_kernel<R, 1>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 1, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 1, 1><<<L.grid, L.block, L.smem, s>>>(A);
   } else {
-    (fm ? k_transport<R, 2, 1> : k_transport<R, 2, 0>)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_kernel<R, 2>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
     k_interact<R, 2, 0><<<L.grid, L.block, L.smem, s>>>(A);
     k_interact<R, 2, 1><<<L.grid, L.block, L.smem, s>>>(A);
@@ -1812,6 +1888,23 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.a.p.jump = jt;
   L.a.edep = d_edep;
   L.a.pstep = d_pstep;
+  if (cfg->geometry == 2) {
+    // the kernels score per (event, touchable); folded into d_edep at the end
+    g.csg = CsgView{C->csg_node, C->csg_kids};
+    g.nvol = C->csg_n;
+    const long long nt = (long long)cfg->nevents * C->csg_n;
+    if (nt > E->vtally_cap) {
+      if (E->vtally) cudaFree(E->vtally);
+      E->vtally = nullptr;
+      E->vtally_cap = 0;
+      if ((err = cudaMalloc((void **)&E->vtally, sizeof(double) * nt)) != cudaSuccess)
+        return cuda_error(err, "transport touchable tally");
+      E->vtally_cap = nt;
+    }
+    if ((err = cudaMemsetAsync(E->vtally, 0, sizeof(double) * nt, s)) != cudaSuccess)
+      return cuda_error(err, "transport touchable tally");
+    L.a.edep = E->vtally;
+  }
   L.a.nstores = nstores;
   L.a.refill_below = cfg->refill_below > 0 ? std::min(cfg->refill_below, cap) : cap / 2;
   L.block = cfg->block_size > 0 ? cfg->block_size : default_block(cfg->engine);
@@ -1870,7 +1963,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
           if (!batched) {
-            (L.a.g.field_map ? k_step_p<R, 3, 1> : k_step_p<R, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(
+            step_kernel_p<R>(kernel_kind(L.a.g))<<<L.grid, L.block, L.smem, s>>>(
                 (const Args<R> *)E->dargs);
             cudaEventRecord(em[q], s);
           } else {
@@ -1904,10 +1997,11 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
   } else {
     int G = cfg->graph_iters > 0 ? cfg->graph_iters : 16;
-    // (re)capture the iteration graph when its launch shape changes; the
-    // arguments themselves are read from the device copy uploaded above
-    std::vector<char> key(4 * sizeof(int) + 2 * sizeof(void *));
-    int shape[4] = {G, L.block, L.grid, L.smem};
+    // (re)capture the iteration graph when its launch shape or its kernels
+    // (field kind, geometry kind) change; the arguments themselves are read
+    // from the device copy uploaded above
+    int shape[6] = {G, L.block, L.grid, L.smem, L.a.g.field_map, L.a.g.geometry == 2};
+    std::vector<char> key(sizeof(shape) + 2 * sizeof(void *));
     const void *ptrs[2] = {E->dargs, E->ctl};
     std::memcpy(key.data(), shape, sizeof(shape));
     std::memcpy(key.data() + sizeof(shape), ptrs, sizeof(ptrs));
@@ -1938,6 +2032,11 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       if (E->h_ctl->in_flight == 0 && E->h_ctl->pending == 0) break;
       if (iters > max_iter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
     }
+  }
+  if (cfg->geometry == 2) {
+    const long long nt = (long long)cfg->nevents * C->csg_n;
+    k_fold_touchables<<<(int)std::min<long long>((nt + 255) / 256, 4096), 256, 0, s>>>(
+        E->vtally, C->csg_score, C->csg_n, C->csg_nscore, nt, d_edep);
   }
   k_count_new_tracks<<<1, 1, 0, s>>>(E->ctl);
   cudaEventRecord(t1, s);
@@ -2020,6 +2119,12 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
   Ctx *C = reinterpret_cast<Ctx *>(ctx);
   if (cfg->field_map && !C->host.fmap)
     return set_error(GX_ERR_ARG, "gx_transport_run: field_map = 1 without a field map (gx_ctx_load_field_map)");
+  if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "gx_transport_run: bad geometry");
+  if (cfg->geometry == 2 && !C->csg_node)
+    return set_error(GX_ERR_ARG, "gx_transport_run: geometry 2 without a volume tree (gx_ctx_load_geometry)");
+  if (cfg->geometry == 2 && nvol != C->csg_nscore)
+    return set_error(GX_ERR_ARG, "gx_transport_run: nvol %d, the volume tree has %d scored touchables", nvol,
+                     C->csg_nscore);
   cudaSetDevice(C->device);
   if (cfg->precision == 1)
     return run<float>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
@@ -2159,6 +2264,9 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
                      kNoallocMaxPrimaries);
   if (cfg->precision != 0)
     return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: FP64 only (precision must be 0)");
+  if (cfg->geometry != 0 && cfg->geometry != 1)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: geometry 0 or 1 only (the volume tree's per-touchable "
+                                 "tally is allocated: use gx_transport_run)");
   if (cfg->geometry == 1 && (cfg->nlayers <= 0 || cfg->t_abs <= 0 || cfg->t_gap <= 0 || cfg->half_trans <= 0 ||
                              nvol < 2 * cfg->nlayers))
     return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: bad calorimeter (nvol must be >= 2 nlayers)");

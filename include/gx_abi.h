@@ -183,9 +183,54 @@ int gx_helix_dostep(const double B[3], double kB2C, int n, const double *d_posx,
                     double *d_newposy, double *d_newposz, double *d_newdirx, double *d_newdiry,
                     double *d_newdirz, gx_stream_t s);
 
+/* ------------------------------------------------------- CSG geometry */
+/* A volume tree for transport geometry 2, built with the calls a VecGeom
+ * detector construction makes (the reference navigates VecGeom,
+ * geometry/NavigationInterface.hpp:63-98, over a tree built in
+ * proxy/test/BasicCpuTransport/ProxyDetectorConstruction.cpp:241-324):
+ *   new UnplacedBox(hx, hy, hz)             -> gx_geom_box
+ *   new UnplacedTube(rmin, rmax, dz, 0, 2pi) -> gx_geom_tube
+ *   new UnplacedSphere / UnplacedOrb (full)  -> gx_geom_sphere
+ *   new LogicalVolume(name, solid) + SetMaterialPtr -> gx_geom_logical_volume
+ *   lv->PlaceDaughter(name, daughter, new Transformation3D(...))
+ *                                            -> gx_geom_place_daughter
+ *   GeoManager::SetWorld + CloseGeometry     -> gx_geom_close
+ * Lengths in mm; materials 0 Galactic, 1 Pb, 2 LAr (the context's tables).
+ * A placement puts a daughter point x at R x + t in its mother (R row-major,
+ * NULL: identity).  Closing unrolls the tree into touchables (one per placed
+ * instance, depth-first, the world first); the touchables of logical volumes
+ * created with scored != 0 get consecutive tally columns in that order
+ * (*nscore of them: pass that as nvol to gx_transport_run).  Solid ids,
+ * logical volume ids and placement ids count from 0 in creation order. */
+typedef struct gx_geom gx_geom;
+int gx_geom_create(gx_geom **out);
+void gx_geom_destroy(gx_geom *g);
+int gx_geom_box(gx_geom *g, double hx, double hy, double hz, int *solid);
+int gx_geom_tube(gx_geom *g, double rmin, double rmax, double dz, int *solid);
+int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid);
+int gx_geom_logical_volume(gx_geom *g, int solid, int material, int scored, int *lv);
+int gx_geom_place_daughter(gx_geom *g, int mother, int daughter, const double translation[3],
+                           const double rotation[9], int *pv);
+int gx_geom_close(gx_geom *g, int world, int *ntouchables, int *nscore);
+/* a touchable of a closed tree: its logical volume, parent touchable (-1 for
+ * the world), tally column (-1: not scored) and global transform */
+int gx_geom_touchable(const gx_geom *g, int i, int *lv, int *parent, int *score, double translation[3],
+                      double rotation[9]);
+/* upload a closed tree into the context (replacing the previous one) */
+int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g);
+/* Navigation probe, one thread per point (device arrays; pos and dir n x 3):
+ * the touchable containing the point (-1 outside the world), the distance to
+ * the next boundary along dir (children are considered up to limit; -1
+ * outside), the touchable entered there (the same one when limit comes
+ * first) and the isotropic safety. */
+int gx_geom_probe(gx_ctx *ctx, int n, const double *d_pos, const double *d_dir, const double *d_limit, int *d_vol,
+                  double *d_snext, int *d_next, double *d_safety, gx_stream_t s);
+
 /* ---------------------------------------------------------- transport */
 typedef struct {
-  int geometry;            /* 0: one box of material box_mat; 1: layered calorimeter */
+  int geometry;            /* 0: one box of material box_mat; 1: layered calorimeter; 2: the context's
+                              CSG tree (gx_ctx_load_geometry; axis, nlayers, t_abs, t_gap, half_trans
+                              and box_* are ignored) */
   int axis;                /* layering (or box) axis: 0 x, 1 y, 2 z */
   int nlayers;
   double t_abs, t_gap;     /* absorber (Pb) and gap (LAr) thickness, mm */

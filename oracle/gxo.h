@@ -162,9 +162,51 @@ void gxo_helix_batch(const double B[3], int n, const double *pos, const double *
                      const double *charge, const double *mom, const double *step, double *newpos,
                      double *newdir);
 
+/* ---------------------------------------------------------- CSG geometry */
+/* gxo_geom.c: a volume tree of placed solids, flattened into touchables
+ * (transport config geometry = 2). */
+enum { GXO_CSG_BOX = 0, GXO_CSG_TUBE = 1, GXO_CSG_SPHERE = 2 };
+#define GXO_CSG_TOL 1e-9 /* surface tolerance, mm */
+typedef struct {
+  int kind;             /* GXO_CSG_* */
+  double a, b, c;       /* box: half lengths; tube: rmin, rmax, half length in z; sphere: rmin, rmax */
+  double t[3], r[9];    /* global placement: x_global = R x_local + t (R row-major) */
+  int rot;              /* 0: R is the identity */
+  double lo[3], hi[3];  /* global bounding box, padded */
+  int mat, parent, kid0, nkid, score, lv;
+} gxo_csg_node_t;
+typedef struct {
+  int n, nscore;        /* touchables; scored ones (numbered depth-first) */
+  gxo_csg_node_t *node; /* node 0 is the world */
+  int *kids;
+} gxo_csg_t;
+/* solids: kind and 3 parameters each; logical volumes: solid, material,
+ * scored flag; placements: mother and daughter logical volume, translation (3)
+ * and rotation (9, row-major; x_mother = R x_daughter + t).  NULL on error. */
+gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, int nlv, const int *lv_solid,
+                         const int *lv_mat, const int *lv_scored, int npv, const int *pv_mother, const int *pv_lv,
+                         const double *pv_t, const double *pv_r, int world);
+void gxo_csg_free(gxo_csg_t *g);
+int gxo_csg_contains(const gxo_csg_t *g, int v, const double *p, const double *d, double tol);
+/* from touchable v (-1 or 0: the world) up until a touchable contains p, then down */
+int gxo_csg_locate(const gxo_csg_t *g, int v, const double *p, const double *d, double tol);
+/* distance to the next boundary from p in v (children closer than limit are
+ * considered); *hit = the child entered, -1 when leaving v */
+double gxo_csg_step(const gxo_csg_t *g, int v, const double *p, const double *d, double limit, int *hit);
+double gxo_csg_safety(const gxo_csg_t *g, int v, const double *p);
+/* the touchable entered at p after gxo_csg_step's crossing */
+int gxo_csg_cross(const gxo_csg_t *g, int v, int hit, const double *p, const double *d);
+/* batch front end for the tests: locate from the world, step (limit), safety,
+ * touchable after the crossing (or the same one when the limit comes first) */
+void gxo_csg_probe(const gxo_csg_t *g, int n, const double *pos, const double *dir, const double *limit, int *vol,
+                   double *snext, int *next, double *safety);
+int gxo_csg_node_count(const gxo_csg_t *g, int *nscore);
+/* info: lv, parent, score, material, children; tr: t[3], R[9] */
+void gxo_csg_node_info(const gxo_csg_t *g, int i, int *info, double *tr);
+
 /* ------------------------------------------------------------ transport */
 typedef struct {
-  int geometry;            /* 0: single box of material box_mat; 1: layered calorimeter */
+  int geometry;            /* 0: single box of material box_mat; 1: layered calorimeter; 2: csg */
   int axis;                /* layering / box axis (0 x, 1 y, 2 z) */
   int nlayers;
   double t_abs, t_gap;     /* absorber (Pb) and gap (LAr) thickness, mm */
@@ -181,6 +223,7 @@ typedef struct {
   int score_events;        /* number of event tallies (>=1) */
   int msc;                 /* 1: multiple scattering of e-/e+ (gxo_transport.c) */
   const float *field_map;  /* non-null: follow this field map (gxo_field_map_load) with RK4, Bz ignored */
+  const gxo_csg_t *csg;    /* geometry 2: the volume tree; tallies are [score_events][csg->nscore] */
 } gxo_config_t;
 
 typedef struct {

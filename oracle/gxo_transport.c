@@ -72,6 +72,7 @@ typedef struct {
  * (Pb), slab 1 gap = material 2 (LAr)); box: vol 0 = box material; -1 outside. */
 static int vol_material(const world_t *w, int vol)
 {
+  if (w->c->geometry == 2) return w->c->csg->node[vol].mat;
   if (w->c->geometry == 0) return w->c->box_mat;
   return (vol & 1) ? 2 : 1;
 }
@@ -109,6 +110,7 @@ static double trans_centre(const world_t *w, int b)
 static int locate(const world_t *w, const double *p, const double *d)
 {
   const gxo_config_t *c = w->c;
+  if (c->geometry == 2) return gxo_csg_locate(c->csg, 0, p, d, GXO_CSG_TOL);
   const double tol = 1e-12;
   int a = c->axis;
   for (int b = 0; b < 3; ++b) {
@@ -139,10 +141,12 @@ static int locate(const world_t *w, const double *p, const double *d)
 }
 
 /* Straight-line distance to the boundary of vol along d; *plane = -1 for the
- * low axis plane, +1 high axis plane, 2 transverse wall. */
+ * low axis plane, +1 high axis plane, 2 transverse wall (csg: the child
+ * entered, -1 leaving vol). */
 static double dist_to_out(const world_t *w, int vol, const double *p, const double *d, int *plane)
 {
   const gxo_config_t *c = w->c;
+  if (c->geometry == 2) return gxo_csg_step(c->csg, vol, p, d, DBL_MAX, plane);
   int a = c->axis;
   double lo, hi, dist = DBL_MAX;
   slab_bounds(w, vol, &lo, &hi);
@@ -172,6 +176,7 @@ static double dist_to_out(const world_t *w, int vol, const double *p, const doub
 static double safety(const world_t *w, int vol, const double *p)
 {
   const gxo_config_t *c = w->c;
+  if (c->geometry == 2) return gxo_csg_safety(c->csg, vol, p);
   int a = c->axis;
   double lo, hi;
   slab_bounds(w, vol, &lo, &hi);
@@ -199,6 +204,7 @@ static int next_volume(const world_t *w, int vol, int plane)
 static int relocate(const world_t *w, int vol, double *p, const double *d)
 {
   const double snap = 1e-6;
+  if (w->c->geometry == 2) return gxo_csg_locate(w->c->csg, vol, p, d, snap);
   int a = w->c->axis;
   double lo, hi;
   slab_bounds(w, vol, &lo, &hi);
@@ -426,10 +432,12 @@ typedef struct {
   double escaped;
   long long steps, substeps, tracks, sec[3], npair, nannih, errors;
   int *pstep;
+  const gxo_csg_t *csg; /* geometry 2: tally bins are the touchables' score indices */
 } tally_t;
 
 static void deposit(tally_t *t, int event, int vol, double e)
 {
+  if (vol >= 0 && t->csg) vol = t->csg->node[vol].score; /* unscored touchables: -1 */
   if (vol >= 0 && e != 0.0) t->edep[(long)event * t->nvol + vol] += e;
 }
 
@@ -666,9 +674,12 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
     if (d < pstep) {
       step = d;
       crossed = 1;
-      newvol = next_volume(w, tr->vol, plane);
       for (int k = 0; k < 3; ++k) tr->pos[k] += step * tr->dir[k];
-      if (plane != 2) {
+      if (w->c->geometry == 2)
+        newvol = gxo_csg_cross(w->c->csg, tr->vol, plane, tr->pos, tr->dir);
+      else
+        newvol = next_volume(w, tr->vol, plane);
+      if (plane != 2 && w->c->geometry != 2) {
         double lo, hi;
         slab_bounds(w, tr->vol, &lo, &hi);
         tr->pos[w->c->axis] = plane > 0 ? hi : lo;
@@ -818,6 +829,7 @@ int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const
   for (int m = 0; m < 3; ++m) msc_material(w.mat[m].Z, w.mat[m].radlen, &w.msc[m]);
   int nt = cfg->nthreads > 0 ? cfg->nthreads : 1;
   int nvol = res->nvol;
+  if (cfg->geometry == 2 && (!cfg->csg || nvol != cfg->csg->nscore)) return -1;
   int nev = cfg->score_events > 0 ? cfg->score_events : 1;
   job_t *jobs = (job_t *)calloc(nt, sizeof(job_t));
   pthread_t *th = (pthread_t *)calloc(nt, sizeof(pthread_t));
@@ -830,6 +842,7 @@ int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const
     jobs[k].t.nvol = nvol;
     jobs[k].t.edep = (double *)calloc((size_t)nev * nvol, sizeof(double));
     jobs[k].t.pstep = res->primary_steps;
+    jobs[k].t.csg = cfg->geometry == 2 ? cfg->csg : NULL;
     pthread_create(&th[k], NULL, worker, &jobs[k]);
   }
   memset(res->edep, 0, sizeof(double) * (size_t)nev * nvol);

@@ -46,7 +46,7 @@ class Config(C.Structure):
                 ("half_trans", D), ("box_half", D * 3), ("box_centre", D * 3), ("box_mat", I),
                 ("Bz", D), ("charged_local", I), ("max_steps", I), ("seed", D * 6),
                 ("first_substream", L), ("nthreads", I), ("score_events", I), ("msc", I),
-                ("field_map", C.c_void_p)]
+                ("field_map", C.c_void_p), ("csg", C.c_void_p)]
 
 
 MODEL_IDS = {"kn": 0, "sg": 1, "bh": 2, "sb": 3, "mb": 4, "bhabha": 5, "annih": 6}
@@ -230,6 +230,59 @@ class Oracle:
         B = np.zeros_like(pos)
         f(handle, len(pos), dp(pos), dp(B))
         return B
+
+    # --------------------------------------------------------- CSG geometry
+    def csg_build(self, geo):
+        """the oracle's flattened tree (gxo_csg_build) of a package
+        CsgGeometry; the handle goes into Config.csg"""
+        f = self.lib.gxo_csg_build
+        f.restype = C.c_void_p
+        f.argtypes = [I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p,
+                      C.c_void_p, C.c_void_p, I]
+        arrs = [np.ascontiguousarray(a) for a in (geo.skind, geo.spar, geo.lv_solid, geo.lv_mat, geo.lv_scored,
+                                                   geo.pv_mother, geo.pv_lv, geo.pv_t, geo.pv_r)]
+        self._keep = arrs
+        v = [a.ctypes.data_as(C.c_void_p) for a in arrs]
+        h = f(len(geo.skind), v[0], v[1], len(geo.lv_solid), v[2], v[3], v[4], len(geo.pv_mother), v[5], v[6], v[7],
+              v[8], geo.world)
+        assert h
+        return h
+
+    def csg_free(self, h):
+        self.lib.gxo_csg_free.argtypes = [C.c_void_p]
+        self.lib.gxo_csg_free(h)
+
+    def csg_counts(self, h):
+        f = self.lib.gxo_csg_node_count
+        f.argtypes = [C.c_void_p, C.POINTER(I)]
+        ns = I()
+        n = f(h, C.byref(ns))
+        return n, ns.value
+
+    def csg_node(self, h, i):
+        f = self.lib.gxo_csg_node_info
+        f.argtypes = [C.c_void_p, I, C.POINTER(I), C.POINTER(D)]
+        info, tr = (I * 5)(), (D * 12)()
+        f(h, i, info, tr)
+        return dict(zip(("lv", "parent", "score", "mat", "nkid"), list(info)), translation=tuple(tr[:3]),
+                    rotation=tuple(tr[3:]))
+
+    def csg_probe(self, h, pos, dirs, limit=1e30):
+        f = self.lib.gxo_csg_probe
+        f.argtypes = [C.c_void_p, I] + [C.c_void_p] * 7
+        pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)
+        dirs = np.ascontiguousarray(dirs, dtype=np.float64).reshape(-1, 3)
+        n = len(pos)
+        lim = np.ascontiguousarray(np.broadcast_to(np.asarray(limit, np.float64), (n,)))
+        vol, nxt = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        snext, saf = np.zeros(n), np.zeros(n)
+        f(h, n, *[a.ctypes.data_as(C.c_void_p) for a in (pos, dirs, lim, vol, snext, nxt, saf)])
+        return vol, snext, nxt, saf
+
+    def csg_contains(self, h, v, p, d, tol=1e-9):
+        f = self.lib.gxo_csg_contains
+        f.argtypes = [C.c_void_p, I, C.POINTER(D), C.POINTER(D), D]
+        return bool(f(h, v, (D * 3)(*p), (D * 3)(*d), tol))
 
     # --------------------------------------------------- multiple scattering
     def material(self, Z, A, density):

@@ -238,7 +238,7 @@ def test_injection_by_live_energy_leaves_results_unchanged(dm, n, capacity, wave
     assert np.array_equal(pa, pb)
     np.testing.assert_allclose(a, b, rtol=1e-9, atol=1e-9 * a.max())
     e0 = prims[1].sum()
-    assert abs(b.sum() + sb["escaped"] - e0) <= 1e-9 * e0
+    assert abs(b.sum() + sb["escaped"] - e0) <= 1e-4 * e0  # FP32 energies
 
 
 def test_run_command_line(capsys):
