@@ -27,6 +27,14 @@
 //     of the distance to its bounding box and the solid's own lower bound.
 // Solids: box (half lengths), tube (rmin, rmax, half length; full phi),
 // sphere (rmin, rmax).  Quadratic roots in the cancellation-free form.
+// A touchable with many children also carries a one-dimensional grid along
+// the axis that separates its children best: equal slabs of its bounding box,
+// each listing (in child order) the children whose bounding box overlaps it.
+// Locating looks only at the point's slab; the step walks the slabs the ray
+// crosses before the nearest boundary found so far; the safety looks at the
+// slabs within the current safety.  Every child that can matter is in a slab
+// looked at, and ties go to the lowest child index, so the results are those
+// of the plain loop over all children.
 // Products and sums are rounded separately (__dmul_rn / __dadd_rn), so that
 // the results do not depend on FMA contraction.
 #pragma once
@@ -40,6 +48,7 @@ constexpr double kCsgTol = 1e-9;    // surface tolerance (mm)
 constexpr double kCsgPad = 1e-6;    // bounding-box padding (mm)
 constexpr int kCsgMaxDepth = 64;    // tree depth, at most
 constexpr int kCsgMaxNodes = 1 << 22;
+constexpr int kCsgGridMin = 8;      // children from which a touchable gets a grid
 constexpr double kCsgInf = 1.7976931348623157e308;
 
 struct CsgNode {
@@ -47,14 +56,29 @@ struct CsgNode {
   double r[9];         // global rotation, row-major (x_global = R x_local + t)
   double lo[3], hi[3]; // global bounding box, padded
   double a, b, c;      // box: half lengths; tube: rmin, rmax, half length in z; sphere: rmin, rmax
+  double glo, ginv, gw; // grid: start along the axis, slabs per mm, slab width
   int kind, rot;       // rot 0: R is the identity
   int mat, parent, kid0, nkid;
+  int gaxis, gn, g0;   // grid axis (-1: none), slabs, first slab's entry in the slab table
 };
 
 struct CsgView {
   const CsgNode *node; // node 0 is the world
   const int *kids;
+  const int *slab;     // per slab: first candidate, candidates (pairs)
+  const int *cand;     // candidates (touchable indices)
 };
+
+// Slab of coordinate x in a touchable's grid (host and device alike).
+__host__ __device__ __forceinline__ int csg_slab(const CsgNode &n, double x)
+{
+  const double u = (x - n.glo) * n.ginv;
+  return u >= 0.0 ? (u < (double)n.gn ? (int)u : n.gn - 1) : 0;
+}
+template <class T> __host__ __device__ __forceinline__ T csg_comp(const T *p, int a)
+{
+  return a == 0 ? p[0] : (a == 1 ? p[1] : p[2]);
+}
 
 __device__ __forceinline__ double cmul(double a, double b) { return __dmul_rn(a, b); }
 __device__ __forceinline__ double cadd(double a, double b) { return __dadd_rn(a, b); }
@@ -321,11 +345,21 @@ __device__ __forceinline__ bool csg_contains(const CsgView &g, int v, const doub
 __device__ __forceinline__ int csg_descend(const CsgView &g, int v, const double *p, const double *d, double tol)
 {
   for (int depth = 0; depth < kCsgMaxDepth; ++depth) {
-    const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
+    const CsgNode &n = g.node[v];
     int next = -1;
-    for (int k = 0; k < nk && next < 0; ++k) {
-      const int c = g.kids[k0 + k];
-      if (csg_contains(g, c, p, d, tol)) next = c;
+    if (n.gaxis >= 0) {
+      const int sl = n.g0 + csg_slab(n, csg_comp(p, n.gaxis));
+      const int j0 = g.slab[2 * sl], nj = g.slab[2 * sl + 1];
+      for (int j = 0; j < nj && next < 0; ++j) {
+        const int c = g.cand[j0 + j];
+        if (csg_contains(g, c, p, d, tol)) next = c;
+      }
+    } else {
+      const int k0 = n.kid0, nk = n.nkid;
+      for (int k = 0; k < nk && next < 0; ++k) {
+        const int c = g.kids[k0 + k];
+        if (csg_contains(g, c, p, d, tol)) next = c;
+      }
     }
     if (next < 0) return v;
     v = next;
@@ -351,20 +385,39 @@ __device__ __forceinline__ double csg_step(const CsgView &g, int v, const double
                                            int &hit)
 {
   double q[3], e[3];
-  csg_local(g.node[v], p, d, q, e);
-  double s = csg_dist_out_local(g.node[v], q, e);
+  const CsgNode &n = g.node[v];
+  csg_local(n, p, d, q, e);
+  double s = csg_dist_out_local(n, q, e);
   hit = -1;
-  const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
-  for (int k = 0; k < nk; ++k) {
-    const int c = g.kids[k0 + k];
+  auto child = [&](int c) {
     const double tb = csg_bbox_ray(g.node[c], p, d);
-    if (!(tb < s && tb < limit)) continue;
+    if (!(tb < s && tb < limit)) return;
     csg_local(g.node[c], p, d, q, e);
     const double t = csg_dist_in_local(g.node[c], q, e);
-    if (t < s) {
+    if (t < s || (t == s && hit >= 0 && c < hit)) {
       s = t;
       hit = c;
     }
+  };
+  if (n.gaxis >= 0) {
+    // the slabs in the order the ray crosses them, while their entry (moved
+    // back by the bounding-box padding) comes before the nearest boundary
+    const double pa = csg_comp(p, n.gaxis), da = csg_comp(d, n.gaxis);
+    const int step = da > 0.0 ? 1 : (da < 0.0 ? -1 : 0);
+    int sl = csg_slab(n, pa);
+    for (int it = 0; it < n.gn; ++it) {
+      const int row = n.g0 + sl;
+      const int j0 = g.slab[2 * row], nj = g.slab[2 * row + 1];
+      for (int j = 0; j < nj; ++j) child(g.cand[j0 + j]);
+      sl += step;
+      if (step == 0 || sl < 0 || sl >= n.gn) break;
+      const double xb = n.glo + (step > 0 ? sl : sl + 1) * n.gw - step * kCsgPad;
+      const double tb = (xb - pa) / da;
+      if (!(tb < s && tb < limit)) break;
+    }
+  } else {
+    const int k0 = n.kid0, nk = n.nkid;
+    for (int k = 0; k < nk; ++k) child(g.kids[k0 + k]);
   }
   return s;
 }
@@ -372,15 +425,28 @@ __device__ __forceinline__ double csg_step(const CsgView &g, int v, const double
 __device__ __forceinline__ double csg_safety(const CsgView &g, int v, const double *p)
 {
   double q[3];
-  csg_local_point(g.node[v], p, q);
-  double s = csg_safety_out_local(g.node[v], q);
-  const int k0 = g.node[v].kid0, nk = g.node[v].nkid;
-  for (int k = 0; k < nk; ++k) {
-    const CsgNode &m = g.node[g.kids[k0 + k]];
+  const CsgNode &n = g.node[v];
+  csg_local_point(n, p, q);
+  double s = csg_safety_out_local(n, q);
+  auto child = [&](int c) {
+    const CsgNode &m = g.node[c];
     const double gap = csg_bbox_gap(m, p);
-    if (gap >= s) continue;
+    if (gap >= s) return;
     csg_local_point(m, p, q);
     s = fmin(s, fmax(gap, csg_safety_in_local(m, q)));
+  };
+  if (n.gaxis >= 0) {
+    // children farther than the safety along the axis cannot lower it
+    const double pa = csg_comp(p, n.gaxis), r = fmax(s, 0.0) + kCsgPad;
+    const int s0 = csg_slab(n, pa - r), s1 = csg_slab(n, pa + r);
+    for (int sl = s0; sl <= s1; ++sl) {
+      const int row = n.g0 + sl;
+      const int j0 = g.slab[2 * row], nj = g.slab[2 * row + 1];
+      for (int j = 0; j < nj; ++j) child(g.cand[j0 + j]);
+    }
+  } else {
+    const int k0 = n.kid0, nk = n.nkid;
+    for (int k = 0; k < nk; ++k) child(g.kids[k0 + k]);
   }
   return s < 0.0 ? 0.0 : s;
 }

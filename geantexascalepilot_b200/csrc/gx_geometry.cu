@@ -37,6 +37,7 @@ struct gx_geom {
   int world = -1, nscore = 0;
   std::vector<gx::CsgNode> nodes;
   std::vector<int> kids, score, lv_of;
+  std::vector<int> slab, cand; // the children's grids (gx_csg.cuh)
 };
 
 namespace gx {
@@ -117,6 +118,9 @@ struct Flattener {
       n.nkid = (int)daughters[lv].size();
       n.kid0 = kcur; // the children's block, reserved before recursing
       kcur += n.nkid;
+      n.gaxis = -1;
+      n.gn = n.g0 = 0;
+      n.glo = n.ginv = n.gw = 0.0;
     }
     int j = 0;
     for (int p : daughters[lv]) {
@@ -133,6 +137,51 @@ struct Flattener {
     return id;
   }
 };
+
+// The slab grid of a touchable with many children: along each axis, slabs
+// of equal width over its bounding box, twice as many as children (at most
+// 4096); each child listed in the slabs its bounding box overlaps; the axis
+// with the fewest listings wins.
+void build_grid(gx_geom &g, int v)
+{
+  CsgNode &n = g.nodes[v];
+  if (n.nkid < kCsgGridMin) return;
+  const int gn = std::min(2 * n.nkid, 4096);
+  long best = -1;
+  int best_axis = -1;
+  for (int a = 0; a < 3; ++a) {
+    CsgNode t = n;
+    t.gn = gn;
+    t.glo = n.lo[a];
+    t.ginv = gn / (n.hi[a] - n.lo[a]);
+    long entries = 0;
+    for (int k = 0; k < n.nkid; ++k) {
+      const CsgNode &c = g.nodes[g.kids[n.kid0 + k]];
+      entries += csg_slab(t, c.hi[a]) - csg_slab(t, c.lo[a]) + 1;
+    }
+    if (best < 0 || entries < best) {
+      best = entries;
+      best_axis = a;
+    }
+  }
+  n.gaxis = best_axis;
+  n.gn = gn;
+  n.glo = n.lo[best_axis];
+  n.gw = (n.hi[best_axis] - n.lo[best_axis]) / gn;
+  n.ginv = gn / (n.hi[best_axis] - n.lo[best_axis]);
+  n.g0 = (int)(g.slab.size() / 2);
+  std::vector<std::vector<int>> lists(gn);
+  for (int k = 0; k < n.nkid; ++k) { // child order within every slab
+    const int c = g.kids[n.kid0 + k];
+    const int s0 = csg_slab(n, g.nodes[c].lo[best_axis]), s1 = csg_slab(n, g.nodes[c].hi[best_axis]);
+    for (int s = s0; s <= s1; ++s) lists[s].push_back(c);
+  }
+  for (int s = 0; s < gn; ++s) {
+    g.slab.push_back((int)g.cand.size());
+    g.slab.push_back((int)lists[s].size());
+    g.cand.insert(g.cand.end(), lists[s].begin(), lists[s].end());
+  }
+}
 
 bool orthonormal(const double *R)
 {
@@ -266,6 +315,9 @@ int gx_geom_close(gx_geom *g, int world, int *ntouchables, int *nscore)
   g->nscore = 0;
   const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, z[3] = {0, 0, 0};
   f.visit(world, -1, I, z, 0);
+  g->slab.clear();
+  g->cand.clear();
+  for (int v = 0; v < (int)g->nodes.size(); ++v) build_grid(*g, v);
   g->world = world;
   if (ntouchables) *ntouchables = (int)g->nodes.size();
   if (nscore) *nscore = g->nscore;
@@ -293,33 +345,30 @@ int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g)
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return cuda_error(e, "gx_ctx_load_geometry: cudaSetDevice");
-  const size_t nn = g->nodes.size(), nk = std::max<size_t>(g->kids.size(), 1);
+  const size_t nn = g->nodes.size();
   CsgNode *dn = nullptr;
-  int *dk = nullptr, *ds = nullptr;
+  int *dk = nullptr, *ds = nullptr, *dsl = nullptr, *dc = nullptr;
+  auto upload = [&](int **dst, const std::vector<int> &src) {
+    const size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(int);
+    cudaError_t r = cudaMalloc((void **)dst, bytes);
+    if (r == cudaSuccess && !src.empty()) r = cudaMemcpy(*dst, src.data(), src.size() * sizeof(int), cudaMemcpyHostToDevice);
+    return r;
+  };
   if ((e = cudaMalloc((void **)&dn, nn * sizeof(CsgNode))) != cudaSuccess ||
-      (e = cudaMalloc((void **)&dk, nk * sizeof(int))) != cudaSuccess ||
-      (e = cudaMalloc((void **)&ds, nn * sizeof(int))) != cudaSuccess) {
-    cudaFree(dn);
-    cudaFree(dk);
-    return cuda_error(e, "gx_ctx_load_geometry: allocation");
-  }
-  if ((e = cudaMemcpy(dn, g->nodes.data(), nn * sizeof(CsgNode), cudaMemcpyHostToDevice)) != cudaSuccess ||
-      (!g->kids.empty() &&
-       (e = cudaMemcpy(dk, g->kids.data(), g->kids.size() * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) ||
-      (e = cudaMemcpy(ds, g->score.data(), nn * sizeof(int), cudaMemcpyHostToDevice)) != cudaSuccess) {
-    cudaFree(dn);
-    cudaFree(dk);
-    cudaFree(ds);
+      (e = cudaMemcpy(dn, g->nodes.data(), nn * sizeof(CsgNode), cudaMemcpyHostToDevice)) != cudaSuccess ||
+      (e = upload(&dk, g->kids)) != cudaSuccess || (e = upload(&ds, g->score)) != cudaSuccess ||
+      (e = upload(&dsl, g->slab)) != cudaSuccess || (e = upload(&dc, g->cand)) != cudaSuccess) {
+    for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc}) cudaFree(q);
     return cuda_error(e, "gx_ctx_load_geometry: upload");
   }
   // the previous tree (if any) stays allocated until the context goes: a
   // captured transport graph may still refer to it
-  c->owned.push_back(dn);
-  c->owned.push_back(dk);
-  c->owned.push_back(ds);
+  for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc}) c->owned.push_back(q);
   c->csg_node = dn;
   c->csg_kids = dk;
   c->csg_score = ds;
+  c->csg_slab = dsl;
+  c->csg_cand = dc;
   c->csg_n = (int)nn;
   c->csg_nscore = g->nscore;
   return GX_OK;
@@ -333,7 +382,7 @@ int gx_geom_probe(gx_ctx *ctx, int n, const double *d_pos, const double *d_dir, 
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c->csg_node) return set_error(GX_ERR_ARG, "gx_geom_probe: no geometry loaded (gx_ctx_load_geometry)");
   if (n == 0) return GX_OK;
-  CsgView v{(const CsgNode *)c->csg_node, c->csg_kids};
+  CsgView v{c->csg_node, c->csg_kids, c->csg_slab, c->csg_cand};
   k_geom_probe<<<(n + 127) / 128, 128, 0, stream_of(s)>>>(v, n, d_pos, d_dir, d_limit, d_vol, d_snext, d_next,
                                                          d_safety);
   cudaError_t e = cudaGetLastError();

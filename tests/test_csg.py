@@ -42,6 +42,38 @@ def mixed_geometry():
     return gm.CloseGeometry()
 
 
+def crowded_geometry():
+    """a world holding 40 rotated boxes, tubes and spheres (its children get
+    the slab grid), one of them holding 12 more"""
+    from geantexascalepilot_b200 import geometry as G
+    rng = np.random.default_rng(23)
+    world = G.LogicalVolume("world", G.UnplacedBox(800.0, 800.0, 800.0))
+    holder = G.LogicalVolume("holder", G.UnplacedBox(60.0, 60.0, 60.0))
+    holder.SetMaterialPtr("G4_lAr")
+    holder.SetScored()
+    for k in range(12):
+        pin = G.LogicalVolume("pin%d" % k, G.UnplacedTube(0.0, 3.0, 50.0))
+        pin.SetMaterialPtr("G4_Pb")
+        pin.SetScored()
+        holder.PlaceDaughter("pin%d" % k, pin, G.Transformation3D(-44.0 + 8.0 * k, 0.0, 0.0))
+    for k in range(40):
+        x, y, z = -650.0 + 32.0 * k, rng.uniform(-600, 600), rng.uniform(-600, 600)
+        if k == 20:
+            world.PlaceDaughter("holder", holder, G.Transformation3D(x, y, z, 15.0, 25.0, 35.0))
+            continue
+        kind = k % 3
+        solid = (G.UnplacedBox(12.0, 40.0, 30.0) if kind == 0 else
+                 G.UnplacedTube(4.0, 14.0, 40.0) if kind == 1 else G.UnplacedSphere(5.0, 14.0))
+        lv = G.LogicalVolume("s%d" % k, solid)
+        lv.SetMaterialPtr(1 + k % 2)
+        lv.SetScored()
+        angles = rng.uniform(0, 180, 3) if k % 2 else (0.0, 0.0, 0.0)
+        world.PlaceDaughter("s%d" % k, lv, G.Transformation3D(x, y, z, *angles))
+    gm = G.GeoManager()
+    gm.SetWorld(world.Place())
+    return gm.CloseGeometry()
+
+
 class Tree:
     """point-in-solid by definition, for the checks"""
 
@@ -76,11 +108,11 @@ class Tree:
             v = nxt[0]
 
 
-def _rays(n, seed, targets):
+def _rays(n, seed, targets, sigma=80.0):
     rng = np.random.default_rng(seed)
     # points near the solids (so that the rays meet them) and uniform directions
     centres = np.array(targets)
-    p = centres[rng.integers(0, len(centres), n)] + rng.normal(0.0, 80.0, (n, 3))
+    p = centres[rng.integers(0, len(centres), n)] + rng.normal(0.0, sigma, (n, 3))
     d = rng.normal(size=(n, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     return p, d

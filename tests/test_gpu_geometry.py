@@ -8,7 +8,7 @@ import pytest
 import torch
 
 from oracle_ctypes import oracle_config
-from test_csg import _rays, mixed_geometry
+from test_csg import _rays, crowded_geometry, mixed_geometry
 
 pytestmark = pytest.mark.gpu
 
@@ -28,15 +28,27 @@ def _run(dm, cfg, prims, nvol, **kw):
     return edep.cpu().numpy(), st, ps.cpu().numpy()
 
 
-def test_probe_matches_oracle(dm, oracle):
+@pytest.mark.parametrize("name", ["mixed", "crowded", "calorimeter"])
+def test_probe_matches_oracle(dm, oracle, name):
     """locate, step, crossing and safety on 20000 rays: the same touchables
     and the same distances (products and sums are rounded separately on the
-    device, as in the oracle)"""
+    device, as in the oracle; the device's slab grids over many children give
+    the oracle's plain loops' results)"""
     from geantexascalepilot_b200 import geometry as G
-    geo = mixed_geometry()
+    sigma = 80.0
+    if name == "mixed":
+        geo = mixed_geometry()
+        centres = [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300)]
+    elif name == "crowded":
+        geo = crowded_geometry()
+        centres = [t["translation"] for t in geo.touchables() if t["parent"] >= 0]
+        sigma = 20.0
+    else:
+        geo = G.calorimeter(axis=0)
+        centres = [(-200.0 + 8.0 * k, 0.0, 0.0) for k in range(50)]
     geo.load(dm)
     h = oracle.csg_build(geo)
-    p, d = _rays(20000, 3, [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300)])
+    p, d = _rays(20000, 3, centres, sigma)
     lim = np.where(np.arange(len(p)) % 4 == 0, 30.0, 1e30)
     ov, os_, on, osf = oracle.csg_probe(h, p, d, lim)
     gv, gs, gn, gsf = [t.cpu().numpy() for t in G.probe(dm, p, d, lim)]
@@ -44,7 +56,8 @@ def test_probe_matches_oracle(dm, oracle):
     assert np.array_equal(gv, ov)
     assert np.array_equal(gn, on)
     inside = ov >= 0
-    assert inside.sum() > 15000
+    assert inside.sum() > 8000
+    assert (on != ov)[inside].sum() > 2000
     np.testing.assert_array_equal(gs[inside], os_[inside])
     np.testing.assert_array_equal(gsf[inside], osf[inside])
 
