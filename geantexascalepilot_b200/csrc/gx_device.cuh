@@ -849,6 +849,22 @@ __device__ __forceinline__ double annih_xs_per_electron(double pi_rcl2, double k
   return pi_rcl2 * ((gamma2 + 4 * gam + 1.) * ::log(gam + bg) - (gam + 3.) * bg) / (bg2 * (gam + 1.));
 }
 
+// The same cross section times the material's electron density (1/mm), in
+// the working precision: FP64 as above; in the FP32-mixed build the Heitler
+// formula in FP32 (single-precision log and square root instead of the FP64
+// ones on every positron step; relative error ~1e-6).
+template <class R> __device__ __forceinline__ R annih_xs(const Data &d, int mat, R kin)
+{
+  if constexpr (sizeof(R) == 8) {
+    return d.mat_nel[mat] * annih_xs_per_electron(d.pi_rcl2, kin);
+  } else {
+    const float ekin = fmaxf(kin, (float)eV), tau = ekin / (float)kEMass, gam = tau + 1.0f;
+    const float bg2 = tau * (tau + 2.0f), bg = sqrtf(bg2);
+    const float f = ((gam * gam + 4.0f * gam + 1.0f) * logf(gam + bg) - (gam + 3.0f) * bg) / (bg2 * (gam + 1.0f));
+    return (float)(d.mat_nel[mat] * d.pi_rcl2) * f;
+  }
+}
+
 // Sandia photo-absorption below 200 keV (Geant4 photo-electric cross section
 // below the reference's LambdaPrim.phot table), 1/mm.
 __device__ __forceinline__ double pe_xs_sandia(const Data &d, int Z, double density, double e)

@@ -305,7 +305,7 @@ template <class R> __device__ __forceinline__ void cross_sections(const Data &d,
   } else {
     xs[0] = lambda_tab<R>(d, GX_Lambda_eIoni_ep, mat, e);
     xs[1] = lambda_tab<R>(d, GX_Lambda_eBrem_ep, mat, e);
-    xs[2] = (R)(d.mat_nel[mat] * annih_xs_per_electron(d.pi_rcl2, (double)e));
+    xs[2] = annih_xs<R>(d, mat, e);
   }
 #pragma unroll
   for (int i = 0; i < 3; ++i)
