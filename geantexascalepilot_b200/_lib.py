@@ -72,6 +72,11 @@ class GunParams(C.Structure):
                 ("first_draw", LL), ("first_event", I)]
 
 
+class SpotGunParams(C.Structure):
+    _fields_ = [("seed", D * 6), ("stream", LL), ("first", LL), ("ntypes", I), ("types", I * 3), ("emin", D),
+                ("emax", D), ("cone_deg", D), ("axis", I), ("centre", D * 3), ("half", D * 2)]
+
+
 AUTOTUNE_MAX_TRIALS = 64
 
 
@@ -125,6 +130,8 @@ _SIGS = {
     "gx_hepevt_load": (I, [C.c_char_p, I, I, PD, I, P, P, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I), P]),
     "gx_transport_run_noalloc": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I,
                                      C.POINTER(TransportStats), P]),
+    "gx_spot_gun": (I, [C.POINTER(SpotGunParams), LL, P, P, P, P, P]),
+    "gx_spot_gun_host": (I, [C.POINTER(SpotGunParams), LL, P, P, P, P]),
     "gx_geom_create": (I, [C.POINTER(P)]),
     "gx_geom_destroy": (None, [P]),
     "gx_geom_box": (I, [P, D, D, D, C.POINTER(I)]),

@@ -9,6 +9,7 @@ cannot be created and every call raises.
 """
 import ctypes as C
 
+import numpy as np
 import torch
 
 from . import _lib
@@ -421,6 +422,43 @@ def egamma_gun(nevents, nparticles, gamma_fraction=0.5, momentum=(1.0e3, 1.0e6),
     d = torch.empty((n, 3), dtype=torch.float64, device="cuda")
     check(lib.gx_egamma_gun(C.byref(g), _ptr(t), _ptr(E), _ptr(pos), _ptr(d), _ptr(ev), _ptr(pdg), _stream()))
     return t, E, pos, d, ev, pdg
+
+
+def _spot_params(n, types, energy, cone_deg, axis, centre, half, seed, stream, first):
+    from ._lib import SpotGunParams
+    g = SpotGunParams()
+    g.seed[:] = [float(x) for x in seed]
+    g.stream, g.first = stream, first
+    g.ntypes = len(types)
+    g.types[:len(types)] = list(types)
+    g.emin, g.emax = energy
+    g.cone_deg, g.axis = cone_deg, axis
+    g.centre[:] = list(centre)
+    g.half[:] = list(half)
+    return g
+
+
+def spot_gun(n, types=(ELECTRON, POSITRON, GAMMA), energy=(10.0, 1.0e5), cone_deg=5.0, axis=2,
+             centre=(0.0, 0.0, -200.0), half=(10.0, 10.0), seed=(12345.0,) * 6, stream=1, first=0, device=True):
+    """Beam-spot gun of the throughput workloads (gx_spot_gun): n primaries
+    from MRG32k3a stream `stream` of the seed, five draws each (log-uniform
+    kinetic energy in `energy`, direction in a cone about +axis, start on the
+    spot centre +- half); types cycle through `types`.  Defaults: C4's.
+    device=True returns CUDA tensors (types, E, pos, dir); device=False runs
+    the host version (gx_spot_gun_host) into numpy arrays."""
+    g = _spot_params(n, types, energy, cone_deg, axis, centre, half, seed, stream, first)
+    if device:
+        t = torch.empty(max(n, 1), dtype=torch.int32, device="cuda")
+        E = torch.empty(max(n, 1), dtype=torch.float64, device="cuda")
+        pos = torch.empty((max(n, 1), 3), dtype=torch.float64, device="cuda")
+        d = torch.empty((max(n, 1), 3), dtype=torch.float64, device="cuda")
+        check(lib.gx_spot_gun(C.byref(g), n, _ptr(t), _ptr(E), _ptr(pos), _ptr(d), _stream()))
+        return t[:n], E[:n], pos[:n], d[:n]
+    t, E = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1))
+    pos, d = np.zeros((max(n, 1), 3)), np.zeros((max(n, 1), 3))
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)  # noqa: E731
+    check(lib.gx_spot_gun_host(C.byref(g), n, vp(t), vp(E), vp(pos), vp(d)))
+    return t[:n], E[:n], pos[:n], d[:n]
 
 
 def set_direction_xyz(x, y, z, mode=MODE_PHYSICS):

@@ -13,7 +13,10 @@ C5  4096 events, Poisson(100) 10 GeV electrons each, 10 degree cone, 4 T,
 
 Calorimeter: 50 layers of 2.3 mm Pb + 5.7 mm LAr, 400 x 400 mm transverse,
 centred on the origin (the front face is at -200 mm on the layering axis).
-Primary generation is host-side numpy (PCG64) seeded from the config's seed.
+C4's primaries and C5's directions come from the beam-spot gun
+(gx_spot_gun_host: MRG32k3a stream 1 of the run seed, separate from the
+transport substreams); C5's multiplicities are Poisson draws of numpy's
+PCG64 seeded with 7.  C1-C3 are monoenergetic pencil beams.
 """
 import numpy as np
 
@@ -75,37 +78,27 @@ def c3(n_e=10000, n_g=10000):
     return cfg, (types, np.full(n, 10000.0), pos, d, None), 100
 
 
-def _cone(rng, n, half_angle_deg):
-    cmin = np.cos(np.radians(half_angle_deg))
-    cost = 1.0 - rng.random(n) * (1.0 - cmin)
-    phi = 2 * np.pi * rng.random(n)
-    sint = np.sqrt((1 - cost) * (1 + cost))
-    return np.stack([sint * np.cos(phi), sint * np.sin(phi), cost], 1)
-
-
 def c4(n=65536):
+    from .api import spot_gun
     cfg = calorimeter(base_config(12345), 2, 4.0)
-    rng = np.random.default_rng(12345)
-    types = (np.arange(n) % 3).astype(np.int32)
-    types = np.array([ELECTRON, POSITRON, GAMMA], np.int32)[types]
-    E = np.exp(rng.uniform(np.log(10.0), np.log(1.0e5), n))
-    pos = np.zeros((n, 3))
-    pos[:, 0] = rng.uniform(-10.0, 10.0, n)
-    pos[:, 1] = rng.uniform(-10.0, 10.0, n)
-    pos[:, 2] = -200.0
-    return cfg, (types, E, pos, _cone(rng, n, 5.0), None), 100
+    types, E, pos, d = spot_gun(n, types=(ELECTRON, POSITRON, GAMMA), energy=(10.0, 1.0e5), cone_deg=5.0, axis=2,
+                                centre=(0.0, 0.0, -200.0), half=(10.0, 10.0), seed=list(cfg.seed), stream=1,
+                                device=False)
+    return cfg, (types, E, pos, d, None), 100
 
 
 def c5(nevents=4096, mean=100):
+    from .api import spot_gun
     cfg = calorimeter(base_config(7), 2, 4.0)
     rng = np.random.default_rng(7)
     mult = rng.poisson(mean, nevents)
     n = int(mult.sum())
     events = np.repeat(np.arange(nevents, dtype=np.int32), mult)
     cfg.nevents = nevents
-    pos = np.zeros((n, 3))
-    pos[:, 2] = -200.0
-    return cfg, (np.full(n, ELECTRON, np.int32), np.full(n, 10000.0), pos, _cone(rng, n, 10.0), events), 100
+    types, E, pos, d = spot_gun(n, types=(ELECTRON,), energy=(1.0e4, 1.0e4), cone_deg=10.0, axis=2,
+                                centre=(0.0, 0.0, -200.0), half=(0.0, 0.0), seed=list(cfg.seed), stream=1,
+                                device=False)
+    return cfg, (types, E, pos, d, events), 100
 
 
 WORKLOADS = {"c1": c1, "c2": c2, "c3": c3, "c4": c4, "c5": c5}

@@ -121,6 +121,119 @@ __global__ void __launch_bounds__(256) k_egamma_gun(const uint64_t *__restrict__
   }
 }
 
+// The beam-spot gun (gx_spot_gun): one primary from its five uniforms.
+struct Spot {
+  long long n, first;
+  int ntypes, types[3], axis;
+  double emin, emax, cos_cone, centre[3], half[2];
+};
+
+__host__ __device__ __forceinline__ void spot_primary(const Spot &g, long long i, const double u[5], int *type,
+                                                      double *E, double *pos, double *dir)
+{
+  *type = g.types[i % g.ntypes];
+  *E = g.emin * ::exp(u[0] * ::log(g.emax / g.emin));
+  const double ct = 1.0 - u[1] * (1.0 - g.cos_cone), st = ::sqrt((1.0 - ct) * (1.0 + ct));
+  const double phi = 2.0 * kPi * u[2];
+  const int a = g.axis, b = (a + 1) % 3, c = (a + 2) % 3;
+  double d[3], p[3];
+  d[a] = ct;
+  d[b] = st * ::cos(phi);
+  d[c] = st * ::sin(phi);
+  p[a] = g.centre[a];
+  p[b] = g.centre[b] + g.half[0] * (2.0 * u[3] - 1.0);
+  p[c] = g.centre[c] + g.half[1] * (2.0 * u[4] - 1.0);
+  for (int k = 0; k < 3; ++k) {
+    dir[k] = d[k];
+    pos[k] = p[k];
+  }
+}
+
+// the stream's state (seed advanced by stream x 2^127, then by 5 first draws)
+void spot_start(const gx_spot_gun_params &p, uint64_t v1[3], uint64_t v2[3])
+{
+  const uint64_t m[2] = {kMod1, kMod2};
+  for (int k = 0; k < 3; ++k) {
+    v1[k] = (uint64_t)p.seed[k];
+    v2[k] = (uint64_t)p.seed[3 + k];
+  }
+  uint64_t J[9];
+  for (int c = 0; c < 2; ++c) {
+    jump_matrix(c, 127, 0, J);
+    for (long long s = 0; s < p.stream; ++s) mat_vec(J, c ? v2 : v1, m[c]);
+  }
+}
+
+__global__ void __launch_bounds__(256) k_spot_gun(const uint64_t *__restrict__ J, Spot g, uint64_t s0, uint64_t s1,
+                                                  uint64_t s2, uint64_t s3, uint64_t s4, uint64_t s5,
+                                                  int *__restrict__ type, double *__restrict__ E,
+                                                  double *__restrict__ pos, double *__restrict__ dir)
+{
+  const long long first = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * kGunChunk;
+  if (first >= g.n) return;
+  const long long last = min(first + (long long)kGunChunk, g.n);
+  uint64_t v1[3] = {s0, s1, s2}, v2[3] = {s3, s4, s5};
+  unsigned long long k = 5ULL * (unsigned long long)(g.first + first);
+  for (int b = 0; k != 0 && b < 64; ++b, k >>= 1)
+    if (k & 1ULL) {
+      matvec_mod(J + 9 * b, v1, kMod1);
+      matvec_mod(J + 9 * (64 + b), v2, kMod2);
+    }
+  Mrg r;
+  for (int c = 0; c < 3; ++c) {
+    r.s[c] = (double)v1[c];
+    r.s[3 + c] = (double)v2[c];
+  }
+  for (long long i = first; i < last; ++i) {
+    double u[5];
+    for (int j = 0; j < 5; ++j) u[j] = r.u01();
+    spot_primary(g, g.first + i, u, &type[i], &E[i], &pos[3 * i], &dir[3 * i]);
+  }
+}
+
+// MRG32k3a on the host in exact integer arithmetic (the same numbers as the
+// device's FP64 recurrence)
+struct HostMrg {
+  int64_t s[6];
+  double u01()
+  {
+    const int64_t m1 = (int64_t)kMod1, m2 = (int64_t)kMod2;
+    int64_t p1 = ((int64_t)kA12 * s[1] - (int64_t)kA13n * s[0]) % m1;
+    if (p1 < 0) p1 += m1;
+    s[0] = s[1];
+    s[1] = s[2];
+    s[2] = p1;
+    int64_t p2 = ((int64_t)kA21 * s[5] - (int64_t)kA23n * s[3]) % m2;
+    if (p2 < 0) p2 += m2;
+    s[3] = s[4];
+    s[4] = s[5];
+    s[5] = p2;
+    return (double)(p1 > p2 ? p1 - p2 : p1 - p2 + m1) * kNorm;
+  }
+};
+
+int spot_check(const gx_spot_gun_params *p, long long n, Spot &g)
+{
+  if (!p || n < 0) return set_error(GX_ERR_ARG, "gx_spot_gun: bad arguments");
+  if (p->ntypes < 1 || p->ntypes > 3 || p->axis < 0 || p->axis > 2 || p->stream < 0 || p->first < 0 ||
+      !(p->emin > 0.0 && p->emax >= p->emin) || !(p->cone_deg >= 0.0 && p->cone_deg <= 180.0))
+    return set_error(GX_ERR_ARG, "gx_spot_gun: bad parameters");
+  for (int k = 0; k < p->ntypes; ++k)
+    if (p->types[k] < 0 || p->types[k] > 2) return set_error(GX_ERR_ARG, "gx_spot_gun: bad particle type");
+  g.n = n;
+  g.first = p->first;
+  g.ntypes = p->ntypes;
+  for (int k = 0; k < 3; ++k) g.types[k] = p->types[k];
+  g.axis = p->axis;
+  g.emin = p->emin;
+  g.emax = p->emax;
+  g.cos_cone = ::cos(p->cone_deg * kPi / 180.0);
+  for (int k = 0; k < 3; ++k) g.centre[k] = p->centre[k];
+  g.half[0] = p->half[0];
+  g.half[1] = p->half[1];
+  return GX_OK;
+}
+
 // One HEPEVT event entry (G4HEPEvtInterface layout, as the reference reads
 // it, proxy/ProxyHepEvtGenerator.hpp:40-49).
 struct HepEntry {
@@ -180,6 +293,54 @@ int gx_egamma_gun(const gx_egamma_gun_params *p, int *d_type, double *d_E, doubl
                                                                                           d_dir, d_event, d_pdg);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GX_OK : cuda_error(e, "k_egamma_gun");
+}
+
+int gx_spot_gun(const gx_spot_gun_params *p, long long n, int *d_type, double *d_E, double *d_pos, double *d_dir,
+                gx_stream_t s)
+{
+  Spot g;
+  int rc = spot_check(p, n, g);
+  if (rc) return rc;
+  if (n > 0 && (!d_type || !d_E || !d_pos || !d_dir)) return set_error(GX_ERR_ARG, "gx_spot_gun: null output");
+  if (n == 0) return GX_OK;
+  uint64_t *J;
+  if ((rc = get_step_jump_table(&J))) return rc;
+  uint64_t v1[3], v2[3];
+  spot_start(*p, v1, v2);
+  const long long threads = (n + kGunChunk - 1) / kGunChunk;
+  k_spot_gun<<<(unsigned)((threads + 255) / 256), 256, 0, stream_of(s)>>>(J, g, v1[0], v1[1], v1[2], v2[0], v2[1],
+                                                                          v2[2], d_type, d_E, d_pos, d_dir);
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "k_spot_gun");
+}
+
+int gx_spot_gun_host(const gx_spot_gun_params *p, long long n, int *type, double *E, double *pos, double *dir)
+{
+  Spot g;
+  int rc = spot_check(p, n, g);
+  if (rc) return rc;
+  if (n > 0 && (!type || !E || !pos || !dir)) return set_error(GX_ERR_ARG, "gx_spot_gun_host: null output");
+  uint64_t v1[3], v2[3];
+  spot_start(*p, v1, v2);
+  if (p->first > 0) {
+    uint64_t J[9];
+    const uint64_t m[2] = {kMod1, kMod2};
+    for (int c = 0; c < 2; ++c) {
+      jump_matrix(c, 0, 5 * p->first, J);
+      mat_vec(J, c ? v2 : v1, m[c]);
+    }
+  }
+  HostMrg r;
+  for (int k = 0; k < 3; ++k) {
+    r.s[k] = (int64_t)v1[k];
+    r.s[3 + k] = (int64_t)v2[k];
+  }
+  for (long long i = 0; i < n; ++i) {
+    double u[5];
+    for (int j = 0; j < 5; ++j) u[j] = r.u01();
+    spot_primary(g, p->first + i, u, &type[i], &E[i], &pos[3 * i], &dir[3 * i]);
+  }
+  return GX_OK;
 }
 
 int gx_pdg_to_type(int pdg) { return pdg_to_type(pdg); }

@@ -328,6 +328,32 @@ typedef struct {
 } gx_egamma_gun_params;
 int gx_egamma_gun(const gx_egamma_gun_params *p, int *d_type, double *d_E, double *d_pos, double *d_dir,
                   int *d_event, int *d_pdg, gx_stream_t s);
+/* Beam-spot gun of the throughput workloads (C4: 2^16 e-/e+/gamma,
+ * log-uniform 10 MeV - 100 GeV, 5 degree cone, 2 x 2 cm spot; C5's
+ * directions): its own MRG32k3a stream, stream `stream` of the run seed
+ * (streams 2^127 draws apart; C4 uses stream 1), separate from the transport
+ * substreams of the same seed.  Primary i (counted from 0 over all calls;
+ * first = index of the first one written) takes draws 5i .. 5i+4: u0 the
+ * kinetic energy emin (emax / emin)^u0, u1 cos theta = 1 - u1 (1 - cos cone),
+ * u2 phi = 2 pi u2 (direction about +axis; the transverse axes in cyclic
+ * order), u3, u4 the start centre +- half[k] (2u - 1) in the two transverse
+ * coordinates; type = types[i % ntypes] (0 gamma, 1 e-, 2 e+).  The device
+ * version jumps each thread to its first draw; the host version draws in
+ * sequence; both write the same primaries. */
+typedef struct {
+  double seed[6];           /* run seed (MRG32k3a state) */
+  long long stream;         /* stream of the seed the gun draws from (>= 0) */
+  long long first;          /* index of the first primary written */
+  int ntypes, types[3];
+  double emin, emax;        /* MeV, emin <= emax */
+  double cone_deg;          /* half angle of the direction cone, degrees */
+  int axis;                 /* beam axis 0 x, 1 y, 2 z */
+  double centre[3];         /* spot centre, mm */
+  double half[2];           /* spot half widths along the two transverse axes, mm */
+} gx_spot_gun_params;
+int gx_spot_gun(const gx_spot_gun_params *p, long long n, int *d_type, double *d_E, double *d_pos, double *d_dir,
+                gx_stream_t s);
+int gx_spot_gun_host(const gx_spot_gun_params *p, long long n, int *type, double *E, double *pos, double *dir);
 /* Particle type of the transport (0 gamma, 1 e-, 2 e+) for a PDG code, -1 for
  * the particles the EM path does not transport. */
 int gx_pdg_to_type(int pdg);

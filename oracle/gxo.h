@@ -279,6 +279,10 @@ double gxo_cut_convert(int particle, int nelem, const double *Z, const double *n
 int gxo_egamma_gun(gxo_mrg_t *r, int nevents, int nparticles, double gamma_fraction, double minp, double maxp,
                    double mineta, double maxeta, double minphi, double maxphi, int *pdg, double *p, double *ekin,
                    double *dir);
+/* the library's beam-spot gun (gx_spot_gun), restated */
+int gxo_spot_gun(const double seed[6], long stream, long first, int n, int ntypes, const int *types, double emin,
+                 double emax, double cone_deg, int axis, const double centre[3], const double half[2], int *type,
+                 double *E, double *pos, double *dir);
 void gxo_egamma_dir(int physics, double x, double y, double z, double *eta, double *phi);
 int gxo_hepevt_read(const char *path, int physics, int max_events, int cap, int *event, int *pdg, double *p,
                     double *ekin, double *dir, int *nev_read, int *bad);

@@ -133,3 +133,40 @@ int gxo_hepevt_read(const char *path, int physics, int max_events, int cap, int 
   *nev_read = nev;
   return k;
 }
+
+/* The beam-spot gun of the throughput workloads (the library's gx_spot_gun;
+ * the reference has no such gun: its benchmarks start from ProxyEgammaGun or
+ * HEPEVT files).  Stream `stream` of the seed (SetNextStream applied
+ * stream + 1 times, MRG32k3a.cpp:51-58); primary i takes draws 5i .. 5i+4,
+ * drawn here in sequence from draw 0: kinetic energy emin (emax / emin)^u0,
+ * cos theta = 1 - u1 (1 - cos cone), phi = 2 pi u2 about +axis (transverse
+ * axes in cyclic order), start centre +- half (2u - 1) in the two transverse
+ * coordinates, type = types[i % ntypes]. */
+int gxo_spot_gun(const double seed[6], long stream, long first, int n, int ntypes, const int *types, double emin,
+                 double emax, double cone_deg, int axis, const double centre[3], const double half[2], int *type,
+                 double *E, double *pos, double *dir)
+{
+  double sd[6];
+  gxo_mrg_t r;
+  for (int k = 0; k < 6; ++k) sd[k] = seed[k];
+  for (long s = 0; s <= stream; ++s) gxo_mrg_next_stream(sd, &r);
+  for (long j = 0; j < 5 * first; ++j) gxo_mrg_u01(&r);
+  const double pi = 3.14159265358979323846;
+  const double cc = cos(cone_deg * pi / 180.0);
+  const int b = (axis + 1) % 3, c = (axis + 2) % 3;
+  for (int i = 0; i < n; ++i) {
+    double u[5];
+    for (int j = 0; j < 5; ++j) u[j] = gxo_mrg_u01(&r);
+    type[i] = types[(first + i) % ntypes];
+    E[i] = emin * exp(u[0] * log(emax / emin));
+    double ct = 1.0 - u[1] * (1.0 - cc), st = sqrt((1.0 - ct) * (1.0 + ct)), phi = 2.0 * pi * u[2];
+    double *d = dir + 3 * i, *p = pos + 3 * i;
+    d[axis] = ct;
+    d[b] = st * cos(phi);
+    d[c] = st * sin(phi);
+    p[axis] = centre[axis];
+    p[b] = centre[b] + half[0] * (2.0 * u[3] - 1.0);
+    p[c] = centre[c] + half[1] * (2.0 * u[4] - 1.0);
+  }
+  return n;
+}

@@ -328,6 +328,16 @@ class Oracle:
         assert k == n
         return pdg, p, ek, d, st
 
+    def spot_gun(self, seed, stream, first, n, types, energy, cone_deg, axis, centre, half):
+        f = self.lib.gxo_spot_gun
+        f.argtypes = [C.POINTER(D), L, L, I, I, C.POINTER(I), D, D, D, I, C.POINTER(D), C.POINTER(D)] + \
+            [C.c_void_p] * 4
+        t, E = np.zeros(max(n, 1), np.int32), np.zeros(max(n, 1))
+        pos, d = np.zeros((max(n, 1), 3)), np.zeros((max(n, 1), 3))
+        f((D * 6)(*seed), stream, first, n, len(types), (I * 3)(*types), energy[0], energy[1], cone_deg, axis,
+          (D * 3)(*centre), (D * 2)(*half), *[a.ctypes.data_as(C.c_void_p) for a in (t, E, pos, d)])
+        return t[:n], E[:n], pos[:n], d[:n]
+
     def egamma_dir(self, physics, x, y, z):
         f = self.lib.gxo_egamma_dir
         f.argtypes = [I, D, D, D, C.POINTER(D), C.POINTER(D)]

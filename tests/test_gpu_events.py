@@ -100,3 +100,19 @@ def test_transport_from_the_gun():
     assert abs(edep.sum().item() + st["escaped"] - e0) <= 1e-9 * e0
     assert edep.shape == (8, nvol) and torch.all(edep.sum(1) > 0)
     dm.close()
+
+
+def test_spot_gun_device_equals_host():
+    """the device beam-spot gun (each thread jumps to its first draw) writes
+    the host version's primaries: positions and types exactly, energies and
+    directions to the last bits of the device's exp / log / sin / cos"""
+    import geantexascalepilot_b200 as gx
+    kw = dict(types=(1, 2, 0), energy=(10.0, 1.0e5), cone_deg=5.0, axis=0, centre=(-200.0, 1.0, 2.0),
+              half=(10.0, 5.0), seed=(7.0,) * 6, stream=1)
+    for first, n in ((0, 50000), (12345, 777)):
+        h = gx.spot_gun(n, first=first, device=False, **kw)
+        g = [x.cpu().numpy() for x in gx.spot_gun(n, first=first, device=True, **kw)]
+        np.testing.assert_array_equal(g[0], h[0])
+        np.testing.assert_array_equal(g[2], h[2])
+        np.testing.assert_allclose(g[1], h[1], rtol=1e-14)
+        np.testing.assert_allclose(g[3], h[3], rtol=1e-14, atol=1e-15)

@@ -110,3 +110,45 @@ def test_hepevt_edge_cases(oracle, tmp_path):
         gx.hepevt_read(str(tmp_path / "missing.data"))
     # max_events stops early
     assert gx.hepevt_read(SAMPLE, max_events=3)["nevents"] == 3
+
+
+SPOT_C4 = dict(types=(1, 2, 0), energy=(10.0, 1.0e5), cone_deg=5.0, axis=2, centre=(0.0, 0.0, -200.0),
+               half=(10.0, 10.0))
+
+
+def test_spot_gun_host_matches_oracle(oracle):
+    """The library's host beam-spot gun (C4's generator) and the oracle's
+    restatement: the same primaries from stream 1 of the seed, also when a
+    shard starts at primary `first` (jumped, against drawn in sequence)."""
+    import geantexascalepilot_b200 as gx
+    seed = (12345.0,) * 6
+    t, E, p, d = gx.spot_gun(3000, seed=seed, stream=1, device=False, **SPOT_C4)
+    o = oracle.spot_gun(seed, 1, 0, 3000, SPOT_C4["types"], SPOT_C4["energy"], SPOT_C4["cone_deg"], SPOT_C4["axis"],
+                        SPOT_C4["centre"], SPOT_C4["half"])
+    for a, b in zip((t, E, p, d), o):
+        np.testing.assert_array_equal(a, b)
+    t2, E2, p2, d2 = gx.spot_gun(1000, seed=seed, stream=1, first=2000, device=False, **SPOT_C4)
+    np.testing.assert_array_equal(E2, E[2000:])
+    np.testing.assert_array_equal(d2, d[2000:])
+    np.testing.assert_array_equal(t2, t[2000:])
+    # C4's shape: types cycle, log-uniform energy, 5 degree cone, 2 x 2 cm spot
+    assert list(t[:6]) == [1, 2, 0, 1, 2, 0]
+    assert E.min() >= 10.0 and E.max() <= 1.0e5
+    assert abs(np.log(E).mean() - 0.5 * (np.log(10.0) + np.log(1.0e5))) < 0.1
+    assert np.all(d[:, 2] >= np.cos(np.radians(5.0)) - 1e-15)
+    np.testing.assert_allclose(np.linalg.norm(d, axis=1), 1.0, rtol=1e-15)
+    assert np.all(np.abs(p[:, :2]) <= 10.0) and np.all(p[:, 2] == -200.0)
+    # another stream, and the transport's substreams, are other numbers
+    _, E0, _, _ = gx.spot_gun(10, seed=seed, stream=0, device=False, **SPOT_C4)
+    assert not np.any(E0 == E[:10])
+
+
+def test_spot_gun_rejects_bad_arguments():
+    import geantexascalepilot_b200 as gx
+    from geantexascalepilot_b200 import GxError
+    for bad in (dict(energy=(0.0, 1.0)), dict(energy=(2.0, 1.0)), dict(types=(3,)), dict(axis=3),
+                dict(cone_deg=200.0), dict(stream=-1)):
+        kw = dict(SPOT_C4)
+        kw.update(bad)
+        with pytest.raises(GxError):
+            gx.spot_gun(4, device=False, **kw)
