@@ -370,7 +370,7 @@ def main():
         if k in per:
             traffic = per[k] * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": traffic, "kernel": "k_transport<float,%d> (%s)" % (k, ["gamma", "e-", "e+"][k]),
+                       "traffic": traffic, "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "algorithmic_bytes_per_launch": nbytes / launches_k,
                        "avg_launch_ms": stp["transport_ms"][k] / launches_k,
