@@ -137,6 +137,7 @@ _SIGS = {
     "gx_geom_box": (I, [P, D, D, D, C.POINTER(I)]),
     "gx_geom_tube": (I, [P, D, D, D, C.POINTER(I)]),
     "gx_geom_sphere": (I, [P, D, D, C.POINTER(I)]),
+    "gx_geom_polyhedron": (I, [P, I, PD, C.POINTER(I)]),
     "gx_geom_logical_volume": (I, [P, I, I, I, C.POINTER(I)]),
     "gx_geom_place_daughter": (I, [P, I, I, PD, PD, C.POINTER(I)]),
     "gx_geom_close": (I, [P, I, C.POINTER(I), C.POINTER(I)]),

@@ -26,7 +26,10 @@
 //   - safety: to the current solid's surface and, for each child, the larger
 //     of the distance to its bounding box and the solid's own lower bound.
 // Solids: box (half lengths), tube (rmin, rmax, half length; full phi),
-// sphere (rmin, rmax).  Quadratic roots in the cancellation-free form.
+// sphere (rmin, rmax), convex polyhedron (the intersection of half-spaces
+// n.x <= d, unit outward normals: trapezoids such as VecGeom's UnplacedTrd,
+// prisms, wedges).  Quadratic roots in the cancellation-free form; the
+// polyhedron's ray distances by clipping the ray against each plane.
 // A touchable with many children also carries a one-dimensional grid along
 // the axis that separates its children best: equal slabs of its bounding box,
 // each listing (in child order) the children whose bounding box overlaps it.
@@ -43,7 +46,8 @@
 
 namespace gx {
 
-enum { kCsgBox = 0, kCsgTube = 1, kCsgSphere = 2 };
+enum { kCsgBox = 0, kCsgTube = 1, kCsgSphere = 2, kCsgPoly = 3 };
+constexpr int kCsgMaxPlanes = 32;   // planes of one polyhedron, at most
 constexpr double kCsgTol = 1e-9;    // surface tolerance (mm)
 constexpr double kCsgPad = 1e-6;    // bounding-box padding (mm)
 constexpr int kCsgMaxDepth = 64;    // tree depth, at most
@@ -60,6 +64,7 @@ struct CsgNode {
   int kind, rot;       // rot 0: R is the identity
   int mat, parent, kid0, nkid;
   int gaxis, gn, g0;   // grid axis (-1: none), slabs, first slab's entry in the slab table
+  int p0, np;          // polyhedron: first plane in the plane table, planes
 };
 
 struct CsgView {
@@ -67,6 +72,7 @@ struct CsgView {
   const int *kids;
   const int *slab;     // per slab: first candidate, candidates (pairs)
   const int *cand;     // candidates (touchable indices)
+  const double *planes; // polyhedra: (nx, ny, nz, d) per plane
 };
 
 // Slab of coordinate x in a touchable's grid (host and device alike).
@@ -121,9 +127,52 @@ __device__ __forceinline__ double dot3(const double *a, const double *b)
   return cadd(cadd(cmul(a[0], b[0]), cmul(a[1], b[1])), cmul(a[2], b[2]));
 }
 
-// inside, or on the surface and not moving out through it
-__device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const double *q, const double *e, double tol)
+// The convex polyhedron's queries: op 0 contains (1 or 0), 1 distance out,
+// 2 distance in, 3 safety out, 4 safety in (a constant at every call site).
+enum { kPolyContains = 0, kPolyOut = 1, kPolyIn = 2, kPolySafeOut = 3, kPolySafeIn = 4 };
+__device__ __forceinline__ double csg_poly(const double *__restrict__ pl, int p0, int np, double q0, double q1,
+                                        double q2, double e0, double e1, double e2, int op, double tol)
 {
+  double tmin = -kCsgInf, tmax = kCsgInf, s = (op == kPolySafeIn) ? -kCsgInf : kCsgInf;
+  for (int k = p0; k < p0 + np; ++k) {
+    const double *p = pl + 4 * k;
+    // n.q - d and n.e
+    const double h = csub(cadd(cadd(cmul(p[0], q0), cmul(p[1], q1)), cmul(p[2], q2)), p[3]);
+    const double ne = cadd(cadd(cmul(p[0], e0), cmul(p[1], e1)), cmul(p[2], e2));
+    if (op == kPolyContains) {
+      if (h > tol || (h >= -tol && ne > 0.0)) return 0.0;
+    } else if (op == kPolyOut) {
+      if (ne > 0.0) s = fmin(s, -h / ne);
+    } else if (op == kPolyIn) {
+      if (ne == 0.0) {
+        if (h > 0.0) return kCsgInf;
+        continue;
+      }
+      const double t = -h / ne;
+      if (ne < 0.0)
+        tmin = fmax(tmin, t);
+      else
+        tmax = fmin(tmax, t);
+    } else if (op == kPolySafeOut) {
+      s = fmin(s, -h);
+    } else {
+      s = fmax(s, h);
+    }
+  }
+  if (op == kPolyContains) return 1.0;
+  if (op == kPolyOut) return s < 0.0 ? 0.0 : s;
+  if (op == kPolyIn) {
+    if (!(tmax > tmin) || tmax <= tol) return kCsgInf;
+    return tmin < 0.0 ? 0.0 : tmin;
+  }
+  return s;
+}
+
+// inside, or on the surface and not moving out through it
+__device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const double *q, const double *e, double tol,
+                                                   const double *pl)
+{
+  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyContains, tol) != 0.0;
   if (n.kind == kCsgBox) {
     const double h0 = n.a, h1 = n.b, h2 = n.c;
     const double a0 = fabs(q[0]), a1 = fabs(q[1]), a2 = fabs(q[2]);
@@ -164,9 +213,11 @@ __device__ __forceinline__ double near_root(double a, double b, double c, double
 }
 
 // distance to leave the solid from a point inside it (or on its surface)
-__device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const double *q, const double *e)
+__device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const double *q, const double *e,
+                                                     const double *pl)
 {
   double s = kCsgInf;
+  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyOut, 0.0);
   if (n.kind == kCsgBox) {
     const double h[3] = {n.a, n.b, n.c};
 #pragma unroll
@@ -206,9 +257,11 @@ __device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const dou
 }
 
 // distance to enter the solid from a point outside it; kCsgInf if missed
-__device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const double *q, const double *e)
+__device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const double *q, const double *e,
+                                                    const double *pl)
 {
   const double tol = kCsgTol;
+  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyIn, tol);
   if (n.kind == kCsgBox) {
     const double h[3] = {n.a, n.b, n.c};
     double tmin = -kCsgInf, tmax = kCsgInf;
@@ -279,8 +332,9 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
   return s;
 }
 
-__device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const double *q)
+__device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const double *q, const double *pl)
 {
+  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeOut, 0.0);
   if (n.kind == kCsgBox) return fmin(fmin(n.a - fabs(q[0]), n.b - fabs(q[1])), n.c - fabs(q[2]));
   if (n.kind == kCsgTube) {
     const double r = sqrt(dot2(q, q)), s = fmin(n.c - fabs(q[2]), n.b - r);
@@ -291,8 +345,9 @@ __device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const d
 }
 
 // a lower bound of the distance to the solid from a point outside it
-__device__ __forceinline__ double csg_safety_in_local(const CsgNode &n, const double *q)
+__device__ __forceinline__ double csg_safety_in_local(const CsgNode &n, const double *q, const double *pl)
 {
+  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeIn, 0.0);
   if (n.kind == kCsgBox) return fmax(fmax(fabs(q[0]) - n.a, fabs(q[1]) - n.b), fabs(q[2]) - n.c);
   if (n.kind == kCsgTube) {
     const double r = sqrt(dot2(q, q));
@@ -338,7 +393,7 @@ __device__ __forceinline__ bool csg_contains(const CsgView &g, int v, const doub
   if (csg_bbox_gap(n, p) > 0.0) return false;
   double q[3], e[3];
   csg_local(n, p, d, q, e);
-  return csg_contains_local(n, q, e, tol);
+  return csg_contains_local(n, q, e, tol, g.planes);
 }
 
 // the deepest touchable at or below v (which contains p) that contains p
@@ -387,13 +442,13 @@ __device__ __forceinline__ double csg_step(const CsgView &g, int v, const double
   double q[3], e[3];
   const CsgNode &n = g.node[v];
   csg_local(n, p, d, q, e);
-  double s = csg_dist_out_local(n, q, e);
+  double s = csg_dist_out_local(n, q, e, g.planes);
   hit = -1;
   auto child = [&](int c) {
     const double tb = csg_bbox_ray(g.node[c], p, d);
     if (!(tb < s && tb < limit)) return;
     csg_local(g.node[c], p, d, q, e);
-    const double t = csg_dist_in_local(g.node[c], q, e);
+    const double t = csg_dist_in_local(g.node[c], q, e, g.planes);
     if (t < s || (t == s && hit >= 0 && c < hit)) {
       s = t;
       hit = c;
@@ -427,13 +482,13 @@ __device__ __forceinline__ double csg_safety(const CsgView &g, int v, const doub
   double q[3];
   const CsgNode &n = g.node[v];
   csg_local_point(n, p, q);
-  double s = csg_safety_out_local(n, q);
+  double s = csg_safety_out_local(n, q, g.planes);
   auto child = [&](int c) {
     const CsgNode &m = g.node[c];
     const double gap = csg_bbox_gap(m, p);
     if (gap >= s) return;
     csg_local_point(m, p, q);
-    s = fmin(s, fmax(gap, csg_safety_in_local(m, q)));
+    s = fmin(s, fmax(gap, csg_safety_in_local(m, q, g.planes)));
   };
   if (n.gaxis >= 0) {
     // children farther than the safety along the axis cannot lower it

@@ -22,6 +22,8 @@ struct gx_geom {
   struct Solid {
     int kind;
     double p[3];
+    int p0, np;  // polyhedron: its planes in `planes`
+    double lo[3], hi[3]; // local bounding box
   };
   struct Lv {
     int solid, mat, scored;
@@ -33,6 +35,7 @@ struct gx_geom {
   std::vector<Solid> solids;
   std::vector<Lv> lvs;
   std::vector<Pv> pvs;
+  std::vector<double> planes; // polyhedra: unit outward normal and offset per plane
   // after gx_geom_close
   int world = -1, nscore = 0;
   std::vector<gx::CsgNode> nodes;
@@ -49,20 +52,6 @@ struct Flattener {
   std::vector<std::vector<int>> daughters; // placements per logical volume, in placement order
   int kcur = 0;
   bool err = false;
-
-  void bbox_half(const CsgNode &n, double h[3])
-  {
-    if (n.kind == kCsgBox) {
-      h[0] = n.a;
-      h[1] = n.b;
-      h[2] = n.c;
-    } else if (n.kind == kCsgTube) {
-      h[0] = h[1] = n.b;
-      h[2] = n.c;
-    } else {
-      h[0] = h[1] = h[2] = n.b;
-    }
-  }
 
   long count(int lv, int depth)
   {
@@ -90,6 +79,8 @@ struct Flattener {
       n.a = s.p[0];
       n.b = s.p[1];
       n.c = s.p[2];
+      n.p0 = s.p0;
+      n.np = s.np;
       std::memcpy(n.t, t, sizeof(n.t));
       std::memcpy(n.r, R, sizeof(n.r));
       n.rot = !(R[0] == 1.0 && R[1] == 0.0 && R[2] == 0.0 && R[3] == 0.0 && R[4] == 1.0 && R[5] == 0.0 &&
@@ -97,14 +88,13 @@ struct Flattener {
       n.mat = g.lvs[lv].mat;
       n.parent = parent;
       if (g.lvs[lv].scored) g.score[id] = g.nscore++;
-      double h[3];
-      bbox_half(n, h);
       for (int k = 0; k < 3; ++k) {
         n.lo[k] = kCsgInf;
         n.hi[k] = -kCsgInf;
       }
       for (int corner = 0; corner < 8; ++corner) {
-        const double x[3] = {(corner & 1) ? h[0] : -h[0], (corner & 2) ? h[1] : -h[1], (corner & 4) ? h[2] : -h[2]};
+        const double x[3] = {(corner & 1) ? s.hi[0] : s.lo[0], (corner & 2) ? s.hi[1] : s.lo[1],
+                             (corner & 4) ? s.hi[2] : s.lo[2]};
         for (int k = 0; k < 3; ++k) {
           const double y = R[3 * k] * x[0] + R[3 * k + 1] * x[1] + R[3 * k + 2] * x[2] + t[k];
           n.lo[k] = std::min(n.lo[k], y);
@@ -183,6 +173,59 @@ void build_grid(gx_geom &g, int v)
   }
 }
 
+// The bounding box of the convex polyhedron {x : n_k . x <= d_k} (unit
+// normals): the extent of its vertices, the points where three planes meet
+// inside all the others.  False when the planes bound no finite volume: no
+// vertex, or an edge direction +-(n_i x n_j) along which no plane closes it.
+bool poly_bbox(const double *pl, int np, double lo[3], double hi[3])
+{
+  int nv = 0;
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = kCsgInf;
+    hi[k] = -kCsgInf;
+  }
+  for (int i = 0; i < np; ++i)
+    for (int j = i + 1; j < np; ++j)
+      for (int k = j + 1; k < np; ++k) {
+        const double *a = pl + 4 * i, *b = pl + 4 * j, *c = pl + 4 * k;
+        const double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+        const double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+        const double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+        const double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+        if (std::fabs(det) < 1e-12) continue;
+        double x[3];
+        for (int m = 0; m < 3; ++m) x[m] = (a[3] * bc[m] + b[3] * ca[m] + c[3] * ab[m]) / det;
+        bool in = true;
+        for (int l = 0; l < np && in; ++l) {
+          const double *p = pl + 4 * l;
+          in = p[0] * x[0] + p[1] * x[1] + p[2] * x[2] - p[3] <= 1e-9 * (1.0 + std::fabs(p[3]));
+        }
+        if (!in) continue;
+        ++nv;
+        for (int m = 0; m < 3; ++m) {
+          lo[m] = std::min(lo[m], x[m]);
+          hi[m] = std::max(hi[m], x[m]);
+        }
+      }
+  if (nv == 0) return false;
+  for (int i = 0; i < np; ++i)
+    for (int j = i + 1; j < np; ++j) {
+      const double *a = pl + 4 * i, *b = pl + 4 * j;
+      const double v[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+      const double len = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      if (len < 1e-12) continue;
+      for (int sgn = -1; sgn <= 1; sgn += 2) {
+        bool open = true;
+        for (int l = 0; l < np && open; ++l) {
+          const double *p = pl + 4 * l;
+          open = sgn * (p[0] * v[0] + p[1] * v[1] + p[2] * v[2]) <= 1e-12 * len;
+        }
+        if (open) return false;
+      }
+    }
+  return true;
+}
+
 bool orthonormal(const double *R)
 {
   for (int i = 0; i < 3; ++i)
@@ -242,7 +285,16 @@ static int add_solid(gx_geom *g, int kind, double a, double b, double c, int *so
 {
   if (!g || !solid) return set_error(GX_ERR_ARG, "gx_geom: null argument");
   if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
-  g->solids.push_back({kind, {a, b, c}});
+  gx_geom::Solid s{kind, {a, b, c}, 0, 0, {0, 0, 0}, {0, 0, 0}};
+  // local bounding box half lengths: box (a, b, c), tube (b, b, c), sphere (b, b, b)
+  double h[3] = {a, b, c};
+  if (kind == kCsgTube) h[0] = b;
+  if (kind == kCsgSphere) h[0] = h[2] = b;
+  for (int k = 0; k < 3; ++k) {
+    s.lo[k] = -h[k];
+    s.hi[k] = h[k];
+  }
+  g->solids.push_back(s);
   *solid = (int)g->solids.size() - 1;
   return GX_OK;
 }
@@ -264,6 +316,29 @@ int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid)
 {
   if (!(rmin >= 0.0 && rmax > rmin)) return set_error(GX_ERR_ARG, "gx_geom_sphere: need 0 <= rmin < rmax");
   return add_solid(g, kCsgSphere, rmin, rmax, 0.0, solid);
+}
+
+int gx_geom_polyhedron(gx_geom *g, int nplanes, const double *planes, int *solid)
+{
+  if (!g || !solid || !planes) return set_error(GX_ERR_ARG, "gx_geom_polyhedron: null argument");
+  if (g->world >= 0) return set_error(GX_ERR_ARG, "gx_geom: the geometry is closed");
+  if (nplanes < 4 || nplanes > kCsgMaxPlanes)
+    return set_error(GX_ERR_ARG, "gx_geom_polyhedron: %d planes (4 to %d)", nplanes, kCsgMaxPlanes);
+  std::vector<double> pl(4 * nplanes);
+  for (int k = 0; k < nplanes; ++k) {
+    const double *p = planes + 4 * k;
+    const double len = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+    if (!(len > 0.0) || !std::isfinite(len) || !std::isfinite(p[3]))
+      return set_error(GX_ERR_ARG, "gx_geom_polyhedron: plane %d has no normal", k);
+    for (int m = 0; m < 4; ++m) pl[4 * k + m] = p[m] / len;
+  }
+  gx_geom::Solid s{kCsgPoly, {0, 0, 0}, (int)(g->planes.size() / 4), nplanes, {0, 0, 0}, {0, 0, 0}};
+  if (!poly_bbox(pl.data(), nplanes, s.lo, s.hi))
+    return set_error(GX_ERR_ARG, "gx_geom_polyhedron: the planes bound no finite volume");
+  g->planes.insert(g->planes.end(), pl.begin(), pl.end());
+  g->solids.push_back(s);
+  *solid = (int)g->solids.size() - 1;
+  return GX_OK;
 }
 
 int gx_geom_logical_volume(gx_geom *g, int solid, int material, int scored, int *lv)
@@ -348,6 +423,7 @@ int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g)
   const size_t nn = g->nodes.size();
   CsgNode *dn = nullptr;
   int *dk = nullptr, *ds = nullptr, *dsl = nullptr, *dc = nullptr;
+  double *dp = nullptr;
   auto upload = [&](int **dst, const std::vector<int> &src) {
     const size_t bytes = std::max<size_t>(src.size(), 1) * sizeof(int);
     cudaError_t r = cudaMalloc((void **)dst, bytes);
@@ -357,18 +433,22 @@ int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g)
   if ((e = cudaMalloc((void **)&dn, nn * sizeof(CsgNode))) != cudaSuccess ||
       (e = cudaMemcpy(dn, g->nodes.data(), nn * sizeof(CsgNode), cudaMemcpyHostToDevice)) != cudaSuccess ||
       (e = upload(&dk, g->kids)) != cudaSuccess || (e = upload(&ds, g->score)) != cudaSuccess ||
-      (e = upload(&dsl, g->slab)) != cudaSuccess || (e = upload(&dc, g->cand)) != cudaSuccess) {
-    for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc}) cudaFree(q);
+      (e = upload(&dsl, g->slab)) != cudaSuccess || (e = upload(&dc, g->cand)) != cudaSuccess ||
+      (e = cudaMalloc((void **)&dp, std::max<size_t>(g->planes.size(), 1) * sizeof(double))) != cudaSuccess ||
+      (!g->planes.empty() && (e = cudaMemcpy(dp, g->planes.data(), g->planes.size() * sizeof(double),
+                                             cudaMemcpyHostToDevice)) != cudaSuccess)) {
+    for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc, (void *)dp}) cudaFree(q);
     return cuda_error(e, "gx_ctx_load_geometry: upload");
   }
   // the previous tree (if any) stays allocated until the context goes: a
   // captured transport graph may still refer to it
-  for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc}) c->owned.push_back(q);
+  for (void *q : {(void *)dn, (void *)dk, (void *)ds, (void *)dsl, (void *)dc, (void *)dp}) c->owned.push_back(q);
   c->csg_node = dn;
   c->csg_kids = dk;
   c->csg_score = ds;
   c->csg_slab = dsl;
   c->csg_cand = dc;
+  c->csg_planes = dp;
   c->csg_n = (int)nn;
   c->csg_nscore = g->nscore;
   return GX_OK;
@@ -382,7 +462,7 @@ int gx_geom_probe(gx_ctx *ctx, int n, const double *d_pos, const double *d_dir, 
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c->csg_node) return set_error(GX_ERR_ARG, "gx_geom_probe: no geometry loaded (gx_ctx_load_geometry)");
   if (n == 0) return GX_OK;
-  CsgView v{c->csg_node, c->csg_kids, c->csg_slab, c->csg_cand};
+  CsgView v{c->csg_node, c->csg_kids, c->csg_slab, c->csg_cand, c->csg_planes};
   k_geom_probe<<<(n + 127) / 128, 128, 0, stream_of(s)>>>(v, n, d_pos, d_dir, d_limit, d_vol, d_snext, d_next,
                                                          d_safety);
   cudaError_t e = cudaGetLastError();

@@ -21,6 +21,7 @@ struct Ctx {
   // the CSG volume tree (gx_ctx_load_geometry): touchables, children, tally column of each
   CsgNode *csg_node = nullptr;
   int *csg_kids = nullptr, *csg_score = nullptr, *csg_slab = nullptr, *csg_cand = nullptr;
+  double *csg_planes = nullptr;
   int csg_n = 0, csg_nscore = 0;
 };
 

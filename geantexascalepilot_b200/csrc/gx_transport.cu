@@ -1890,7 +1890,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.a.pstep = d_pstep;
   if (cfg->geometry == 2) {
     // the kernels score per (event, touchable); folded into d_edep at the end
-    g.csg = CsgView{C->csg_node, C->csg_kids, C->csg_slab, C->csg_cand};
+    g.csg = CsgView{C->csg_node, C->csg_kids, C->csg_slab, C->csg_cand, C->csg_planes};
     g.nvol = C->csg_n;
     const long long nt = (long long)cfg->nevents * C->csg_n;
     if (nt > E->vtally_cap) {

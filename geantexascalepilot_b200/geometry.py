@@ -4,6 +4,8 @@ The classes take the calls a VecGeom detector construction makes, as the
 reference's does (source/Geant/proxy/test/BasicCpuTransport/
 ProxyDetectorConstruction.cpp:241-324): ``UnplacedBox`` / ``UnplacedTube`` /
 ``UnplacedSphere`` / ``UnplacedOrb``, ``LogicalVolume`` with
+``UnplacedTrd`` (and any convex polyhedron given by its planes,
+``ConvexPolyhedron``), ``LogicalVolume`` with
 ``SetMaterialPtr`` and ``PlaceDaughter(name, lv, Transformation3D)``, and a
 ``GeoManager`` with ``SetWorld`` and ``CloseGeometry``.  Closing gives a
 ``CsgGeometry``: the tree as flat arrays, which ``load(dm)`` builds through the
@@ -24,7 +26,7 @@ import numpy as np
 
 from ._lib import check, lib
 
-BOX, TUBE, SPHERE = 0, 1, 2
+BOX, TUBE, SPHERE, POLY = 0, 1, 2, 3
 MATERIALS = {"G4_Galactic": 0, "G4_Pb": 1, "G4_lAr": 2}
 
 
@@ -71,6 +73,31 @@ class UnplacedOrb(UnplacedSphere):
         """UnplacedOrb([name,] r)"""
         (r,) = _strip_name(args)
         super().__init__(0.0, r)
+
+
+class ConvexPolyhedron:
+    """{x : n_k . x <= d_k}: planes as rows (nx, ny, nz, d), outward normals
+    of any length (4 to 32 planes; they must bound a finite volume)"""
+    kind = POLY
+
+    def __init__(self, planes):
+        self.planes = np.asarray(planes, np.float64).reshape(-1, 4)
+        self.par = (0.0, 0.0, 0.0)
+
+
+class UnplacedTrd(ConvexPolyhedron):
+    def __init__(self, *args):
+        """UnplacedTrd([name,] x1, x2, y1, y2, z): half lengths x1, y1 at -z and
+        x2, y2 at +z, half length z along z"""
+        a = _strip_name(args)
+        if len(a) == 4:  # UnplacedTrd(x1, x2, y, z)
+            a = (a[0], a[1], a[2], a[2], a[3])
+        x1, x2, y1, y2, z = (float(v) for v in a)
+        kx, ky = (x2 - x1) / (2.0 * z), (y2 - y1) / (2.0 * z)
+        mx, my = 0.5 * (x1 + x2), 0.5 * (y1 + y2)
+        # x <= mx + kx z, -x <= mx + kx z, and the same in y; |z| <= z
+        super().__init__([[1.0, 0.0, -kx, mx], [-1.0, 0.0, -kx, mx], [0.0, 1.0, -ky, my], [0.0, -1.0, -ky, my],
+                          [0.0, 0.0, 1.0, z], [0.0, 0.0, -1.0, z]])
 
 
 def euler_zxz(phi, theta, psi):
@@ -155,9 +182,14 @@ class CsgGeometry:
     daughter logical volume, translation, rotation), the world's logical
     volume; the same arrays feed gx_geom_* and the oracle."""
 
-    def __init__(self, skind, spar, lv_solid, lv_mat, lv_scored, pv_mother, pv_lv, pv_t, pv_r, world, names=None):
+    def __init__(self, skind, spar, lv_solid, lv_mat, lv_scored, pv_mother, pv_lv, pv_t, pv_r, world, names=None,
+                 splane_off=None, splanes=None):
         self.skind = np.asarray(skind, np.int32)
         self.spar = np.asarray(spar, np.float64).reshape(-1, 3)
+        # polyhedra: the planes of solid s are splanes[splane_off[s]:splane_off[s + 1]]
+        self.splane_off = (np.zeros(len(self.skind) + 1, np.int32) if splane_off is None
+                           else np.asarray(splane_off, np.int32))
+        self.splanes = np.zeros((0, 4)) if splanes is None else np.asarray(splanes, np.float64).reshape(-1, 4)
         self.lv_solid = np.asarray(lv_solid, np.int32)
         self.lv_mat = np.asarray(lv_mat, np.int32)
         self.lv_scored = np.asarray(lv_scored, np.int32)
@@ -195,9 +227,15 @@ class CsgGeometry:
                 pv_lv.append(index[id(pv.logical)])
                 pv_t.append(pv.transformation.t)
                 pv_r.append(pv.transformation.r)
+        off, planes = [0], []
+        for s in solids:
+            if s.kind == POLY:
+                planes.extend(s.planes.tolist())
+            off.append(len(planes))
         return cls([s.kind for s in solids], [s.par for s in solids], [sindex[id(lv.solid)] for lv in lvs],
                    [lv.material for lv in lvs], [int(lv.scored) for lv in lvs], pv_mother, pv_lv,
-                   np.array(pv_t).reshape(-1, 3), np.array(pv_r).reshape(-1, 9), 0, [lv.name for lv in lvs])
+                   np.array(pv_t).reshape(-1, 3), np.array(pv_r).reshape(-1, 9), 0, [lv.name for lv in lvs],
+                   off, np.array(planes).reshape(-1, 4))
 
     # ------------------------------------------------------------ C ABI
     def build(self):
@@ -206,8 +244,12 @@ class CsgGeometry:
         check(lib.gx_geom_create(C.byref(h)))
         try:
             out = C.c_int()
-            for k, p in zip(self.skind, self.spar):
-                if k == BOX:
+            for s, (k, p) in enumerate(zip(self.skind, self.spar)):
+                if k == POLY:
+                    pl = np.ascontiguousarray(self.splanes[self.splane_off[s]:self.splane_off[s + 1]])
+                    check(lib.gx_geom_polyhedron(h, len(pl), pl.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 C.byref(out)))
+                elif k == BOX:
                     check(lib.gx_geom_box(h, p[0], p[1], p[2], C.byref(out)))
                 elif k == TUBE:
                     check(lib.gx_geom_tube(h, p[0], p[1], p[2], C.byref(out)))

@@ -191,6 +191,7 @@ int gx_helix_dostep(const double B[3], double kB2C, int n, const double *d_posx,
  *   new UnplacedBox(hx, hy, hz)             -> gx_geom_box
  *   new UnplacedTube(rmin, rmax, dz, 0, 2pi) -> gx_geom_tube
  *   new UnplacedSphere / UnplacedOrb (full)  -> gx_geom_sphere
+ *   new UnplacedTrd(x1, x2, y1, y2, z) etc.  -> gx_geom_polyhedron (its planes)
  *   new LogicalVolume(name, solid) + SetMaterialPtr -> gx_geom_logical_volume
  *   lv->PlaceDaughter(name, daughter, new Transformation3D(...))
  *                                            -> gx_geom_place_daughter
@@ -208,6 +209,12 @@ void gx_geom_destroy(gx_geom *g);
 int gx_geom_box(gx_geom *g, double hx, double hy, double hz, int *solid);
 int gx_geom_tube(gx_geom *g, double rmin, double rmax, double dz, int *solid);
 int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid);
+/* A convex polyhedron {x : n_k . x <= d_k, k < nplanes} (4 to 32 planes,
+ * planes[4k .. 4k+3] = outward normal n_k, any length, and offset d_k, in the
+ * same length scale): VecGeom's UnplacedTrd / UnplacedTrapezoid /
+ * UnplacedParallelepiped and the like are such intersections.  Rejected when
+ * the planes bound no finite volume. */
+int gx_geom_polyhedron(gx_geom *g, int nplanes, const double *planes, int *solid);
 int gx_geom_logical_volume(gx_geom *g, int solid, int material, int scored, int *lv);
 int gx_geom_place_daughter(gx_geom *g, int mother, int daughter, const double translation[3],
                            const double rotation[9], int *pv);

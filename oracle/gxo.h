@@ -165,7 +165,7 @@ void gxo_helix_batch(const double B[3], int n, const double *pos, const double *
 /* ---------------------------------------------------------- CSG geometry */
 /* gxo_geom.c: a volume tree of placed solids, flattened into touchables
  * (transport config geometry = 2). */
-enum { GXO_CSG_BOX = 0, GXO_CSG_TUBE = 1, GXO_CSG_SPHERE = 2 };
+enum { GXO_CSG_BOX = 0, GXO_CSG_TUBE = 1, GXO_CSG_SPHERE = 2, GXO_CSG_POLY = 3 };
 #define GXO_CSG_TOL 1e-9 /* surface tolerance, mm */
 typedef struct {
   int kind;             /* GXO_CSG_* */
@@ -174,18 +174,22 @@ typedef struct {
   int rot;              /* 0: R is the identity */
   double lo[3], hi[3];  /* global bounding box, padded */
   int mat, parent, kid0, nkid, score, lv;
+  int p0, np;           /* polyhedron: its planes in the plane table */
 } gxo_csg_node_t;
 typedef struct {
   int n, nscore;        /* touchables; scored ones (numbered depth-first) */
   gxo_csg_node_t *node; /* node 0 is the world */
   int *kids;
+  double *planes;       /* polyhedra: unit outward normal and offset per plane */
 } gxo_csg_t;
-/* solids: kind and 3 parameters each; logical volumes: solid, material,
+/* solids: kind and 3 parameters each (polyhedra: planes splanes[4 off[s] ..
+ * 4 off[s+1]), normal and offset each); logical volumes: solid, material,
  * scored flag; placements: mother and daughter logical volume, translation (3)
  * and rotation (9, row-major; x_mother = R x_daughter + t).  NULL on error. */
-gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, int nlv, const int *lv_solid,
-                         const int *lv_mat, const int *lv_scored, int npv, const int *pv_mother, const int *pv_lv,
-                         const double *pv_t, const double *pv_r, int world);
+gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const int *splane_off,
+                         const double *splanes, int nlv, const int *lv_solid, const int *lv_mat, const int *lv_scored,
+                         int npv, const int *pv_mother, const int *pv_lv, const double *pv_t, const double *pv_r,
+                         int world);
 void gxo_csg_free(gxo_csg_t *g);
 int gxo_csg_contains(const gxo_csg_t *g, int v, const double *p, const double *d, double tol);
 /* from touchable v (-1 or 0: the world) up until a touchable contains p, then down */

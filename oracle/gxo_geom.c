@@ -24,8 +24,10 @@
  *   - safety: to the current solid's surface and to each child (the larger of
  *     the distance to its bounding box and the solid's own lower bound).
  * Solids: box (half lengths), tube (rmin, rmax, half length in z; full phi),
- * sphere (rmin, rmax).  Quadratic roots are taken in the cancellation-free
- * form (near root c / (-b + sqrt(D)), far root -c / (b + sqrt(D))). */
+ * sphere (rmin, rmax), convex polyhedron (intersection of half-spaces
+ * n.x <= d; the ray clipped against each plane).  Quadratic roots are taken in
+ * the cancellation-free form (near root c / (-b + sqrt(D)), far root
+ * -c / (b + sqrt(D))). */
 #include "gxo.h"
 
 #include <math.h>
@@ -45,6 +47,8 @@ typedef struct {
   int nsolid, nlv, npv;
   const int *skind;
   const double *spar;
+  const int *splane_off;
+  double *slo, *shi; /* local bounding box per solid */
   const int *lv_solid, *lv_mat, *lv_scored;
   const int *pv_mother, *pv_lv;
   const double *pv_t, *pv_r;
@@ -52,18 +56,57 @@ typedef struct {
   int kcur, scur, err;
 } build_t;
 
-static void bbox_half(int kind, const double *par, double h[3])
+/* The bounding box of the convex polyhedron {x : n_k . x <= d_k} (unit
+ * normals): the extent of the points where three planes meet inside all the
+ * others.  0 when the planes bound no finite volume (no such point, or an
+ * edge direction +-(n_i x n_j) that no plane closes). */
+static int poly_bbox(const double *pl, int np, double lo[3], double hi[3])
 {
-  if (kind == GXO_CSG_BOX) {
-    h[0] = par[0];
-    h[1] = par[1];
-    h[2] = par[2];
-  } else if (kind == GXO_CSG_TUBE) {
-    h[0] = h[1] = par[1];
-    h[2] = par[2];
-  } else {
-    h[0] = h[1] = h[2] = par[1];
+  int nv = 0;
+  for (int k = 0; k < 3; ++k) {
+    lo[k] = CSG_INF;
+    hi[k] = -CSG_INF;
   }
+  for (int i = 0; i < np; ++i)
+    for (int j = i + 1; j < np; ++j)
+      for (int k = j + 1; k < np; ++k) {
+        const double *a = pl + 4 * i, *b = pl + 4 * j, *c = pl + 4 * k;
+        double bc[3] = {b[1] * c[2] - b[2] * c[1], b[2] * c[0] - b[0] * c[2], b[0] * c[1] - b[1] * c[0]};
+        double ca[3] = {c[1] * a[2] - c[2] * a[1], c[2] * a[0] - c[0] * a[2], c[0] * a[1] - c[1] * a[0]};
+        double ab[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+        double det = a[0] * bc[0] + a[1] * bc[1] + a[2] * bc[2];
+        if (fabs(det) < 1e-12) continue;
+        double x[3];
+        for (int m = 0; m < 3; ++m) x[m] = (a[3] * bc[m] + b[3] * ca[m] + c[3] * ab[m]) / det;
+        int in = 1;
+        for (int l = 0; l < np && in; ++l) {
+          const double *p = pl + 4 * l;
+          in = p[0] * x[0] + p[1] * x[1] + p[2] * x[2] - p[3] <= 1e-9 * (1.0 + fabs(p[3]));
+        }
+        if (!in) continue;
+        ++nv;
+        for (int m = 0; m < 3; ++m) {
+          lo[m] = dmin(lo[m], x[m]);
+          hi[m] = dmax(hi[m], x[m]);
+        }
+      }
+  if (nv == 0) return 0;
+  for (int i = 0; i < np; ++i)
+    for (int j = i + 1; j < np; ++j) {
+      const double *a = pl + 4 * i, *b = pl + 4 * j;
+      double v[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+      double len = sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+      if (len < 1e-12) continue;
+      for (int sgn = -1; sgn <= 1; sgn += 2) {
+        int open = 1;
+        for (int l = 0; l < np && open; ++l) {
+          const double *p = pl + 4 * l;
+          open = sgn * (p[0] * v[0] + p[1] * v[1] + p[2] * v[2]) <= 1e-12 * len;
+        }
+        if (open) return 0;
+      }
+    }
+  return 1;
 }
 
 static int visit(build_t *b, int lv, int parent, const double R[9], const double t[3], int depth)
@@ -80,6 +123,8 @@ static int visit(build_t *b, int lv, int parent, const double R[9], const double
   n->a = b->spar[3 * s];
   n->b = b->spar[3 * s + 1];
   n->c = b->spar[3 * s + 2];
+  n->p0 = b->splane_off ? b->splane_off[s] : 0;
+  n->np = (n->kind == GXO_CSG_POLY) ? b->splane_off[s + 1] - b->splane_off[s] : 0;
   memcpy(n->t, t, sizeof(n->t));
   memcpy(n->r, R, sizeof(n->r));
   n->rot = !(R[0] == 1.0 && R[1] == 0.0 && R[2] == 0.0 && R[3] == 0.0 && R[4] == 1.0 && R[5] == 0.0 &&
@@ -89,14 +134,13 @@ static int visit(build_t *b, int lv, int parent, const double R[9], const double
   n->lv = lv;
   n->score = b->lv_scored[lv] ? g->nscore++ : -1;
   /* global bounding box: the local one's eight corners */
-  double h[3];
-  bbox_half(n->kind, &n->a, h);
+  const double *slo = b->slo + 3 * s, *shi = b->shi + 3 * s;
   for (int k = 0; k < 3; ++k) {
     n->lo[k] = CSG_INF;
     n->hi[k] = -CSG_INF;
   }
   for (int corner = 0; corner < 8; ++corner) {
-    double x[3] = {(corner & 1) ? h[0] : -h[0], (corner & 2) ? h[1] : -h[1], (corner & 4) ? h[2] : -h[2]};
+    double x[3] = {(corner & 1) ? shi[0] : slo[0], (corner & 2) ? shi[1] : slo[1], (corner & 4) ? shi[2] : slo[2]};
     for (int k = 0; k < 3; ++k) {
       double y = R[3 * k] * x[0] + R[3 * k + 1] * x[1] + R[3 * k + 2] * x[2] + t[k];
       n->lo[k] = dmin(n->lo[k], y);
@@ -145,22 +189,52 @@ static long count_nodes(const build_t *b, int lv, int depth)
   return n;
 }
 
-gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, int nlv, const int *lv_solid,
-                         const int *lv_mat, const int *lv_scored, int npv, const int *pv_mother, const int *pv_lv,
-                         const double *pv_t, const double *pv_r, int world)
+gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const int *splane_off,
+                         const double *splanes, int nlv, const int *lv_solid, const int *lv_mat, const int *lv_scored,
+                         int npv, const int *pv_mother, const int *pv_lv, const double *pv_t, const double *pv_r,
+                         int world)
 {
   if (world < 0 || world >= nlv) return NULL;
-  build_t b = {nsolid, nlv, npv, skind, spar, lv_solid, lv_mat, lv_scored, pv_mother, pv_lv, pv_t, pv_r,
-               NULL, 0, 0, 0};
+  build_t b = {nsolid, nlv, npv, skind, spar, splane_off, NULL, NULL, lv_solid, lv_mat, lv_scored, pv_mother, pv_lv,
+               pv_t, pv_r, NULL, 0, 0, 0};
   long total = count_nodes(&b, world, 0);
   if (total < 0) return NULL;
   gxo_csg_t *g = (gxo_csg_t *)calloc(1, sizeof(gxo_csg_t));
+  /* solids' local bounding boxes; polyhedra's planes normalised */
+  int nplanes = splane_off ? splane_off[nsolid] : 0;
+  g->planes = (double *)calloc((size_t)(4 * nplanes + 4), sizeof(double));
+  b.slo = (double *)calloc((size_t)(3 * nsolid + 3), sizeof(double));
+  b.shi = (double *)calloc((size_t)(3 * nsolid + 3), sizeof(double));
+  int bad = 0;
+  for (int s = 0; s < nsolid && !bad; ++s) {
+    const double *p = spar + 3 * s;
+    double *lo = b.slo + 3 * s, *hi = b.shi + 3 * s;
+    if (skind[s] == GXO_CSG_POLY) {
+      int p0 = splane_off[s], np = splane_off[s + 1] - p0;
+      for (int k = p0; k < p0 + np; ++k) {
+        const double *q = splanes + 4 * k;
+        double len = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
+        for (int m = 0; m < 4; ++m) g->planes[4 * k + m] = q[m] / len;
+      }
+      bad = np < 4 || !poly_bbox(g->planes + 4 * p0, np, lo, hi);
+      continue;
+    }
+    double h[3] = {p[0], p[1], p[2]};
+    if (skind[s] == GXO_CSG_TUBE) h[0] = p[1];
+    if (skind[s] == GXO_CSG_SPHERE) h[0] = h[2] = p[1];
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = -h[k];
+      hi[k] = h[k];
+    }
+  }
   g->node = (gxo_csg_node_t *)calloc((size_t)total, sizeof(gxo_csg_node_t));
   g->kids = (int *)calloc((size_t)total, sizeof(int));
   b.g = g;
   const double I[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1}, z[3] = {0, 0, 0};
-  visit(&b, world, -1, I, z, 0);
-  if (b.err) {
+  if (!bad) visit(&b, world, -1, I, z, 0);
+  free(b.slo);
+  free(b.shi);
+  if (b.err || bad) {
     gxo_csg_free(g);
     return NULL;
   }
@@ -172,6 +246,7 @@ void gxo_csg_free(gxo_csg_t *g)
   if (!g) return;
   free(g->node);
   free(g->kids);
+  free(g->planes);
   free(g);
 }
 
@@ -193,8 +268,24 @@ static void to_local(const gxo_csg_node_t *n, const double *p, const double *d, 
 }
 
 /* inside, or on the surface and not moving out through it */
-static int contains_local(const gxo_csg_node_t *n, const double *q, const double *e, double tol)
+/* n.q - d and n.e of plane k */
+static void plane_at(const double *pl, int k, const double *q, const double *e, double *h, double *ne)
 {
+  const double *p = pl + 4 * k;
+  *h = p[0] * q[0] + p[1] * q[1] + p[2] * q[2] - p[3];
+  *ne = p[0] * e[0] + p[1] * e[1] + p[2] * e[2];
+}
+
+static int contains_local(const gxo_csg_node_t *n, const double *q, const double *e, double tol, const double *pl)
+{
+  if (n->kind == GXO_CSG_POLY) {
+    for (int k = n->p0; k < n->p0 + n->np; ++k) {
+      double h, ne;
+      plane_at(pl, k, q, e, &h, &ne);
+      if (h > tol || (h >= -tol && ne > 0.0)) return 0;
+    }
+    return 1;
+  }
   if (n->kind == GXO_CSG_BOX) {
     const double h[3] = {n->a, n->b, n->c};
     for (int k = 0; k < 3; ++k) {
@@ -233,9 +324,17 @@ static double far_root(double a, double b, double c, double sq) { return b > 0.0
 static double near_root(double a, double b, double c, double sq) { return b < 0.0 ? c / (sq - b) : -(b + sq) / a; }
 
 /* distance to leave the solid from a point inside (or on its surface) */
-static double dist_out_local(const gxo_csg_node_t *n, const double *q, const double *e)
+static double dist_out_local(const gxo_csg_node_t *n, const double *q, const double *e, const double *pl)
 {
   double s = CSG_INF;
+  if (n->kind == GXO_CSG_POLY) {
+    for (int k = n->p0; k < n->p0 + n->np; ++k) {
+      double h, ne;
+      plane_at(pl, k, q, e, &h, &ne);
+      if (ne > 0.0) s = dmin(s, -h / ne);
+    }
+    return s < 0.0 ? 0.0 : s;
+  }
   if (n->kind == GXO_CSG_BOX) {
     const double h[3] = {n->a, n->b, n->c};
     for (int k = 0; k < 3; ++k) {
@@ -277,8 +376,27 @@ static double dist_out_local(const gxo_csg_node_t *n, const double *q, const dou
 }
 
 /* distance to enter the solid from a point outside it; CSG_INF if missed */
-static double dist_in_local(const gxo_csg_node_t *n, const double *q, const double *e, double tol)
+static double dist_in_local(const gxo_csg_node_t *n, const double *q, const double *e, double tol,
+                            const double *pl)
 {
+  if (n->kind == GXO_CSG_POLY) { /* the ray clipped against every plane */
+    double tmin = -CSG_INF, tmax = CSG_INF;
+    for (int k = n->p0; k < n->p0 + n->np; ++k) {
+      double h, ne;
+      plane_at(pl, k, q, e, &h, &ne);
+      if (ne == 0.0) {
+        if (h > 0.0) return CSG_INF;
+        continue;
+      }
+      double t = -h / ne;
+      if (ne < 0.0)
+        tmin = dmax(tmin, t);
+      else
+        tmax = dmin(tmax, t);
+    }
+    if (!(tmax > tmin) || tmax <= tol) return CSG_INF;
+    return tmin < 0.0 ? 0.0 : tmin;
+  }
   if (n->kind == GXO_CSG_BOX) {
     const double h[3] = {n->a, n->b, n->c};
     double tmin = -CSG_INF, tmax = CSG_INF;
@@ -345,8 +463,16 @@ static double dist_in_local(const gxo_csg_node_t *n, const double *q, const doub
   return s;
 }
 
-static double safety_out_local(const gxo_csg_node_t *n, const double *q)
+static double safety_out_local(const gxo_csg_node_t *n, const double *q, const double *pl)
 {
+  if (n->kind == GXO_CSG_POLY) {
+    double s = CSG_INF;
+    for (int k = n->p0; k < n->p0 + n->np; ++k) {
+      const double *p = pl + 4 * k;
+      s = dmin(s, -(p[0] * q[0] + p[1] * q[1] + p[2] * q[2] - p[3]));
+    }
+    return s;
+  }
   if (n->kind == GXO_CSG_BOX)
     return dmin(dmin(n->a - fabs(q[0]), n->b - fabs(q[1])), n->c - fabs(q[2]));
   if (n->kind == GXO_CSG_TUBE) {
@@ -359,8 +485,16 @@ static double safety_out_local(const gxo_csg_node_t *n, const double *q)
 }
 
 /* a lower bound of the distance to the solid from a point outside it */
-static double safety_in_local(const gxo_csg_node_t *n, const double *q)
+static double safety_in_local(const gxo_csg_node_t *n, const double *q, const double *pl)
 {
+  if (n->kind == GXO_CSG_POLY) {
+    double s = -CSG_INF;
+    for (int k = n->p0; k < n->p0 + n->np; ++k) {
+      const double *p = pl + 4 * k;
+      s = dmax(s, p[0] * q[0] + p[1] * q[1] + p[2] * q[2] - p[3]);
+    }
+    return s;
+  }
   if (n->kind == GXO_CSG_BOX)
     return dmax(dmax(fabs(q[0]) - n->a, fabs(q[1]) - n->b), fabs(q[2]) - n->c);
   if (n->kind == GXO_CSG_TUBE) {
@@ -406,7 +540,7 @@ int gxo_csg_contains(const gxo_csg_t *g, int v, const double *p, const double *d
   if (bbox_gap(n, p) > 0.0) return 0;
   double q[3], e[3];
   to_local(n, p, d, q, e);
-  return contains_local(n, q, e, tol);
+  return contains_local(n, q, e, tol, g->planes);
 }
 
 /* the deepest touchable at or below v (which contains p) containing p */
@@ -440,7 +574,7 @@ double gxo_csg_step(const gxo_csg_t *g, int v, const double *p, const double *d,
   const gxo_csg_node_t *n = &g->node[v];
   double q[3], e[3];
   to_local(n, p, d, q, e);
-  double s = dist_out_local(n, q, e);
+  double s = dist_out_local(n, q, e, g->planes);
   *hit = -1;
   for (int k = 0; k < n->nkid; ++k) {
     int c = g->kids[n->kid0 + k];
@@ -448,7 +582,7 @@ double gxo_csg_step(const gxo_csg_t *g, int v, const double *p, const double *d,
     double tb = bbox_ray(m, p, d);
     if (!(tb < s && tb < limit)) continue;
     to_local(m, p, d, q, e);
-    double t = dist_in_local(m, q, e, GXO_CSG_TOL);
+    double t = dist_in_local(m, q, e, GXO_CSG_TOL, g->planes);
     if (t < s) {
       s = t;
       *hit = c;
@@ -463,13 +597,13 @@ double gxo_csg_safety(const gxo_csg_t *g, int v, const double *p)
   double q[3], e[3];
   const double zero[3] = {0, 0, 0};
   to_local(n, p, zero, q, e);
-  double s = safety_out_local(n, q);
+  double s = safety_out_local(n, q, g->planes);
   for (int k = 0; k < n->nkid; ++k) {
     const gxo_csg_node_t *m = &g->node[g->kids[n->kid0 + k]];
     double gap = bbox_gap(m, p);
     if (gap >= s) continue;
     to_local(m, p, zero, q, e);
-    s = dmin(s, dmax(gap, safety_in_local(m, q)));
+    s = dmin(s, dmax(gap, safety_in_local(m, q, g->planes)));
   }
   return s < 0.0 ? 0.0 : s;
 }

@@ -237,15 +237,15 @@ class Oracle:
         CsgGeometry; the handle goes into Config.csg"""
         f = self.lib.gxo_csg_build
         f.restype = C.c_void_p
-        f.argtypes = [I, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p,
-                      C.c_void_p, C.c_void_p, I]
-        arrs = [np.ascontiguousarray(a) for a in (geo.skind, geo.spar, geo.lv_solid, geo.lv_mat, geo.lv_scored,
-                                                   geo.pv_mother, geo.pv_lv, geo.pv_t, geo.pv_r)]
+        f.argtypes = [I, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, I, C.c_void_p, C.c_void_p, C.c_void_p, I,
+                      C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, I]
+        arrs = [np.ascontiguousarray(a) for a in (geo.skind, geo.spar, geo.splane_off, geo.splanes, geo.lv_solid,
+                                                   geo.lv_mat, geo.lv_scored, geo.pv_mother, geo.pv_lv, geo.pv_t,
+                                                   geo.pv_r)]
         self._keep = arrs
         v = [a.ctypes.data_as(C.c_void_p) for a in arrs]
-        h = f(len(geo.skind), v[0], v[1], len(geo.lv_solid), v[2], v[3], v[4], len(geo.pv_mother), v[5], v[6], v[7],
-              v[8], geo.world)
-        assert h
+        h = f(len(geo.skind), v[0], v[1], v[2], v[3], len(geo.lv_solid), v[4], v[5], v[6], len(geo.pv_mother), v[7],
+              v[8], v[9], v[10], geo.world)
         return h
 
     def csg_free(self, h):

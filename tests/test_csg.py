@@ -12,8 +12,16 @@ import pytest
 from oracle_ctypes import oracle_config
 
 
+def hex_prism(apothem, half_z):
+    """a hexagonal prism as a convex polyhedron (8 planes)"""
+    from geantexascalepilot_b200 import geometry as G
+    planes = [[math.cos(k * math.pi / 3), math.sin(k * math.pi / 3), 0.0, apothem] for k in range(6)]
+    return G.ConvexPolyhedron(planes + [[0, 0, 2.0, 2.0 * half_z], [0, 0, -1.0, half_z]])
+
+
 def mixed_geometry():
-    """boxes, tubes and spheres, rotated and nested, in a Galactic world"""
+    """boxes, tubes, spheres, trapezoids and a hexagonal prism, rotated and
+    nested, in a Galactic world"""
     from geantexascalepilot_b200 import geometry as G
     world = G.LogicalVolume("world", G.UnplacedBox(600.0, 600.0, 600.0))
     tube = G.LogicalVolume("tube", G.UnplacedTube(50.0, 150.0, 100.0))
@@ -31,8 +39,20 @@ def mixed_geometry():
     rod = G.LogicalVolume("rod", G.UnplacedTube(0.0, 8.0, 30.0))
     rod.SetMaterialPtr("G4_lAr")
     rod.SetScored()
+    wedge = G.LogicalVolume("wedge", G.UnplacedTrd(3.0, 8.0, 4.0, 6.0, 7.0))
+    wedge.SetMaterialPtr("G4_Pb")
+    wedge.SetScored()
+    trd = G.LogicalVolume("trd", G.UnplacedTrd("trd", 20.0, 40.0, 15.0, 30.0, 25.0))
+    trd.SetMaterialPtr("G4_Pb")
+    trd.SetScored()
+    hexa = G.LogicalVolume("hex", hex_prism(30.0, 40.0))
+    hexa.SetMaterialPtr("G4_lAr")
+    hexa.SetScored()
     box.PlaceDaughter("orb", orb, G.Transformation3D(5.0, -10.0, 20.0))
     box.PlaceDaughter("rod", rod, G.Transformation3D(-12.0, 15.0, -10.0, 0.0, 90.0, 0.0))
+    box.PlaceDaughter("wedge", wedge, G.Transformation3D(15.0, 20.0, -30.0, 10.0, 0.0, 0.0))
+    world.PlaceDaughter("trd", trd, G.Transformation3D(250.0, 200.0, -200.0, 20.0, 30.0, 40.0))
+    world.PlaceDaughter("hex", hexa, G.Transformation3D(200.0, -250.0, 250.0, 0.0, 35.0, 10.0))
     world.PlaceDaughter("tube", tube, G.Transformation3D(100.0, -50.0, 20.0, 30.0, 40.0, 0.0))
     world.PlaceDaughter("shell", shell, G.Transformation3D(-250.0, 150.0, 0.0))
     world.PlaceDaughter("box_a", box, G.Transformation3D(0.0, 350.0, -100.0, 0.0, 90.0, 45.0))
@@ -61,9 +81,10 @@ def crowded_geometry():
         if k == 20:
             world.PlaceDaughter("holder", holder, G.Transformation3D(x, y, z, 15.0, 25.0, 35.0))
             continue
-        kind = k % 3
+        kind = k % 4
         solid = (G.UnplacedBox(12.0, 40.0, 30.0) if kind == 0 else
-                 G.UnplacedTube(4.0, 14.0, 40.0) if kind == 1 else G.UnplacedSphere(5.0, 14.0))
+                 G.UnplacedTube(4.0, 14.0, 40.0) if kind == 1 else
+                 G.UnplacedSphere(5.0, 14.0) if kind == 2 else G.UnplacedTrd(6.0, 14.0, 20.0, 30.0, 25.0))
         lv = G.LogicalVolume("s%d" % k, solid)
         lv.SetMaterialPtr(1 + k % 2)
         lv.SetScored()
@@ -87,6 +108,10 @@ class Tree:
         q = R.T @ (x - np.array(nd["translation"]))
         s = geo.lv_solid[nd["lv"]]
         kind, (a, b, c) = geo.skind[s], geo.spar[s]
+        if kind == 3:
+            pl = geo.splanes[geo.splane_off[s]:geo.splane_off[s + 1]]
+            n = pl[:, :3] / np.linalg.norm(pl[:, :3], axis=1, keepdims=True)
+            return bool(np.all(n @ q < pl[:, 3] / np.linalg.norm(pl[:, :3], axis=1)))
         if kind == 0:
             return abs(q[0]) < a and abs(q[1]) < b and abs(q[2]) < c
         if kind == 1:
@@ -122,8 +147,9 @@ def test_oracle_navigation_against_point_in_solid(oracle):
     geo = mixed_geometry()
     h = oracle.csg_build(geo)
     tree = Tree(oracle, h)
-    assert tree.n == 1 + 1 + 1 + 2 * 3
-    p, d = _rays(300, 11, [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300)])
+    assert tree.n == 1 + 1 + 1 + 2 * 4 + 2
+    p, d = _rays(400, 11, [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300), (250, 200, -200),
+                           (200, -250, 250)])
     vol, snext, nxt, saf = oracle.csg_probe(h, p, d)
     rng = np.random.default_rng(5)
     checked_hits = 0
@@ -242,5 +268,28 @@ def test_library_builder_rejects_bad_trees():
     lib.gx_geom_destroy(h)
     with pytest.raises(ValueError):
         G.UnplacedTube(0.0, 1.0, 1.0, 0.0, 1.0)
+    # polyhedra whose planes bound no finite volume: a slab open along z, a
+    # pyramid without a base, contradictory planes
+    open_prism = [[1, 0, 0, 1], [-1, 0, 0, 1], [0, 1, 0, 1], [0, -1, 0, 1]]
+    pyramid = [[1, 0, 1, 0], [-1, 0, 1, 0], [0, 1, 1, 0], [0, -1, 1, 0]]
+    empty = [[1, 0, 0, -1], [-1, 0, 0, -1], [0, 1, 0, 1], [0, -1, 0, 1], [0, 0, 1, 1], [0, 0, -1, 1]]
+    for planes in (open_prism, pyramid, empty):
+        h = C.c_void_p()
+        assert lib.gx_geom_create(C.byref(h)) == 0
+        arr = (C.c_double * (4 * len(planes)))(*[x for p in planes for x in p])
+        assert lib.gx_geom_polyhedron(h, len(planes), arr, C.byref(s)) != 0
+        assert b"finite volume" in lib.gx_last_error_string() or b"planes" in lib.gx_last_error_string()
+        lib.gx_geom_destroy(h)
     with pytest.raises(GxError):
         G.CsgGeometry([0], [[1, 1, 1]], [0], [9], [0], [], [], [], [], 0).build()
+
+
+def test_oracle_rejects_unbounded_polyhedra(oracle):
+    from geantexascalepilot_b200 import geometry as G
+    for planes in ([[1, 0, 0, 1], [-1, 0, 0, 1], [0, 1, 0, 1], [0, -1, 0, 1]],
+                   [[1, 0, 1, 0], [-1, 0, 1, 0], [0, 1, 1, 0], [0, -1, 1, 0]]):
+        world = G.LogicalVolume("w", G.UnplacedBox(10.0, 10.0, 10.0))
+        world.PlaceDaughter("p", G.LogicalVolume("p", G.ConvexPolyhedron(planes)))
+        gm = G.GeoManager()
+        gm.SetWorld(world)
+        assert not oracle.csg_build(gm.CloseGeometry())
