@@ -349,7 +349,11 @@ def main():
     stp = one(1, 1, profile=1)
     k = int(np.argmax(stp["transport_ms"]))
     launches_k = max(1, stp["step_launches"][k])
-    nbytes = (stp["transport_read"][k] + stp["transport_written"][k]) * stp["bytes_per_track"]
+    # algorithmic bytes: one read and one write of the track record per step
+    # (a step reads and writes the state once); the kernel keeps a track in
+    # registers across steps, so the records it actually moves are fewer
+    nbytes = stp["transport_steps"][k] * 2 * stp["bytes_per_track"]
+    moved = (stp["transport_read"][k] + stp["transport_written"][k]) * stp["bytes_per_track"]
     achieved = nbytes / (stp["transport_ms"][k] / 1e3) / 1e9
     peaks = {}
     try:
@@ -373,6 +377,9 @@ def main():
                        "traffic": traffic, "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "algorithmic_bytes_per_launch": nbytes / launches_k,
+                       "steps_per_launch": stp["transport_steps"][k] / launches_k,
+                       "record_bytes_moved_per_launch": moved / launches_k,
+                       "record_bytes_moved_gbs": moved / (stp["transport_ms"][k] / 1e3) / 1e9,
                        "avg_launch_ms": stp["transport_ms"][k] / launches_k,
                        "share_of_step_kernel_time": stp["transport_ms"][k] / max(1e-9, sum(stp["step_ms"])),
                        "records_per_launch": (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k}

@@ -51,7 +51,8 @@ class TransportStats(C.Structure):
                 ("n_annih", LL), ("errors", LL), ("escaped", D), ("iterations", LL), ("peak_in_flight", LL),
                 ("kernel_ms", D), ("step_ms", D * 3), ("step_launches", LL * 3), ("tracks_read", LL * 3),
                 ("tracks_written", LL * 3), ("bytes_per_track", LL), ("transport_ms", D * 3),
-                ("transport_read", LL * 3), ("transport_written", LL * 3), ("transport_queued", LL * 3)]
+                ("transport_read", LL * 3), ("transport_written", LL * 3), ("transport_queued", LL * 3),
+                ("transport_steps", LL * 3)]
 
     def as_dict(self):
         return {"steps": self.steps, "substeps": self.substeps, "tracks": self.tracks,
@@ -63,7 +64,7 @@ class TransportStats(C.Structure):
                 "tracks_read": list(self.tracks_read), "tracks_written": list(self.tracks_written),
                 "bytes_per_track": self.bytes_per_track, "transport_ms": list(self.transport_ms),
                 "transport_read": list(self.transport_read), "transport_written": list(self.transport_written),
-                "transport_queued": list(self.transport_queued)}
+                "transport_queued": list(self.transport_queued), "transport_steps": list(self.transport_steps)}
 
 
 class GunParams(C.Structure):

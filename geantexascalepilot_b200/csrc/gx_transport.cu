@@ -45,13 +45,14 @@ struct Geom {
   CsgView csg; // geometry 2: the context's volume tree
 };
 
-constexpr int kNStat = 25;
+constexpr int kNStat = 28;
 // S_READ/S_WRITE: track records read and written by all step kernels of a
 // type; S_TREAD/S_TWRITE: by its transport kernel alone; S_TQUEUE: of those
-// writes, the records put in an interaction buffer.
+// writes, the records put in an interaction buffer; S_TSTEP: steps completed
+// in the transport kernel of a type.
 enum { S_STEPS, S_SUBSTEPS, S_TRACKS, S_SEC0, S_SEC1, S_SEC2, S_PAIR, S_ANNIH, S_ERR, S_OVERFLOW,
        S_READ0, S_READ1, S_READ2, S_WRITE0, S_WRITE1, S_WRITE2, S_TREAD0, S_TREAD1, S_TREAD2,
-       S_TWRITE0, S_TWRITE1, S_TWRITE2, S_TQUEUE0, S_TQUEUE1, S_TQUEUE2 };
+       S_TWRITE0, S_TWRITE1, S_TWRITE2, S_TQUEUE0, S_TQUEUE1, S_TQUEUE2, S_TSTEP0, S_TSTEP1, S_TSTEP2 };
 
 struct Ctl {
   int parity;
@@ -1126,12 +1127,15 @@ __device__ __forceinline__ void tally_begin(Local &L, const Geom &g, double *ede
   for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
 }
 
+// steps_slot >= 0: the stat that also receives this kernel's step count
 __device__ __forceinline__ void tally_end(Local &L, Ctl *ctl, double *edep, double *sm_edep,
-                                          unsigned long long *sm_stat, double *sm_esc, int *sm_err)
+                                          unsigned long long *sm_stat, double *sm_esc, int *sm_err,
+                                          int steps_slot = -1)
 {
 #pragma unroll
   for (int k = 0; k < kNStat; ++k)
     if (L.st[k]) atomicAdd(&sm_stat[k], (unsigned long long)L.st[k]);
+  if (steps_slot >= 0 && L.st[S_STEPS]) atomicAdd(&sm_stat[steps_slot], (unsigned long long)L.st[S_STEPS]);
   if (L.retired != 0.0) atomicAdd(&sm_esc[1], L.retired);
   if (L.err) atomicOr(sm_err, L.err);
   __syncthreads();
@@ -1382,7 +1386,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
     }
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
-  tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
+  tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err, S_TSTEP0 + PT);
 }
 
 // Post-step interaction of process PROC for the buffered tracks of type PT:
@@ -2068,6 +2072,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       stats->transport_read[q] = (long long)c.stat[S_TREAD0 + q];
       stats->transport_written[q] = (long long)c.stat[S_TWRITE0 + q];
       stats->transport_queued[q] = (long long)c.stat[S_TQUEUE0 + q];
+      stats->transport_steps[q] = (long long)c.stat[S_TSTEP0 + q];
     }
     stats->bytes_per_track = (long long)(3 * sizeof(double) + 8 * sizeof(R) + 6 * sizeof(uint32_t) +
                                          3 * sizeof(int) + (batched ? 0 : sizeof(int)));

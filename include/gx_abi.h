@@ -289,6 +289,7 @@ typedef struct {
   long long transport_read[3];    /* track records read */
   long long transport_written[3]; /* records written: survivors and interacting tracks */
   long long transport_queued[3];  /* of those, records written to the interaction buffers */
+  long long transport_steps[3];   /* steps completed in the transport kernel */
 } gx_transport_stats;
 
 void gx_transport_config_default(gx_transport_config *cfg);
