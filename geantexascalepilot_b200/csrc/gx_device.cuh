@@ -36,6 +36,7 @@ enum : int {
   kErrStepCap = 2,     // a track exceeded max_steps
   kErrFieldCap = 4,    // field propagation sub-step cap
   kErrOverflow = 8,    // track store / stack full
+  kErrEvent = 16,      // a primary's event index outside the tally
 };
 
 // --------------------------------------------------------------- math policy

@@ -380,7 +380,7 @@ struct Local {
     retired += e;
     if (vol < 0 || vol >= nvol || e == 0.0) return;
     if (event < 0 || event >= nevents) { // a primary with an event index outside the tally
-      err |= kErrOverflow;
+      err |= kErrEvent;
       return;
     }
     int bin = event * nvol + vol;
@@ -2077,6 +2077,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     stats->bytes_per_track = (long long)(3 * sizeof(double) + 8 * sizeof(R) + 6 * sizeof(uint32_t) +
                                          3 * sizeof(int) + (batched ? 0 : sizeof(int)));
   }
+  if (c.err_flags & kErrEvent)
+    return set_error(GX_ERR_ARG, "transport: a primary's event index is outside [0, nevents = %d)", cfg->nevents);
   if (c.err_flags & kErrOverflow) return set_error(GX_ERR_OVERFLOW, "transport: track stores and stacks full");
   if (c.err_flags) return set_error(GX_ERR_ITERCAP, "transport: an iteration cap was hit (flags %d)", c.err_flags);
   return GX_OK;
@@ -2393,6 +2395,9 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
     stats->tracks_written[0] = (long long)hc.stat[S_WRITE0];
     stats->bytes_per_track = 128;
   }
+  if (hc.err_flags & kErrEvent)
+    return set_error(GX_ERR_ARG, "gx_transport_run_noalloc: a primary's event index is outside [0, nevents = %d)",
+                     cfg->nevents);
   if (hc.err_flags & kErrOverflow)
     return set_error(GX_ERR_OVERFLOW, "gx_transport_run_noalloc: more than %lld tracks in flight and deferred",
                      2 * kNoallocCapacity);

@@ -241,6 +241,34 @@ def test_injection_by_live_energy_leaves_results_unchanged(dm, n, capacity, wave
     assert abs(b.sum() + sb["escaped"] - e0) <= 1e-4 * e0  # FP32 energies
 
 
+def test_transport_edge_cases(dm):
+    """no primaries; primaries outside the world or leaving it at once; a
+    primary whose event index is outside the tally (an argument error, not a
+    store overflow)"""
+    import geantexascalepilot_b200 as gx
+    from geantexascalepilot_b200 import GxError, configs
+    cfg, prims, nvol = configs.c3(2, 2)
+    for engine in (0, 1):
+        for prec in (0, 1):
+            e, st, _ = run_gpu(dm, cfg, tuple(p[:0] if p is not None else None for p in prims), nvol,
+                               precision=prec, engine=engine)
+            assert st["steps"] == 0 and st["errors"] == 0 and not e.any()
+    types = np.array([1, 0, 2], np.int32)
+    E = np.array([1000.0, 500.0, 250.0])
+    pos = np.array([[-500.0, 0, 0], [-200.0, 0, 0], [0.0, 300.0, 0]])  # outside; on the front face; outside
+    d = np.array([[1.0, 0, 0], [-1.0, 0, 0], [1.0, 0, 0]])               # the second leaves at once
+    e, st, _ = run_gpu(dm, cfg, (types, E, pos, d, None), nvol, precision=0, engine=1)
+    assert st["steps"] == 0 and not e.any()
+    assert st["escaped"] == pytest.approx(1000.0 + 500.0 + 250.0)  # kinetic energies (primaries never entered)
+    ev = np.array([0, 5, 0], np.int32)
+    pos[:] = [-200.0, 0, 0]
+    d[:] = [1.0, 0, 0]
+    cfg.nevents = 2
+    with pytest.raises(GxError, match="event index"):
+        gx.transport(dm, cfg, types, E, pos, d, events=ev, nvol=nvol)
+    cfg.nevents = 1
+
+
 def test_run_command_line(capsys):
     import json
     from geantexascalepilot_b200 import run
