@@ -3,7 +3,7 @@
 
 One bench "step" is the complete transport of one batch of the headline
 workload (C3: 10^4 electrons + 10^4 photons of 10 GeV through the 50-layer
-Pb/LAr calorimeter in a 4 T field; BASELINE configs[2]) with the FP32-mixed
+Pb/LAr calorimeter in a 4 T field) with the FP32-mixed
 batched engine.  `value` is track-steps/s over the timed steps with the
 primaries already resident in HBM; `e2e` is the same metric through the
 public host-buffer entry point (gx_transport_run_host), primaries copied in
