@@ -2,8 +2,8 @@
  * gxo.h -- ORACLE (test infrastructure only).
  *
  * A plain-C, scalar CPU restatement of the reference's electromagnetic
- * particle-transport step path (Geant-RnD/GeantExascalePilot).  It is the
- * checker for the CUDA product in geantexascalepilot_b200/: only the tests,
+ * particle-transport step path (Geant-RnD/GeantExascalePilot), against which
+ * the CUDA product in geantexascalepilot_b200/ is tested: only the tests,
  * __graft_entry__.smoke() and bench.py's CPU-baseline leg load it, and never
  * as the thing measured or shipped.
  *

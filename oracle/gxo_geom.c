@@ -1,6 +1,6 @@
 /* gxo_geom.c -- CSG geometry and navigation for the oracle's step loop
- * (transport config geometry = 2).  Test infrastructure: the checker for the
- * library's device navigator, never part of the product.
+ * (transport config geometry = 2).  Test infrastructure: the library's device
+ * navigator is tested against it; never part of the product.
  *
  * The reference navigates a VecGeom volume tree (NavigationInterface::
  * FindNextBoundary, source/Geant/geometry/NavigationInterface.hpp:63-98, calls

@@ -15,7 +15,7 @@ def pytest_configure(config):
 
 
 def _ensure_oracle():
-    # make rebuilds the checker only when a source is newer than it
+    # make rebuilds the oracle only when a source is newer than it
     subprocess.check_call(["make", "-s", "-C", os.path.join(REPO, "oracle")])
     return os.path.join(REPO, "oracle", "liboracle.so")
 

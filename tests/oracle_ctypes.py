@@ -1,4 +1,4 @@
-"""ctypes front ends for the two CPU checkers (test infrastructure).
+"""ctypes front ends for the two CPU references of the tests (test infrastructure).
 
 ``Oracle`` wraps oracle/liboracle.so, the plain-C restatement of the
 reference's transport path.  ``Reference`` wraps oracle/_ref/libgxref.so,
