@@ -251,8 +251,8 @@ __device__ __forceinline__ int relocate(const Geom &g, int vol, double *p, const
 // Kernel variants, template parameters so that each kernel carries only the
 // code it runs: bit 0 follows the field map (Runge-Kutta sub-steps) instead of
 // the uniform field's helix, bit 1 navigates the CSG tree (gx_csg.cuh) instead
-// of the analytic volumes above.
-enum { kKindFieldMap = 1, kKindCsg = 2 };
+// of the analytic volumes above, bit 2 applies multiple scattering.
+enum { kKindFieldMap = 1, kKindCsg = 2, kKindMsc = 4 };
 
 template <int K> __device__ __forceinline__ double nav_safety(const Geom &g, int vol, const double *p)
 {
@@ -508,7 +508,8 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
 }
 
 // ------------------------------------------------------- multiple scattering
-// Multiple scattering of e-/e+ (config msc = 1): the Urban model as published
+// Multiple scattering of e-/e+ (config msc = 1, or 2 with lateral
+// displacement): the Urban model as published
 // (L. Urban, CERN-OPEN-2006-077); the reference has only a placeholder
 // (proxy/ProxyScattering.hpp:53-71) and ships the transport mean free path
 // tables (LambdaMod1.msc: E^2 / lambda1).  The oracle restates the same model
@@ -521,8 +522,15 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
 //     of a central exponential part (Highland-type width theta0), a power tail
 //     and a uniform part, weighted so that <cos theta> = exp(-tau); where the
 //     published weights would need a uniform part above 1 it is dropped and
-//     the central / tail split keeps that mean; phi uniform.
-// Not modelled: lateral displacement, the e+ correction of theta0.
+//     the central / tail split keeps that mean; phi uniform;
+//   lateral displacement (msc = 2), after a step that ends inside its volume:
+//     r = 0.73 r_max, r_max = sqrt(t^2 - z^2) the largest displacement the
+//     true and geometric lengths allow (the fixed fraction of early versions
+//     of the model), perpendicular to the direction at the start of the step,
+//     at the azimuth of the deflection (the displacement follows the turn),
+//     cut to 0.99 of the safety at the end point so that it never crosses a
+//     boundary, and none within 1e-5 mm of one.
+// Not modelled: the e+ correction of theta0.
 constexpr double kMscFr = 0.04, kMscFs = 0.6, kMscTmin = 1.0e-5;
 constexpr double kMscTauBig = 8.0, kMscTauSmall = 1.0e-16, kMscTauLim = 1.0e-6;
 
@@ -632,20 +640,46 @@ __device__ __forceinline__ R msc_cos_theta(Mrg &rng, const double *c, R t, R lam
 
 // deflect the direction by the sampled angle (no draw for phi when it is 0)
 template <class R>
-__device__ __forceinline__ void msc_deflect(const Data &d, Track<R> &t, int mat, R step, R lam0, R e0)
+// Returns false when the direction is kept (no azimuth drawn); sp, cp: the
+// azimuth of the deflection.
+__device__ __forceinline__ bool msc_deflect(const Data &d, Track<R> &t, int mat, R step, R lam0, R e0, R &sp, R &cp)
 {
   const R lam1 = msc_lambda1<R>(d, t.type, mat, t.E);
   R ct = msc_cos_theta<R>(t.rng, d.mat_msc[mat], step, lam0, lam1, e0, t.E);
-  if (!(ct < R(1))) return;
+  if (!(ct < R(1))) return false;
   if (ct < R(-1)) ct = R(-1);
   const R st = M<R>::sqrt((R(1) - ct) * (R(1) + ct));
-  R sp, cp;
   M<R>::sincos2pi(t.rng.template u<R>(), &sp, &cp);
   R u = st * cp, v = st * sp, w = ct;
   rotate_to_lab(u, v, w, t.dir[0], t.dir[1], t.dir[2]);
   t.dir[0] = u;
   t.dir[1] = v;
   t.dir[2] = w;
+  return true;
+}
+
+// The lateral displacement of a multiple-scattering step that ended inside
+// its volume (config msc = 2): 0.73 sqrt(t^2 - z^2) perpendicular to the
+// step's starting direction (d0, d1, d2) at the deflection's azimuth, cut to
+// 0.99 of the safety at the end point, none within kMscTmin of a boundary.
+// Out of line: the common path (msc 0 or 1) carries only the call.
+template <class R, int K>
+__device__ __noinline__ double3 msc_displacement(const Geom &g, int vol, double x, double y, double z, double t,
+                                                 double zg, R cp, R sp, R d0, R d1, R d2)
+{
+  double3 out = make_double3(0.0, 0.0, 0.0);
+  const double rmax2 = (t - zg) * (t + zg);
+  if (!(rmax2 > 0.0)) return out;
+  const double p[3] = {x, y, z};
+  const double saf = nav_safety<K>(g, vol, p);
+  if (!(saf > kMscTmin)) return out;
+  const double r = fmin(0.73 * sqrt(rmax2), 0.99 * saf);
+  R u = cp, v = sp, w = R(0);
+  rotate_to_lab(u, v, w, d0, d1, d2);
+  out.x = r * (double)u;
+  out.y = r * (double)v;
+  out.z = r * (double)w;
+  return out;
 }
 
 enum { kDone = 0, kAlive = 1, kInteract = 2 };
@@ -747,7 +781,7 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
   // geometric length to move
   c.lam0 = R(0);
   c.e0 = t.E;
-  if (charged && g.msc) {
+  if ((K & kKindMsc) != 0 && charged) {
     const R lam0 = msc_lambda1<R>(d, t.type, mat, t.E);
     if (t.msc_r0 <= R(0)) {
       R range = vec_value_fast<R>(d, d.vec[t.type == 2 ? GX_Range_ep : GX_Range_em][mat], t.E);
@@ -875,7 +909,7 @@ __device__ __forceinline__ double field_map_substep(const Data &d, const Geom &g
   return s;
 }
 
-// K: the kernel variant (kKindFieldMap, kKindCsg bits).
+// K: the kernel variant (kKindFieldMap, kKindCsg, kKindMsc bits).
 template <class R, int K>
 __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c, Local &L)
 {
@@ -941,14 +975,15 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
 // NIL update, continuous loss and the outcome of the step: kDone (track
 // finished), kAlive (no interaction this step) or kInteract with *proc set
 // (for a stopped e+, proc 2 = annihilation at rest, at E = 0).
-template <class R>
+template <class R, int K>
 __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &t, const StepCtx<R> &c, Local &L,
                                         int *proc)
 {
   const int np = (t.type == 1) ? 2 : 3;
   // the true length of the step: all of it, or back from where a boundary
   // stopped it
-  const double step = c.lam0 > R(0) ? (c.crossed ? msc_geom_to_true<R>(c.total, c.lam0, c.ttrue) : c.ttrue) : c.total;
+  const bool msc = (K & kKindMsc) != 0 && c.lam0 > R(0); // multiple scattering applied to this step
+  const double step = msc ? (c.crossed ? msc_geom_to_true<R>(c.total, c.lam0, c.ttrue) : c.ttrue) : c.total;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
     if (i < np) t.nil[i] -= (R)step * c.xs(i);
@@ -973,7 +1008,18 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
       }
       return kDone;
     }
-    if (c.lam0 > R(0)) msc_deflect<R>(d, t, vol_material(g, c.vol0), (R)step, c.lam0, c.e0);
+    if (msc) {
+      const R d0 = t.dir[0], d1 = t.dir[1], d2 = t.dir[2]; // the direction the step started in
+      R sp, cp;
+      const bool turned = msc_deflect<R>(d, t, vol_material(g, c.vol0), (R)step, c.lam0, c.e0, sp, cp);
+      if (g.msc == 2 && turned && !c.crossed) {
+        const double3 dx =
+            msc_displacement<R, K>(g, t.vol, t.pos[0], t.pos[1], t.pos[2], step, c.total, cp, sp, d0, d1, d2);
+        t.pos[0] += dx.x;
+        t.pos[1] += dx.y;
+        t.pos[2] += dx.z;
+      }
+    }
   }
   if (c.crossed) {
     t.msc_r0 = R(-1); // a new volume: the step limit starts again
@@ -1003,7 +1049,7 @@ __device__ __forceinline__ int transport_part(const Data &d, const Geom &g, Trac
   if (step_begin<R, K>(d, g, t, c))
     while (!field_substep<R, K>(d, g, t, c, L)) {
     }
-  return step_end(d, g, t, c, L, proc);
+  return step_end<R, K>(d, g, t, c, L, proc);
 }
 
 // The whole OneStep, interaction included (the fused form the plain loop
@@ -1354,7 +1400,7 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
       done = true;
     }
     if (done) {
-      r = step_end(d, a.g, t, c, L, &proc);
+      r = step_end<R, K>(d, a.g, t, c, L, &proc);
       ++nst;
       if (t.prim >= 0 && a.pstep) atomicAdd(&a.pstep[t.prim], 1);
     }
@@ -1706,13 +1752,20 @@ __global__ void k_fold_touchables(const double *__restrict__ vt, const int *__re
 }
 
 // The variant of the step kernels for a geometry and field (kKind* bits).
-static int kernel_kind(const Geom &g) { return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0); }
+static int kernel_kind(const Geom &g)
+{
+  return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0) | (g.msc ? kKindMsc : 0);
+}
 template <class R, int PT> static void (*transport_kernel(int kind))(const Args<R> *)
 {
   switch (kind) {
   case 1: return k_transport<R, PT, 1>;
   case 2: return k_transport<R, PT, 2>;
   case 3: return k_transport<R, PT, 3>;
+  case 4: return k_transport<R, PT, 4>;
+  case 5: return k_transport<R, PT, 5>;
+  case 6: return k_transport<R, PT, 6>;
+  case 7: return k_transport<R, PT, 7>;
   default: return k_transport<R, PT, 0>;
   }
 }
@@ -1722,6 +1775,10 @@ template <class R> static void (*step_kernel_p(int kind))(const Args<R> *)
   case 1: return k_step_p<R, 3, 1>;
   case 2: return k_step_p<R, 3, 2>;
   case 3: return k_step_p<R, 3, 3>;
+  case 4: return k_step_p<R, 3, 4>;
+  case 5: return k_step_p<R, 3, 5>;
+  case 6: return k_step_p<R, 3, 6>;
+  case 7: return k_step_p<R, 3, 7>;
   default: return k_step_p<R, 3, 0>;
   }
 }
@@ -2004,7 +2061,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     // (re)capture the iteration graph when its launch shape or its kernels
     // (field kind, geometry kind) change; the arguments themselves are read
     // from the device copy uploaded above
-    int shape[6] = {G, L.block, L.grid, L.smem, L.a.g.field_map, L.a.g.geometry == 2};
+    int shape[6] = {G, L.block, L.grid, L.smem, kernel_kind(L.a.g), 0};
     std::vector<char> key(sizeof(shape) + 2 * sizeof(void *));
     const void *ptrs[2] = {E->dargs, E->ctl};
     std::memcpy(key.data(), shape, sizeof(shape));
@@ -2127,6 +2184,7 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
   if (cfg->field_map && !C->host.fmap)
     return set_error(GX_ERR_ARG, "gx_transport_run: field_map = 1 without a field map (gx_ctx_load_field_map)");
   if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "gx_transport_run: bad geometry");
+  if (cfg->msc < 0 || cfg->msc > 2) return set_error(GX_ERR_ARG, "gx_transport_run: msc must be 0, 1 or 2");
   if (cfg->geometry == 2 && !C->csg_node)
     return set_error(GX_ERR_ARG, "gx_transport_run: geometry 2 without a volume tree (gx_ctx_load_geometry)");
   if (cfg->geometry == 2 && nvol != C->csg_nscore)
@@ -2365,7 +2423,8 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   for (;;) {
     k_refill<double><<<L.grid, L.block, 0, s>>>(L.a);
     k_refill_done<<<1, 1, 0, s>>>(ctl);
-    (cfg->field_map ? k_step<double, 3, 1> : k_step<double, 3, 0>)<<<L.grid, L.block, L.smem, s>>>(L.a);
+    (cfg->msc ? (cfg->field_map ? k_step<double, 3, 5> : k_step<double, 3, 4>)
+              : (cfg->field_map ? k_step<double, 3, 1> : k_step<double, 3, 0>))<<<L.grid, L.block, L.smem, s>>>(L.a);
     k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
     if ((err = cudaGetLastError()) != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: launch");
     if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||

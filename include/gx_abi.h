@@ -264,8 +264,9 @@ typedef struct {
   int steps_per_launch;    /* batched engine: steps of one track per transport launch, at most; a track
                               stays in registers between them (0: default 16; 1: one step per iteration) */
   int msc;                 /* 1: multiple scattering of e-/e+ (Urban-type: safety-based step limit, true /
-                              geometric path conversion, angular deflection; no lateral displacement);
-                              0: off (the reference has none, proxy/ProxyScattering.hpp:53-71) */
+                              geometric path conversion, angular deflection); 2: the same with lateral
+                              displacement (within the safety); 0: off (the reference has none,
+                              proxy/ProxyScattering.hpp:53-71) */
   int field_map;           /* 1: the context's field map (gx_ctx_load_field_map) with fourth-order
                               Runge-Kutta sub-steps, Bz ignored; 0: uniform Bz with the helix */
 } gx_transport_config;

@@ -262,7 +262,8 @@ static void cross_sections(const world_t *w, int type, int mat, double e, double
 static int nproc(int type) { return type == 1 ? 2 : 3; }
 
 /* ------------------------------------------------------ multiple scattering
- * Multiple scattering of e-/e+ (physics mode, config msc = 1): the Urban
+ * Multiple scattering of e-/e+ (physics mode, config msc = 1; 2 adds the
+ * lateral displacement): the Urban
  * model as published (L. Urban, CERN-OPEN-2006-077): the reference has only a
  * placeholder (proxy/ProxyScattering.hpp:53-71); it ships the transport mean
  * free path tables (LambdaMod1.msc.e-/e+: E^2 / lambda1, MeV^2 / mm).
@@ -276,8 +277,12 @@ static int nproc(int type) { return type == 1 ? 2 : 3; }
  *     tau = t / lambda1 (averaged over the loss); phi uniform.  Where the
  *     published weights would need a uniform part above 1, the uniform part is
  *     dropped and the central/tail split set to keep that mean (a choice of
- *     this restatement).
- * Not modelled: lateral displacement, the e+ correction of theta0. */
+ *     this restatement);
+ *   lateral displacement (msc = 2) after a step that ends inside its volume:
+ *     0.73 sqrt(t^2 - z^2) perpendicular to the starting direction at the
+ *     deflection's azimuth, cut to 0.99 of the end point's safety, none when
+ *     that safety is below MSC_TMIN.
+ * Not modelled: the e+ correction of theta0. */
 #define MSC_FR 0.04
 #define MSC_FS 0.6
 #define MSC_TMIN 1.0e-5
@@ -410,11 +415,12 @@ static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, dou
 }
 
 /* deflect the direction by the sampled angle (no draw for phi when it is 0) */
-static void msc_deflect(const world_t *w, track_t *tr, int mat, double t, double lam0, double e0)
+/* returns 0 when the direction is kept (no azimuth drawn); *phi: the azimuth */
+static int msc_deflect(const world_t *w, track_t *tr, int mat, double t, double lam0, double e0, double *phi_out)
 {
   double lam1 = msc_lambda1(w, tr->type, mat, tr->E);
   double ct = msc_cos_theta(&tr->rng, &w->msc[mat], t, lam0, lam1, e0, tr->E);
-  if (ct >= 1.0) return;
+  if (ct >= 1.0) return 0;
   if (ct < -1.0) ct = -1.0;
   double st = sqrt((1 - ct) * (1 + ct));
   double phi = TWOPI * gxo_mrg_u01(&tr->rng);
@@ -423,6 +429,8 @@ static void msc_deflect(const world_t *w, track_t *tr, int mat, double t, double
   tr->dir[0] = u;
   tr->dir[1] = v;
   tr->dir[2] = z;
+  *phi_out = phi;
+  return 1;
 }
 
 /* ---------------------------------------------------------- one track step */
@@ -693,6 +701,7 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
   }
   /* the true length of the step: all of it, or back from where a boundary
    * stopped it */
+  const double zgeom = step; /* the geometric length moved */
   if (msc && lam0 > 0.0) step = crossed ? msc_geom_to_true(step, lam0, ttrue) : ttrue;
   for (int i = 0; i < np; ++i) tr->nil[i] -= step * xs[i];
   t->steps++;
@@ -718,7 +727,23 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
       }
       return 0;
     }
-    if (msc && lam0 > 0.0) msc_deflect(w, tr, mat, step, lam0, e0);
+    if (msc && lam0 > 0.0) {
+      const double d0 = tr->dir[0], d1 = tr->dir[1], d2 = tr->dir[2];
+      double phi = 0.0;
+      int turned = msc_deflect(w, tr, mat, step, lam0, e0, &phi);
+      if (w->c->msc == 2 && turned && !crossed) { /* lateral displacement */
+        const double rmax2 = (step - zgeom) * (step + zgeom);
+        const double saf = rmax2 > 0.0 ? safety(w, tr->vol, tr->pos) : 0.0;
+        if (saf > MSC_TMIN) {
+          double r = fmin(0.73 * sqrt(rmax2), 0.99 * saf);
+          double u = cos(phi), v = sin(phi), z = 0.0;
+          gxo_rotate_to_lab(&u, &v, &z, d0, d1, d2);
+          tr->pos[0] += r * u;
+          tr->pos[1] += r * v;
+          tr->pos[2] += r * z;
+        }
+      }
+    }
   }
   if (crossed) {
     tr->msc_r0 = -1.0; /* a new volume: the step limit starts again */

@@ -278,15 +278,16 @@ def test_run_command_line(capsys):
     assert out["stats"]["steps"] > 200 and out["stats"]["errors"] == 0
 
 
-def test_multiple_scattering_fp64_matches_oracle(dm, oracle):
-    """With multiple scattering on, the FP64 engine and the oracle run the
-    same model on the same streams.  Its sampling takes logs, exponentials and
-    sines whose last bits differ between CUDA and glibc, which can flip a
-    rejection and send a track another way: compare the showers
-    statistically (C2, 1 GeV e-, 48 showers)."""
+@pytest.mark.parametrize("msc", [1, 2])
+def test_multiple_scattering_fp64_matches_oracle(dm, oracle, msc):
+    """With multiple scattering on (2: with lateral displacement), the FP64
+    engine and the oracle run the same model on the same streams.  Its
+    sampling takes logs, exponentials and sines whose last bits differ between
+    CUDA and glibc, which can flip a rejection and send a track another way:
+    compare the showers statistically (C2, 1 GeV e-, 48 showers)."""
     from geantexascalepilot_b200 import configs
     cfg, prims, nvol = configs.c2(48)
-    edep, st, _ = run_gpu(dm, cfg, prims, nvol, msc=1)
+    edep, st, _ = run_gpu(dm, cfg, prims, nvol, msc=msc)
     ref = run_oracle(oracle, cfg, prims, nvol)
     cfg.msc = 0
     assert st["errors"] == 0 and ref["errors"] == 0

@@ -59,7 +59,7 @@ def test_showers_with_multiple_scattering(oracle):
     from geantexascalepilot_b200 import configs
     cfg, prims, nvol = configs.c2(8)
     res = {}
-    for msc in (0, 1):
+    for msc in (0, 1, 2):
         c = oracle_config(cfg, 4)
         c.msc = msc
         res[msc] = r = oracle.transport(c, *prims[:4], nvol=nvol)
@@ -69,3 +69,9 @@ def test_showers_with_multiple_scattering(oracle):
     # the extra step limit adds steps; the primaries' energy stays in the calorimeter
     assert res[1]["steps"] > 1.05 * res[0]["steps"]
     assert res[1]["edep"].sum() > 0.95 * prims[1].sum()
+    # the lateral displacement moves tracks towards boundaries (smaller
+    # safeties, so more safety-limited steps) without changing the shower's
+    # scale
+    assert res[1]["steps"] < res[2]["steps"] < 1.15 * res[1]["steps"]
+    assert abs(res[2]["tracks"] - res[1]["tracks"]) < 0.03 * res[1]["tracks"]
+    assert res[2]["edep"].sum() > 0.95 * prims[1].sum()
