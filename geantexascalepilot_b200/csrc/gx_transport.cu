@@ -1343,8 +1343,7 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
 // tracks in a field), with the start and the end of a step attached to it, so
 // a lane whose step needs several sub-steps does not hold up the others.
 // All stores and buffers are written at slots reserved per warp, contiguous.
-template <class R, int PT, int K>
-__global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
+template <class R, int PT, int K> __device__ __forceinline__ void transport_body(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1433,6 +1432,18 @@ __global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> 
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err, S_TSTEP0 + PT);
+}
+
+template <class R, int PT, int K>
+__global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
+{
+  transport_body<R, PT, K>(A);
+}
+// The FP32 CSG variants: held to the 128 registers of the others they spill
+// 100-300 bytes; at 168 (three 128-thread blocks per SM) nearly none.
+template <class R, int PT, int K> __global__ void __maxnreg__(168) k_transport_csg(const Args<R> *__restrict__ A)
+{
+  transport_body<R, PT, K>(A);
 }
 
 // Post-step interaction of process PROC for the buffered tracks of type PT:
@@ -1756,17 +1767,24 @@ static int kernel_kind(const Geom &g)
 {
   return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0) | (g.msc ? kKindMsc : 0);
 }
+template <class R, int PT, int K> static void (*transport_variant())(const Args<R> *)
+{
+  if constexpr (sizeof(R) == 4 && (K & kKindCsg) != 0)
+    return k_transport_csg<R, PT, K>;
+  else
+    return k_transport<R, PT, K>;
+}
 template <class R, int PT> static void (*transport_kernel(int kind))(const Args<R> *)
 {
   switch (kind) {
-  case 1: return k_transport<R, PT, 1>;
-  case 2: return k_transport<R, PT, 2>;
-  case 3: return k_transport<R, PT, 3>;
-  case 4: return k_transport<R, PT, 4>;
-  case 5: return k_transport<R, PT, 5>;
-  case 6: return k_transport<R, PT, 6>;
-  case 7: return k_transport<R, PT, 7>;
-  default: return k_transport<R, PT, 0>;
+  case 1: return transport_variant<R, PT, 1>();
+  case 2: return transport_variant<R, PT, 2>();
+  case 3: return transport_variant<R, PT, 3>();
+  case 4: return transport_variant<R, PT, 4>();
+  case 5: return transport_variant<R, PT, 5>();
+  case 6: return transport_variant<R, PT, 6>();
+  case 7: return transport_variant<R, PT, 7>();
+  default: return transport_variant<R, PT, 0>();
   }
 }
 template <class R> static void (*step_kernel_p(int kind))(const Args<R> *)
