@@ -43,7 +43,7 @@ class TransportConfig(C.Structure):
                 ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
                 ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I),
-                ("field_map", I)]
+                ("field_map", I), ("steps_per_launch_by_type", I * 3)]
 
 
 class TransportStats(C.Structure):

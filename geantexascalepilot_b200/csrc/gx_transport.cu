@@ -96,7 +96,7 @@ template <class R> struct Args {
   // compactly so the interaction kernels read them coalesced (batched engine)
   Store<R> ibuf[3][3];
   long long qcap;
-  int step_budget; // steps of one track per transport launch, at most
+  int step_budget[3]; // steps of one track per transport launch, at most, per particle type
 };
 
 // ---------------------------------------------------------------- geometry
@@ -1358,7 +1358,7 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
-  const int budget = a.step_budget;
+  const int budget = a.step_budget[PT];
   Track<R> t;
   StepCtx<R> c;
   GammaXs<R> gxs;
@@ -1930,7 +1930,14 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         if (q != 1 || pr != 2) L.a.ibuf[q][pr] = carve<R>(base, off, cap, false);
     L.a.qcap = cap;
   }
-  L.a.step_budget = cfg->steps_per_launch > 0 ? cfg->steps_per_launch : kDefaultStepsPerLaunch;
+  {
+    // positrons are few and long-lived: a shorter budget keeps their kernel
+    // (on its own stream) off the iteration's critical path
+    const int spl = cfg->steps_per_launch > 0 ? cfg->steps_per_launch : kDefaultStepsPerLaunch;
+    for (int q = 0; q < 3; ++q)
+      L.a.step_budget[q] = cfg->steps_per_launch_by_type[q] > 0 ? cfg->steps_per_launch_by_type[q]
+                                                                : (q == 2 ? std::max(1, spl / 4) : spl);
+  }
   if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
   L.a.d = C->dev;
   L.a.ctl = E->ctl;

@@ -269,6 +269,8 @@ typedef struct {
                               proxy/ProxyScattering.hpp:53-71) */
   int field_map;           /* 1: the context's field map (gx_ctx_load_field_map) with fourth-order
                               Runge-Kutta sub-steps, Bz ignored; 0: uniform Bz with the helix */
+  int steps_per_launch_by_type[3]; /* batched engine: steps per transport launch for gamma, e-, e+
+                              (0: from steps_per_launch; e+ a quarter of it, at least 1) */
 } gx_transport_config;
 
 typedef struct {
