@@ -137,6 +137,7 @@ _SIGS = {
     "gx_geom_destroy": (None, [P]),
     "gx_geom_box": (I, [P, D, D, D, C.POINTER(I)]),
     "gx_geom_tube": (I, [P, D, D, D, C.POINTER(I)]),
+    "gx_geom_tube_segment": (I, [P, D, D, D, D, D, C.POINTER(I)]),
     "gx_geom_sphere": (I, [P, D, D, C.POINTER(I)]),
     "gx_geom_polyhedron": (I, [P, I, PD, C.POINTER(I)]),
     "gx_geom_logical_volume": (I, [P, I, I, I, C.POINTER(I)]),

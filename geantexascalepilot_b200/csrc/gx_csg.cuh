@@ -25,8 +25,8 @@
 //     direction: a point on a face it moves out through is outside;
 //   - safety: to the current solid's surface and, for each child, the larger
 //     of the distance to its bounding box and the solid's own lower bound.
-// Solids: box (half lengths), tube (rmin, rmax, half length; full phi),
-// sphere (rmin, rmax), convex polyhedron (the intersection of half-spaces
+// Solids: box (half lengths), tube (rmin, rmax, half length; full phi or a
+// phi segment), sphere (rmin, rmax), convex polyhedron (the intersection of half-spaces
 // n.x <= d, unit outward normals: trapezoids such as VecGeom's UnplacedTrd,
 // prisms, wedges).  Quadratic roots in the cancellation-free form; the
 // polyhedron's ray distances by clipping the ray against each plane.
@@ -127,6 +127,63 @@ __device__ __forceinline__ double dot3(const double *a, const double *b)
   return cadd(cadd(cmul(a[0], b[0]), cmul(a[1], b[1])), cmul(a[2], b[2]));
 }
 
+// The phi segment of a tube: phi in [s, s + dphi], bounded by the half-planes
+// at s and at e = s + dphi; (cos s, sin s, cos e, sin e) in the plane table at
+// p0, np = 1 for dphi <= pi (the wedge is the intersection of the half-spaces
+// n1.q <= 0, n1 = (sin s, -cos s), and n2.q <= 0, n2 = (-sin e, cos e)), 2 for
+// dphi > pi (their union).  h_k = n_k.q, ne_k = n_k.e.
+struct Wedge {
+  double cs, ss, ce, se;
+  int mode;
+  __device__ __forceinline__ double h1(double x, double y) const { return csub(cmul(ss, x), cmul(cs, y)); }
+  __device__ __forceinline__ double h2(double x, double y) const { return csub(cmul(ce, y), cmul(se, x)); }
+  // inside the half-space, or on its plane and not moving out
+  __device__ __forceinline__ static bool in(double h, double ne, double tol)
+  {
+    return h < -tol || (h <= tol && ne <= 0.0);
+  }
+  __device__ __forceinline__ bool contains(const double *q, const double *e, double tol) const
+  {
+    const bool a = in(h1(q[0], q[1]), h1(e[0], e[1]), tol), b = in(h2(q[0], q[1]), h2(e[0], e[1]), tol);
+    return mode == 1 ? (a && b) : (a || b);
+  }
+  // a point (no direction) within tol of the wedge
+  __device__ __forceinline__ bool holds(double x, double y, double tol) const
+  {
+    const bool a = h1(x, y) <= tol, b = h2(x, y) <= tol;
+    return mode == 1 ? (a && b) : (a || b);
+  }
+  // distance to leave the wedge from a point inside it
+  __device__ __forceinline__ double out(const double *q, const double *e, double tol) const
+  {
+    const double a = h1(q[0], q[1]), na = h1(e[0], e[1]), b = h2(q[0], q[1]), nb = h2(e[0], e[1]);
+    const double ta = na > 0.0 ? -a / na : kCsgInf, tb = nb > 0.0 ? -b / nb : kCsgInf;
+    if (mode == 1) return fmin(ta, tb);
+    const bool ia = in(a, na, tol), ib = in(b, nb, tol);
+    if (ia && ib) return fmax(ta, tb);
+    // inside one half-space only: out when it is left, unless the other is
+    // entered first (moving into it, it is never left again)
+    if (ia) return (nb < 0.0 && -b / nb <= ta) ? kCsgInf : ta;
+    if (ib) return (na < 0.0 && -a / na <= tb) ? kCsgInf : tb;
+    return 0.0;
+  }
+  __device__ __forceinline__ double safety_out(const double *q) const
+  {
+    const double a = -h1(q[0], q[1]), b = -h2(q[0], q[1]);
+    return mode == 1 ? fmin(a, b) : fmax(a, b);
+  }
+  __device__ __forceinline__ double safety_in(const double *q) const
+  {
+    const double a = h1(q[0], q[1]), b = h2(q[0], q[1]);
+    return mode == 1 ? fmax(a, b) : fmin(a, b);
+  }
+};
+__device__ __forceinline__ Wedge csg_wedge(const CsgNode &n, const double *pl)
+{
+  const double *w = pl + 4 * n.p0;
+  return Wedge{w[0], w[1], w[2], w[3], n.np};
+}
+
 // The convex polyhedron's queries: op 0 contains (1 or 0), 1 distance out,
 // 2 distance in, 3 safety out, 4 safety in (a constant at every call site).
 enum { kPolyContains = 0, kPolyOut = 1, kPolyIn = 2, kPolySafeOut = 3, kPolySafeIn = 4 };
@@ -187,6 +244,7 @@ __device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const doubl
     const double az = fabs(q[2]);
     if (az > n.c + tol) return false;
     if (az >= n.c - tol && cmul(q[2], e[2]) > 0.0) return false;
+    if (n.np && !csg_wedge(n, pl).contains(q, e, tol)) return false;
     r = sqrt(dot2(q, q));
     out = dot2(q, e);
   } else {
@@ -253,6 +311,7 @@ __device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const dou
       if (D2 >= 0.0) s = fmin(s, near_root(a, b, c2, sqrt(D2)));
     }
   }
+  if (n.kind == kCsgTube && n.np) s = fmin(s, csg_wedge(n, pl).out(q, e, kCsgTol));
   return s < 0.0 ? 0.0 : s;
 }
 
@@ -288,6 +347,13 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
   double a, b, r2;
   if (n.kind == kCsgTube) {
     const double dz = n.c;
+    const bool seg = n.np != 0;
+    Wedge w{0.0, 0.0, 0.0, 0.0, 0};
+    if (seg) w = csg_wedge(n, pl);
+    // the hit point at t is in the phi segment
+    auto in_phi = [&](double t) {
+      return !seg || w.holds(cadd(q[0], cmul(t, e[0])), cadd(q[1], cmul(t, e[1])), tol);
+    };
     double tz = -1.0;
     if (q[2] >= dz && e[2] < 0.0)
       tz = (dz - q[2]) / e[2];
@@ -296,7 +362,7 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
     if (tz >= 0.0) {
       const double x = cadd(q[0], cmul(tz, e[0])), y = cadd(q[1], cmul(tz, e[1]));
       const double r = sqrt(cadd(cmul(x, x), cmul(y, y)));
-      if (r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol)) s = tz;
+      if (r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol) && in_phi(tz)) s = tz;
     }
     a = dot2(e, e);
     b = dot2(q, e);
@@ -305,14 +371,30 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
       const double c = csub(r2, cmul(rmax, rmax)), D = csub(cmul(b, b), cmul(a, c));
       if (c >= 0.0 && b < 0.0 && D >= 0.0) { // the outer surface from outside
         const double t = near_root(a, b, c, sqrt(D));
-        if (t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol) s = t;
+        if (t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol && in_phi(t)) s = t;
       }
       if (rmin > 0.0) { // the inner surface from the bore
         const double c2 = csub(r2, cmul(rmin, rmin)), D2 = csub(cmul(b, b), cmul(a, c2));
         if (D2 >= 0.0) {
           const double t = far_root(a, b, c2, sqrt(D2));
-          if (t >= 0.0 && t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol) s = t;
+          if (t >= 0.0 && t < s && fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol && in_phi(t)) s = t;
         }
+      }
+    }
+    if (seg) { // the two half-planes, entered from their outer side
+#pragma unroll
+      for (int k = 0; k < 2; ++k) {
+        const double h = k == 0 ? w.h1(q[0], q[1]) : w.h2(q[0], q[1]);
+        const double ne = k == 0 ? w.h1(e[0], e[1]) : w.h2(e[0], e[1]);
+        if (!(ne < 0.0) || h < -tol) continue;
+        const double t = fmax(-h / ne, 0.0);
+        if (!(t < s)) continue;
+        const double x = cadd(q[0], cmul(t, e[0])), y = cadd(q[1], cmul(t, e[1]));
+        const double along = k == 0 ? cadd(cmul(w.cs, x), cmul(w.ss, y)) : cadd(cmul(w.ce, x), cmul(w.se, y));
+        const double r = sqrt(cadd(cmul(x, x), cmul(y, y)));
+        if (along >= -tol && r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol) &&
+            fabs(cadd(q[2], cmul(t, e[2]))) <= dz + tol)
+          s = t;
       }
     }
     return s;
@@ -337,8 +419,10 @@ __device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const d
   if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeOut, 0.0);
   if (n.kind == kCsgBox) return fmin(fmin(n.a - fabs(q[0]), n.b - fabs(q[1])), n.c - fabs(q[2]));
   if (n.kind == kCsgTube) {
-    const double r = sqrt(dot2(q, q)), s = fmin(n.c - fabs(q[2]), n.b - r);
-    return n.a > 0.0 ? fmin(s, r - n.a) : s;
+    const double r = sqrt(dot2(q, q));
+    double s = fmin(n.c - fabs(q[2]), n.b - r);
+    if (n.a > 0.0) s = fmin(s, r - n.a);
+    return n.np ? fmin(s, csg_wedge(n, pl).safety_out(q)) : s;
   }
   const double r = sqrt(dot3(q, q));
   return n.a > 0.0 ? fmin(n.b - r, r - n.a) : n.b - r;
@@ -351,7 +435,8 @@ __device__ __forceinline__ double csg_safety_in_local(const CsgNode &n, const do
   if (n.kind == kCsgBox) return fmax(fmax(fabs(q[0]) - n.a, fabs(q[1]) - n.b), fabs(q[2]) - n.c);
   if (n.kind == kCsgTube) {
     const double r = sqrt(dot2(q, q));
-    return fmax(fmax(fabs(q[2]) - n.c, r - n.b), n.a - r);
+    const double s = fmax(fmax(fabs(q[2]) - n.c, r - n.b), n.a - r);
+    return n.np ? fmax(s, csg_wedge(n, pl).safety_in(q)) : s;
   }
   const double r = sqrt(dot3(q, q));
   return fmax(r - n.b, n.a - r);

@@ -312,6 +312,25 @@ int gx_geom_tube(gx_geom *g, double rmin, double rmax, double dz, int *solid)
   return add_solid(g, kCsgTube, rmin, rmax, dz, solid);
 }
 
+int gx_geom_tube_segment(gx_geom *g, double rmin, double rmax, double dz, double sphi, double dphi, int *solid)
+{
+  const double pi = 3.14159265358979323846;
+  if (!(dphi > 0.0) || !std::isfinite(sphi))
+    return set_error(GX_ERR_ARG, "gx_geom_tube_segment: need dphi > 0 and a finite sphi");
+  if (dphi >= 2.0 * pi) return gx_geom_tube(g, rmin, rmax, dz, solid);
+  int rc = gx_geom_tube(g, rmin, rmax, dz, solid);
+  if (rc) return rc;
+  // the half-planes' directions (cos s, sin s, cos e, sin e), e = sphi + dphi,
+  // as one row of the plane table; np = 1 (dphi <= pi: the wedge is convex)
+  // or 2 (the union of the two half-spaces)
+  gx_geom::Solid &s = g->solids[*solid];
+  const double e = sphi + dphi;
+  s.p0 = (int)(g->planes.size() / 4);
+  s.np = dphi <= pi ? 1 : 2;
+  g->planes.insert(g->planes.end(), {std::cos(sphi), std::sin(sphi), std::cos(e), std::sin(e)});
+  return GX_OK;
+}
+
 int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid)
 {
   if (!(rmin >= 0.0 && rmax > rmin)) return set_error(GX_ERR_ARG, "gx_geom_sphere: need 0 <= rmin < rmax");

@@ -3,10 +3,9 @@
 The classes take the calls a VecGeom detector construction makes, as the
 reference's does (source/Geant/proxy/test/BasicCpuTransport/
 ProxyDetectorConstruction.cpp:241-324): ``UnplacedBox`` / ``UnplacedTube`` /
-``UnplacedSphere`` / ``UnplacedOrb``, ``LogicalVolume`` with
-``UnplacedTrd`` (and any convex polyhedron given by its planes,
-``ConvexPolyhedron``), ``LogicalVolume`` with
-``SetMaterialPtr`` and ``PlaceDaughter(name, lv, Transformation3D)``, and a
+``UnplacedSphere`` / ``UnplacedOrb`` / ``UnplacedTrd`` (and any convex
+polyhedron given by its planes, ``ConvexPolyhedron``; tubes may be phi
+segments), ``LogicalVolume`` with ``SetMaterialPtr`` and ``PlaceDaughter(name, lv, Transformation3D)``, and a
 ``GeoManager`` with ``SetWorld`` and ``CloseGeometry``.  Closing gives a
 ``CsgGeometry``: the tree as flat arrays, which ``load(dm)`` builds through the
 C ABI (gx_geom_*) and uploads into a context.  Two additions: a material is an
@@ -47,12 +46,17 @@ class UnplacedTube:
     kind = TUBE
 
     def __init__(self, *args):
-        """UnplacedTube([name,] rmin, rmax, dz[, sphi, dphi]): full phi only"""
+        """UnplacedTube([name,] rmin, rmax, dz[, sphi, dphi]): phi in radians;
+        dphi >= 2 pi (or no phi) is the full tube"""
         a = _strip_name(args)
         rmin, rmax, dz = a[:3]
-        if len(a) > 3 and not (len(a) == 5 and abs(a[4] - 2 * math.pi) < 1e-12):
-            raise ValueError("UnplacedTube: only full-phi tubes are supported")
+        if len(a) not in (3, 5):
+            raise ValueError("UnplacedTube: (rmin, rmax, dz) or (rmin, rmax, dz, sphi, dphi)")
         self.par = (float(rmin), float(rmax), float(dz))
+        # the phi segment, None for the full tube
+        self.phi = None if len(a) == 3 or a[4] >= 2 * math.pi else (float(a[3]), float(a[4]))
+        if self.phi is not None and not self.phi[1] > 0.0:
+            raise ValueError("UnplacedTube: dphi must be > 0")
 
 
 class UnplacedSphere:
@@ -186,7 +190,8 @@ class CsgGeometry:
                  splane_off=None, splanes=None):
         self.skind = np.asarray(skind, np.int32)
         self.spar = np.asarray(spar, np.float64).reshape(-1, 3)
-        # polyhedra: the planes of solid s are splanes[splane_off[s]:splane_off[s + 1]]
+        # polyhedra: the planes of solid s are splanes[splane_off[s]:splane_off[s + 1]];
+        # a tube with a phi segment has one row there, (sphi, dphi, 0, 0)
         self.splane_off = (np.zeros(len(self.skind) + 1, np.int32) if splane_off is None
                            else np.asarray(splane_off, np.int32))
         self.splanes = np.zeros((0, 4)) if splanes is None else np.asarray(splanes, np.float64).reshape(-1, 4)
@@ -231,6 +236,8 @@ class CsgGeometry:
         for s in solids:
             if s.kind == POLY:
                 planes.extend(s.planes.tolist())
+            elif s.kind == TUBE and getattr(s, "phi", None) is not None:
+                planes.append([s.phi[0], s.phi[1], 0.0, 0.0])  # a tube's phi segment: (sphi, dphi)
             off.append(len(planes))
         return cls([s.kind for s in solids], [s.par for s in solids], [sindex[id(lv.solid)] for lv in lvs],
                    [lv.material for lv in lvs], [int(lv.scored) for lv in lvs], pv_mother, pv_lv,
@@ -251,6 +258,9 @@ class CsgGeometry:
                                                  C.byref(out)))
                 elif k == BOX:
                     check(lib.gx_geom_box(h, p[0], p[1], p[2], C.byref(out)))
+                elif k == TUBE and self.splane_off[s + 1] > self.splane_off[s]:
+                    sphi, dphi = self.splanes[self.splane_off[s]][:2]
+                    check(lib.gx_geom_tube_segment(h, p[0], p[1], p[2], sphi, dphi, C.byref(out)))
                 elif k == TUBE:
                     check(lib.gx_geom_tube(h, p[0], p[1], p[2], C.byref(out)))
                 else:

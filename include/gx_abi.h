@@ -189,7 +189,7 @@ int gx_helix_dostep(const double B[3], double kB2C, int n, const double *d_posx,
  * geometry/NavigationInterface.hpp:63-98, over a tree built in
  * proxy/test/BasicCpuTransport/ProxyDetectorConstruction.cpp:241-324):
  *   new UnplacedBox(hx, hy, hz)             -> gx_geom_box
- *   new UnplacedTube(rmin, rmax, dz, 0, 2pi) -> gx_geom_tube
+ *   new UnplacedTube(rmin, rmax, dz, 0, 2pi) -> gx_geom_tube (a phi segment: gx_geom_tube_segment)
  *   new UnplacedSphere / UnplacedOrb (full)  -> gx_geom_sphere
  *   new UnplacedTrd(x1, x2, y1, y2, z) etc.  -> gx_geom_polyhedron (its planes)
  *   new LogicalVolume(name, solid) + SetMaterialPtr -> gx_geom_logical_volume
@@ -208,6 +208,10 @@ int gx_geom_create(gx_geom **out);
 void gx_geom_destroy(gx_geom *g);
 int gx_geom_box(gx_geom *g, double hx, double hy, double hz, int *solid);
 int gx_geom_tube(gx_geom *g, double rmin, double rmax, double dz, int *solid);
+/* new UnplacedTube(rmin, rmax, dz, sphi, dphi): the tube between the
+ * half-planes at phi = sphi and sphi + dphi (radians, 0 < dphi; 2 pi or more
+ * is the full tube) */
+int gx_geom_tube_segment(gx_geom *g, double rmin, double rmax, double dz, double sphi, double dphi, int *solid);
 int gx_geom_sphere(gx_geom *g, double rmin, double rmax, int *solid);
 /* A convex polyhedron {x : n_k . x <= d_k, k < nplanes} (4 to 32 planes,
  * planes[4k .. 4k+3] = outward normal n_k, any length, and offset d_k, in the

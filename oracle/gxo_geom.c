@@ -23,7 +23,8 @@
  *     direction: a point on a face it moves out through is outside;
  *   - safety: to the current solid's surface and to each child (the larger of
  *     the distance to its bounding box and the solid's own lower bound).
- * Solids: box (half lengths), tube (rmin, rmax, half length in z; full phi),
+ * Solids: box (half lengths), tube (rmin, rmax, half length in z; full phi or
+ * a phi segment [s, s + dphi] between two half-planes),
  * sphere (rmin, rmax), convex polyhedron (intersection of half-spaces
  * n.x <= d; the ray clipped against each plane).  Quadratic roots are taken in
  * the cancellation-free form (near root c / (-b + sqrt(D)), far root
@@ -49,6 +50,7 @@ typedef struct {
   const double *spar;
   const int *splane_off;
   double *slo, *shi; /* local bounding box per solid */
+  int *smode;        /* tubes: phi segment mode (0 full) */
   const int *lv_solid, *lv_mat, *lv_scored;
   const int *pv_mother, *pv_lv;
   const double *pv_t, *pv_r;
@@ -125,6 +127,8 @@ static int visit(build_t *b, int lv, int parent, const double R[9], const double
   n->c = b->spar[3 * s + 2];
   n->p0 = b->splane_off ? b->splane_off[s] : 0;
   n->np = (n->kind == GXO_CSG_POLY) ? b->splane_off[s + 1] - b->splane_off[s] : 0;
+  if (n->kind == GXO_CSG_TUBE && b->splane_off && b->splane_off[s + 1] > b->splane_off[s])
+    n->np = b->smode[s]; /* a phi segment: 1 (dphi <= pi) or 2 */
   memcpy(n->t, t, sizeof(n->t));
   memcpy(n->r, R, sizeof(n->r));
   n->rot = !(R[0] == 1.0 && R[1] == 0.0 && R[2] == 0.0 && R[3] == 0.0 && R[4] == 1.0 && R[5] == 0.0 &&
@@ -195,8 +199,8 @@ gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const
                          int world)
 {
   if (world < 0 || world >= nlv) return NULL;
-  build_t b = {nsolid, nlv, npv, skind, spar, splane_off, NULL, NULL, lv_solid, lv_mat, lv_scored, pv_mother, pv_lv,
-               pv_t, pv_r, NULL, 0, 0, 0};
+  build_t b = {nsolid, nlv, npv, skind, spar, splane_off, NULL, NULL, NULL, lv_solid, lv_mat, lv_scored, pv_mother,
+               pv_lv, pv_t, pv_r, NULL, 0, 0, 0};
   long total = count_nodes(&b, world, 0);
   if (total < 0) return NULL;
   gxo_csg_t *g = (gxo_csg_t *)calloc(1, sizeof(gxo_csg_t));
@@ -205,6 +209,7 @@ gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const
   g->planes = (double *)calloc((size_t)(4 * nplanes + 4), sizeof(double));
   b.slo = (double *)calloc((size_t)(3 * nsolid + 3), sizeof(double));
   b.shi = (double *)calloc((size_t)(3 * nsolid + 3), sizeof(double));
+  b.smode = (int *)calloc((size_t)(nsolid + 1), sizeof(int));
   int bad = 0;
   for (int s = 0; s < nsolid && !bad; ++s) {
     const double *p = spar + 3 * s;
@@ -218,6 +223,19 @@ gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const
       }
       bad = np < 4 || !poly_bbox(g->planes + 4 * p0, np, lo, hi);
       continue;
+    }
+    if (skind[s] == GXO_CSG_TUBE && splane_off && splane_off[s + 1] > splane_off[s]) {
+      /* a phi segment: the row holds (sphi, dphi); stored as the half-planes'
+       * directions (cos s, sin s, cos e, sin e), e = sphi + dphi */
+      const double *row = splanes + 4 * splane_off[s];
+      double sphi = row[0], dphi = row[1], e = sphi + dphi;
+      double *w = g->planes + 4 * splane_off[s];
+      w[0] = cos(sphi);
+      w[1] = sin(sphi);
+      w[2] = cos(e);
+      w[3] = sin(e);
+      b.smode[s] = dphi <= 3.14159265358979323846 ? 1 : 2;
+      bad = !(dphi > 0.0 && dphi < 2.0 * 3.14159265358979323846);
     }
     double h[3] = {p[0], p[1], p[2]};
     if (skind[s] == GXO_CSG_TUBE) h[0] = p[1];
@@ -234,6 +252,7 @@ gxo_csg_t *gxo_csg_build(int nsolid, const int *skind, const double *spar, const
   if (!bad) visit(&b, world, -1, I, z, 0);
   free(b.slo);
   free(b.shi);
+  free(b.smode);
   if (b.err || bad) {
     gxo_csg_free(g);
     return NULL;
@@ -268,6 +287,53 @@ static void to_local(const gxo_csg_node_t *n, const double *p, const double *d, 
 }
 
 /* inside, or on the surface and not moving out through it */
+/* The phi segment of a tube: (cos s, sin s, cos e, sin e) at plane-table row
+ * p0, np = 1 for dphi <= pi (the intersection of n1.q <= 0, n1 = (sin s,
+ * -cos s), and n2.q <= 0, n2 = (-sin e, cos e)), 2 for dphi > pi (their union). */
+typedef struct { double cs, ss, ce, se; int mode; } wedge_t;
+static wedge_t wedge_of(const gxo_csg_node_t *n, const double *pl)
+{
+  const double *w = pl + 4 * n->p0;
+  wedge_t x = {w[0], w[1], w[2], w[3], n->np};
+  return x;
+}
+static double wh1(const wedge_t *w, double x, double y) { return w->ss * x - w->cs * y; }
+static double wh2(const wedge_t *w, double x, double y) { return w->ce * y - w->se * x; }
+static int win(double h, double ne, double tol) { return h < -tol || (h <= tol && ne <= 0.0); }
+static int wedge_contains(const wedge_t *w, const double *q, const double *e, double tol)
+{
+  int a = win(wh1(w, q[0], q[1]), wh1(w, e[0], e[1]), tol), b = win(wh2(w, q[0], q[1]), wh2(w, e[0], e[1]), tol);
+  return w->mode == 1 ? (a && b) : (a || b);
+}
+static int wedge_holds(const wedge_t *w, double x, double y, double tol)
+{
+  int a = wh1(w, x, y) <= tol, b = wh2(w, x, y) <= tol;
+  return w->mode == 1 ? (a && b) : (a || b);
+}
+/* distance to leave the wedge from inside: the first plane left (dphi <= pi);
+ * for the union, the end of the stretch of the ray inside either half-space */
+static double wedge_out(const wedge_t *w, const double *q, const double *e, double tol)
+{
+  double a = wh1(w, q[0], q[1]), na = wh1(w, e[0], e[1]), b = wh2(w, q[0], q[1]), nb = wh2(w, e[0], e[1]);
+  double ta = na > 0.0 ? -a / na : CSG_INF, tb = nb > 0.0 ? -b / nb : CSG_INF;
+  if (w->mode == 1) return dmin(ta, tb);
+  int ia = win(a, na, tol), ib = win(b, nb, tol);
+  if (ia && ib) return dmax(ta, tb);
+  if (ia) return (nb < 0.0 && -b / nb <= ta) ? CSG_INF : ta;
+  if (ib) return (na < 0.0 && -a / na <= tb) ? CSG_INF : tb;
+  return 0.0;
+}
+static double wedge_safety_out(const wedge_t *w, const double *q)
+{
+  double a = -wh1(w, q[0], q[1]), b = -wh2(w, q[0], q[1]);
+  return w->mode == 1 ? dmin(a, b) : dmax(a, b);
+}
+static double wedge_safety_in(const wedge_t *w, const double *q)
+{
+  double a = wh1(w, q[0], q[1]), b = wh2(w, q[0], q[1]);
+  return w->mode == 1 ? dmax(a, b) : dmin(a, b);
+}
+
 /* n.q - d and n.e of plane k */
 static void plane_at(const double *pl, int k, const double *q, const double *e, double *h, double *ne)
 {
@@ -299,6 +365,10 @@ static int contains_local(const gxo_csg_node_t *n, const double *q, const double
     double a = fabs(q[2]);
     if (a > n->c + tol) return 0;
     if (a >= n->c - tol && q[2] * e[2] > 0.0) return 0;
+    if (n->np) {
+      wedge_t w = wedge_of(n, pl);
+      if (!wedge_contains(&w, q, e, tol)) return 0;
+    }
     double r = sqrt(q[0] * q[0] + q[1] * q[1]), out = q[0] * e[0] + q[1] * e[1];
     if (r > n->b + tol) return 0;
     if (r >= n->b - tol && out > 0.0) return 0;
@@ -362,6 +432,10 @@ static double dist_out_local(const gxo_csg_node_t *n, const double *q, const dou
         if (D2 >= 0.0) s = dmin(s, near_root(a, b, c2, sqrt(D2)));
       }
     }
+    if (n->np) {
+      wedge_t w = wedge_of(n, pl);
+      s = dmin(s, wedge_out(&w, q, e, GXO_CSG_TOL));
+    }
     return s < 0.0 ? 0.0 : s;
   }
   double a = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
@@ -420,6 +494,10 @@ static double dist_in_local(const gxo_csg_node_t *n, const double *q, const doub
   double s = CSG_INF;
   if (n->kind == GXO_CSG_TUBE) {
     const double rmin = n->a, rmax = n->b, dz = n->c;
+    const int seg = n->np != 0;
+    wedge_t w = {0, 0, 0, 0, 0};
+    if (seg) w = wedge_of(n, pl);
+#define IN_PHI(t) (!seg || wedge_holds(&w, q[0] + (t) * e[0], q[1] + (t) * e[1], tol))
     /* the end planes */
     double tz = -1.0;
     if (q[2] >= dz && e[2] < 0.0)
@@ -428,7 +506,7 @@ static double dist_in_local(const gxo_csg_node_t *n, const double *q, const doub
       tz = (-dz - q[2]) / e[2];
     if (tz >= 0.0) {
       double x = q[0] + tz * e[0], y = q[1] + tz * e[1], r = sqrt(x * x + y * y);
-      if (r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol)) s = tz;
+      if (r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol) && IN_PHI(tz)) s = tz;
     }
     double a = e[0] * e[0] + e[1] * e[1];
     if (a > 0.0) {
@@ -436,14 +514,29 @@ static double dist_in_local(const gxo_csg_node_t *n, const double *q, const doub
       double c = r2 - rmax * rmax, D = b * b - a * c;
       if (c >= 0.0 && b < 0.0 && D >= 0.0) { /* the outer surface from outside */
         double t = near_root(a, b, c, sqrt(D));
-        if (t < s && fabs(q[2] + t * e[2]) <= dz + tol) s = t;
+        if (t < s && fabs(q[2] + t * e[2]) <= dz + tol && IN_PHI(t)) s = t;
       }
       if (rmin > 0.0) { /* the inner surface from the bore */
         double c2 = r2 - rmin * rmin, D2 = b * b - a * c2;
         if (D2 >= 0.0) {
           double t = far_root(a, b, c2, sqrt(D2));
-          if (t >= 0.0 && t < s && fabs(q[2] + t * e[2]) <= dz + tol) s = t;
+          if (t >= 0.0 && t < s && fabs(q[2] + t * e[2]) <= dz + tol && IN_PHI(t)) s = t;
         }
+      }
+    }
+#undef IN_PHI
+    if (seg) { /* the two half-planes, entered from their outer side */
+      for (int k = 0; k < 2; ++k) {
+        double h = k == 0 ? wh1(&w, q[0], q[1]) : wh2(&w, q[0], q[1]);
+        double ne = k == 0 ? wh1(&w, e[0], e[1]) : wh2(&w, e[0], e[1]);
+        if (!(ne < 0.0) || h < -tol) continue;
+        double t = dmax(-h / ne, 0.0);
+        if (!(t < s)) continue;
+        double x = q[0] + t * e[0], y = q[1] + t * e[1];
+        double along = k == 0 ? w.cs * x + w.ss * y : w.ce * x + w.se * y;
+        double r = sqrt(x * x + y * y);
+        if (along >= -tol && r <= rmax + tol && (rmin <= 0.0 || r >= rmin - tol) && fabs(q[2] + t * e[2]) <= dz + tol)
+          s = t;
       }
     }
     return s;
@@ -478,7 +571,12 @@ static double safety_out_local(const gxo_csg_node_t *n, const double *q, const d
   if (n->kind == GXO_CSG_TUBE) {
     double r = sqrt(q[0] * q[0] + q[1] * q[1]);
     double s = dmin(n->c - fabs(q[2]), n->b - r);
-    return n->a > 0.0 ? dmin(s, r - n->a) : s;
+    if (n->a > 0.0) s = dmin(s, r - n->a);
+    if (n->np) {
+      wedge_t w = wedge_of(n, pl);
+      s = dmin(s, wedge_safety_out(&w, q));
+    }
+    return s;
   }
   double r = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
   return n->a > 0.0 ? dmin(n->b - r, r - n->a) : n->b - r;
@@ -499,7 +597,12 @@ static double safety_in_local(const gxo_csg_node_t *n, const double *q, const do
     return dmax(dmax(fabs(q[0]) - n->a, fabs(q[1]) - n->b), fabs(q[2]) - n->c);
   if (n->kind == GXO_CSG_TUBE) {
     double r = sqrt(q[0] * q[0] + q[1] * q[1]);
-    return dmax(dmax(fabs(q[2]) - n->c, r - n->b), n->a - r);
+    double s = dmax(dmax(fabs(q[2]) - n->c, r - n->b), n->a - r);
+    if (n->np) {
+      wedge_t w = wedge_of(n, pl);
+      s = dmax(s, wedge_safety_in(&w, q));
+    }
+    return s;
   }
   double r = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]);
   return dmax(r - n->b, n->a - r);

@@ -51,6 +51,14 @@ def mixed_geometry():
     box.PlaceDaughter("orb", orb, G.Transformation3D(5.0, -10.0, 20.0))
     box.PlaceDaughter("rod", rod, G.Transformation3D(-12.0, 15.0, -10.0, 0.0, 90.0, 0.0))
     box.PlaceDaughter("wedge", wedge, G.Transformation3D(15.0, 20.0, -30.0, 10.0, 0.0, 0.0))
+    arc = G.LogicalVolume("arc", G.UnplacedTube(40.0, 90.0, 60.0, 0.3, math.radians(100.0)))
+    arc.SetMaterialPtr("G4_Pb")
+    arc.SetScored()
+    horseshoe = G.LogicalVolume("horseshoe", G.UnplacedTube("hs", 0.0, 70.0, 50.0, -1.0, math.radians(270.0)))
+    horseshoe.SetMaterialPtr("G4_lAr")
+    horseshoe.SetScored()
+    world.PlaceDaughter("arc", arc, G.Transformation3D(-100.0, -350.0, -300.0, 10.0, 60.0, 0.0))
+    world.PlaceDaughter("horseshoe", horseshoe, G.Transformation3D(350.0, -50.0, 350.0))
     world.PlaceDaughter("trd", trd, G.Transformation3D(250.0, 200.0, -200.0, 20.0, 30.0, 40.0))
     world.PlaceDaughter("hex", hexa, G.Transformation3D(200.0, -250.0, 250.0, 0.0, 35.0, 10.0))
     world.PlaceDaughter("tube", tube, G.Transformation3D(100.0, -50.0, 20.0, 30.0, 40.0, 0.0))
@@ -116,6 +124,10 @@ class Tree:
             return abs(q[0]) < a and abs(q[1]) < b and abs(q[2]) < c
         if kind == 1:
             r = math.hypot(q[0], q[1])
+            if geo.splane_off[s + 1] > geo.splane_off[s]:  # a phi segment
+                sphi, dphi = geo.splanes[geo.splane_off[s]][:2]
+                if (math.atan2(q[1], q[0]) - sphi) % (2 * math.pi) >= dphi:
+                    return False
             return a < r < b and abs(q[2]) < c if a > 0 else r < b and abs(q[2]) < c
         r = np.linalg.norm(q)
         return a < r < b if a > 0 else r < b
@@ -147,9 +159,9 @@ def test_oracle_navigation_against_point_in_solid(oracle):
     geo = mixed_geometry()
     h = oracle.csg_build(geo)
     tree = Tree(oracle, h)
-    assert tree.n == 1 + 1 + 1 + 2 * 4 + 2
-    p, d = _rays(400, 11, [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300), (250, 200, -200),
-                           (200, -250, 250)])
+    assert tree.n == 1 + 1 + 1 + 2 * 4 + 2 + 2
+    p, d = _rays(500, 11, [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300), (250, 200, -200),
+                           (200, -250, 250), (-100, -350, -300), (350, -50, 350)])
     vol, snext, nxt, saf = oracle.csg_probe(h, p, d)
     rng = np.random.default_rng(5)
     checked_hits = 0
@@ -267,7 +279,12 @@ def test_library_builder_rejects_bad_trees():
     assert b"touchables" in lib.gx_last_error_string()
     lib.gx_geom_destroy(h)
     with pytest.raises(ValueError):
-        G.UnplacedTube(0.0, 1.0, 1.0, 0.0, 1.0)
+        G.UnplacedTube(0.0, 1.0, 1.0, 0.0, -1.0)
+    h = C.c_void_p()
+    assert lib.gx_geom_create(C.byref(h)) == 0
+    assert lib.gx_geom_tube_segment(h, 0.0, 1.0, 1.0, 0.0, 0.0, C.byref(s)) != 0
+    assert lib.gx_geom_tube_segment(h, 0.0, 1.0, 1.0, 0.5, 7.0, C.byref(s)) == 0  # 2 pi or more: the full tube
+    lib.gx_geom_destroy(h)
     # polyhedra whose planes bound no finite volume: a slab open along z, a
     # pyramid without a base, contradictory planes
     open_prism = [[1, 0, 0, 1], [-1, 0, 0, 1], [0, 1, 0, 1], [0, -1, 0, 1]]

@@ -39,7 +39,7 @@ def test_probe_matches_oracle(dm, oracle, name):
     if name == "mixed":
         geo = mixed_geometry()
         centres = [(100, -50, 20), (-250, 150, 0), (0, 350, -100), (-300, -300, 300), (250, 200, -200),
-                   (200, -250, 250)]
+                   (200, -250, 250), (-100, -350, -300), (350, -50, 350)]
     elif name == "crowded":
         geo = crowded_geometry()
         centres = [t["translation"] for t in geo.touchables() if t["parent"] >= 0]
