@@ -4,6 +4,7 @@
     python -m geantexascalepilot_b200.run c5 --nevents 64 --mean 100 --profile
     python -m geantexascalepilot_b200.run c4 --n 4096 --autotune
     python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --profile --capacity 2097152
+    python -m geantexascalepilot_b200.run c3 --geometry csg --msc 1 --field-map
 
 Prints one JSON line: the workload, the transport statistics (steps,
 propagation sub-steps, tracks, secondaries, iterations, per-kernel device
@@ -29,6 +30,12 @@ def main(argv=None):
     p.add_argument("--capacity", type=int, default=0,
                    help="track slots per particle type and store (0: the engine's default, 2^24)")
     p.add_argument("--repeat", type=int, default=1, help="transport the workload this many times")
+    p.add_argument("--geometry", choices=["layers", "csg"], default="layers",
+                   help="the analytic layered navigator, or the calorimeter as a CSG volume tree")
+    p.add_argument("--msc", type=int, default=None, choices=[0, 1, 2],
+                   help="multiple scattering: 0 off, 1 angular deflection, 2 with lateral displacement")
+    p.add_argument("--field-map", action="store_true",
+                   help="the shipped CMS field map (Runge-Kutta sub-steps) instead of the workload's uniform field")
     p.add_argument("--device", type=int, default=0)
     a = p.parse_args(argv)
 
@@ -49,6 +56,18 @@ def main(argv=None):
     cfg.capacity = a.capacity
     dm = gx.ProxyDataManager(device=a.device)
     out = {"workload": a.workload, "primaries": int(len(prims[0])), "precision": a.precision, "engine": a.engine}
+    if a.geometry == "csg":
+        from geantexascalepilot_b200 import geometry
+        dm.load_geometry(geometry.calorimeter(axis=cfg.axis))
+        cfg.geometry = 2
+        out["geometry"] = "csg"
+    if a.msc is not None:
+        cfg.msc = a.msc
+        out["msc"] = a.msc
+    if a.field_map:
+        dm.load_field_map()
+        cfg.field_map = 1
+        out["field_map"] = "cms"
     if a.autotune:
         cfg.profile = 0
         out["autotune"] = gx.autotune(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)[0]
