@@ -339,3 +339,26 @@ def test_multiple_scattering_fp32_vs_fp64_and_field(dm):
     big = a > 0.002 * a.sum()
     assert np.all(np.abs(a - b)[big] <= 0.01 * a[big] + 5 * 0.2 / np.sqrt(80) * a[big])
     assert abs(out[0][1]["steps"] - out[1][1]["steps"]) <= 0.02 * out[0][1]["steps"]
+
+
+def test_run_command_line_geometry_msc_field_map(capsys):
+    """The command line's CSG tree, multiple scattering and field-map options
+    reach the engine: the same C3 showers through the tree calorimeter, with
+    msc, and through the CMS map all conserve energy."""
+    import json
+    from geantexascalepilot_b200 import run
+    outs = {}
+    for name, extra in (("layers", []), ("csg", ["--geometry", "csg"]), ("msc", ["--msc", "2"]),
+                        ("map", ["--field-map"])):
+        assert run.main(["c3", "--electrons", "20", "--photons", "20", "--capacity", "262144"] + extra) == 0
+        outs[name] = json.loads(capsys.readouterr().out.strip().splitlines()[-1])
+    assert outs["csg"]["geometry"] == "csg" and outs["msc"]["msc"] == 2 and outs["map"]["field_map"] == "cms"
+    e0 = 40 * 1e4
+    for name, o in outs.items():
+        st = o["stats"]
+        assert st["errors"] == 0, name
+        assert abs(o["edep_total"] + st["escaped"] - e0) <= 1e-5 * e0, name  # FP32-mixed energies
+    # the tree calorimeter is the layered one: same streams, steps within 2%
+    a, b = outs["layers"]["stats"]["steps"], outs["csg"]["stats"]["steps"]
+    assert abs(a - b) < 0.02 * a
+    assert outs["msc"]["stats"]["steps"] > a
