@@ -378,6 +378,16 @@ def main():
                 per[int(f[0])] = float(f[1])
         if k in per:
             traffic = per[k] * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
+    pipes = None
+    pf = os.path.join(REPO, "profiles", "transport_kernel_pipes.txt")
+    if os.path.exists(pf):
+        # FP64 / FP32 / ALU pipe and issue utilisation (% of peak) of this
+        # kernel from the same ncu capture: the kernel is latency-bound
+        for line in open(pf):
+            f = line.split()
+            if len(f) == 6 and not line.startswith("#") and int(f[0]) == k:
+                pipes = {"fp64_pct": float(f[1]), "fp32_fma_pct": float(f[2]), "alu_pct": float(f[3]),
+                         "issue_pct": float(f[4]), "active_lanes_of_32": float(f[5]), "source": "ncu"}
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "traffic": traffic, "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
@@ -387,7 +397,8 @@ def main():
                        "record_bytes_moved_gbs": moved / (stp["transport_ms"][k] / 1e3) / 1e9,
                        "avg_launch_ms": stp["transport_ms"][k] / launches_k,
                        "share_of_step_kernel_time": stp["transport_ms"][k] / max(1e-9, sum(stp["step_ms"])),
-                       "records_per_launch": (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k}
+                       "records_per_launch": (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k,
+                       "pipes": pipes}
 
     if rank == 0:
         v, n, dtc = cpu_baseline(c3_sample(args.electrons, args.photons), args.cpu_seconds, os.cpu_count() or 1)
