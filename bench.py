@@ -298,12 +298,11 @@ def main():
 
     # the other two throughput workloads on the same engine (FP32-mixed):
     # C4, 2^16 mixed e-/e+/gamma, log-uniform 10 MeV - 100 GeV, 4 T along z;
-    # C5, events of Poisson(100) 10 GeV electrons scored per event (256 of the
-    # 4096 events, to keep the run short)
+    # C5, 4096 events of Poisson(100) 10 GeV electrons scored per event
     # and C3 itself through the CSG volume tree (the calorimeter built from
     # placed boxes, as the reference's detector construction does)
     extra = {}
-    for name, fn in (("c4", lambda: configs.c4(65536)), ("c5", lambda: configs.c5(256, 100)),
+    for name, fn in (("c4", lambda: configs.c4(65536)), ("c5", lambda: configs.c5(4096, 100)),
                      ("c3_csg_tree", lambda: configs.c3())):
         c, pr, nv = fn()
         c.precision, c.engine, c.first_substream = 1, 1, rank * len(pr[0])
