@@ -11,6 +11,7 @@ from .api import (ANNIHILATION, BETHE_HEITLER, BHABHA, ELECTRON, GAMMA, KLEIN_NI
                   MRG32k3a, ProxyAnnihilation, ProxyBetheHeitler, ProxyBhabhaScattering, ProxyBremsstrahlung,
                   ProxyCompton, ProxyConversion, ProxyDataManager, ProxyIonization, ProxyKleinNishina,
                   ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, autotune,
-                  cut_convert, default_config, egamma_gun, hepevt_load, hepevt_read, pdg_to_type, set_direction_xyz,
+                  cut_convert, default_config, egamma_gun, hepevt_load, hepevt_read, math_eval, pdg_to_type,
+                  set_direction_xyz,
                   spot_gun, transport, transport_host, transport_noalloc)
 from . import configs, geometry, sharding  # noqa: F401

@@ -43,7 +43,7 @@ class TransportConfig(C.Structure):
                 ("max_steps", I), ("seed", D * 6), ("first_substream", LL), ("nevents", I), ("precision", I),
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
                 ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I),
-                ("field_map", I), ("steps_per_launch_by_type", I * 3)]
+                ("field_map", I), ("steps_per_launch_by_type", I * 3), ("fp64_parity", I)]
 
 
 class TransportStats(C.Structure):
@@ -119,6 +119,7 @@ _SIGS = {
     "gx_ioni_along_gpil": (I, [P, I, I, P, P, P, I, P]),
     "gx_ioni_along_doit": (I, [P, I, I, P, P, P, P, I, P]),
     "gx_helix_dostep": (I, [PD, D, I] + [P] * 15 + [P]),
+    "gx_math_eval": (I, [I, I, I, P, P, P, P]),
     "gx_transport_config_default": (None, [C.POINTER(TransportConfig)]),
     "gx_transport_run": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P, C.POINTER(TransportStats), P]),
     "gx_transport_run_host": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P,

@@ -8,6 +8,7 @@ tracks held in torch CUDA tensors and calls the CUDA kernels through the C ABI
 cannot be created and every call raises.
 """
 import ctypes as C
+import os
 
 import numpy as np
 import torch
@@ -307,6 +308,21 @@ class ConstFieldHelixStepper:
         return torch.stack(outs[:3], 1), torch.stack(outs[3:], 1)
 
 
+MATH_FUNCS = {"log": 0, "exp": 1, "pow": 2, "sin": 3, "cos": 4, "expm1": 5, "log1p": 6}
+
+
+def math_eval(name, x, y=None, cuda_libm=False):
+    """gx_math_eval: the FP64 parity variant's elementary function `name`
+    (gx_math.h), or CUDA's own with cuda_libm, at the arguments x (and y for
+    pow), on the device; returns a CUDA tensor."""
+    xt = _dev(x, torch.float64)
+    yt = _dev(y, torch.float64) if y is not None else None
+    out = torch.empty_like(xt)
+    check(lib.gx_math_eval(MATH_FUNCS[name], int(bool(cuda_libm)), xt.numel(), _ptr(xt), _ptr(yt), _ptr(out),
+                           _stream()))
+    return out
+
+
 def default_config():
     cfg = TransportConfig()
     lib.gx_transport_config_default(C.byref(cfg))
@@ -372,8 +388,19 @@ def transport_host(dm, cfg, types, E, pos, direction, events=None, nvol=None):
     return edep, st.as_dict()
 
 
-NOALLOC_CAPACITY = 16384
-NOALLOC_MAX_PRIMARIES = 4096
+def _abi_define(name):
+    """An integer #define of include/gx_abi.h (the one place the limits live)."""
+    import re
+    hdr = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include", "gx_abi.h")
+    with open(hdr) as f:
+        m = re.search(r"^#define\s+%s\s+(\d+)" % name, f.read(), re.M)
+    if not m:
+        raise RuntimeError("%s not defined in %s" % (name, hdr))
+    return int(m.group(1))
+
+
+NOALLOC_CAPACITY = _abi_define("GX_NOALLOC_CAPACITY")
+NOALLOC_MAX_PRIMARIES = _abi_define("GX_NOALLOC_MAX_PRIMARIES")
 
 
 def transport_noalloc(dm, cfg, types, E, pos, direction, events=None, nvol=None, edep=None):

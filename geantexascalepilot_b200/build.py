@@ -38,17 +38,19 @@ def system_libstdcxx():
     return None
 
 
-# The per-function batch kernels and the particle gun reproduce the reference's
-# FP64 arithmetic operation by operation: no fused multiply-adds there, so they
-# round like the host code (only the transcendental functions differ).  The
-# transport engine keeps contraction.
-PER_FILE = {"gx_kernels.cu": ["-fmad=false"], "gx_events.cu": ["-fmad=false"]}
+# The per-function batch kernels, the particle gun and the FP64 parity variant
+# of the transport reproduce FP64 host arithmetic operation by operation: no
+# fused multiply-adds there, so they round like the host code.  The transport
+# engine itself keeps contraction.
+PER_FILE = {"gx_kernels.cu": ["-fmad=false"], "gx_events.cu": ["-fmad=false"],
+            "gx_transport_parity.cu": ["-fmad=false"]}
 
 
 def _compile(src, verbose):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    deps = glob.glob(os.path.join(CSRC, "*.cuh")) + [os.path.join(os.path.dirname(PKG), "include", "gx_abi.h"), src,
-                                                     os.path.abspath(__file__)]
+    # every source of the directory: headers, and .cu files that include others
+    deps = glob.glob(os.path.join(CSRC, "*")) + [os.path.join(os.path.dirname(PKG), "include", "gx_abi.h"),
+                                                 os.path.abspath(__file__)]
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
     extra = PER_FILE.get(os.path.basename(src), [])

@@ -507,6 +507,7 @@ int gx_ctx_destroy(gx_ctx *ctx)
   if (!ctx) return GX_OK;
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   release_engine(c);
+  parity::release_engine(c);
   for (void *p : c->owned) cudaFree(p);
   delete c;
   return GX_OK;

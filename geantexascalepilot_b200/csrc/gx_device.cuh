@@ -9,7 +9,34 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
+#include "gx_math.h"
+
 namespace gx {
+
+// Elementary functions of the FP64 arithmetic: CUDA's in the library's
+// kernels; in the FP64 parity variant of the transport (the translation unit
+// compiled with GX_PARITY, without contraction) those of gx_math.h, which the
+// oracle's parity build compiles too, so that the two take the same path
+// track by track.
+#ifdef GX_PARITY
+__device__ __forceinline__ double dlog(double x) { return gxm_log(x); }
+__device__ __forceinline__ double dexp(double x) { return gxm_exp(x); }
+__device__ __forceinline__ double dpow(double x, double y) { return gxm_pow(x, y); }
+__device__ __forceinline__ double dexpm1(double x) { return gxm_expm1(x); }
+__device__ __forceinline__ double dlog1p(double x) { return gxm_log1p(x); }
+__device__ __forceinline__ void dsincos(double x, double *s, double *c) { gxm_sincos(x, s, c); }
+#else
+__device__ __forceinline__ double dlog(double x) { return ::log(x); }
+__device__ __forceinline__ double dexp(double x) { return ::exp(x); }
+__device__ __forceinline__ double dpow(double x, double y) { return ::pow(x, y); }
+__device__ __forceinline__ double dexpm1(double x) { return ::expm1(x); }
+__device__ __forceinline__ double dlog1p(double x) { return ::log1p(x); }
+__device__ __forceinline__ void dsincos(double x, double *s, double *c)
+{
+  *s = ::sin(x);
+  *c = ::cos(x);
+}
+#endif
 
 // ------------------------------------------------------------------ constants
 // CLHEP units (mm, MeV, ns) as in source/Geant/proxy/ProxySystemOfUnits.hpp.
@@ -26,8 +53,21 @@ constexpr double kM1 = 4294967087.0;
 constexpr double kM2 = 4294944443.0;
 constexpr double kNorm = 1.0 / (4294967087.0 + 1.0);
 constexpr double kA12 = 1403580.0, kA13n = 810728.0, kA21 = 527612.0, kA23n = 1370589.0;
-constexpr double kRh1 = 2.3283065498378290e-010, kRl1 = -1.7354913086174288e-026;
-constexpr double kRh2 = 2.3283188252407387e-010, kRl2 = 2.4081018096503646e-026;
+// 1/m as the unevaluated sum rh + rl of two doubles (rh = 1/m rounded, rl the
+// rest rounded), for the exact quotient trunc(p rh + p rl) of a draw.  Derived
+// here with Dekker's exact product (T. J. Dekker, Numer. Math. 18 (1971)
+// 224-242; Veltkamp's split at 2^27 + 1): m rh = ph + pl exactly, so
+// 1/m - rh = (1 - m rh) / m = ((1 - ph) - pl) / m, where 1 - ph is exact.
+constexpr double dekker_hi(double a) { return 134217729.0 * a - (134217729.0 * a - a); }
+constexpr double dekker_prod_err(double a, double b)
+{
+  return ((dekker_hi(a) * dekker_hi(b) - a * b) + dekker_hi(a) * (b - dekker_hi(b)) +
+          (a - dekker_hi(a)) * dekker_hi(b)) +
+         (a - dekker_hi(a)) * (b - dekker_hi(b));
+}
+constexpr double recip_lo(double m) { return ((1.0 - m * (1.0 / m)) - dekker_prod_err(m, 1.0 / m)) / m; }
+constexpr double kRh1 = 1.0 / kM1, kRl1 = recip_lo(kM1);
+constexpr double kRh2 = 1.0 / kM2, kRl2 = recip_lo(kM2);
 
 // ------------------------------------------------------------------- errors
 enum : int {
@@ -42,24 +82,26 @@ enum : int {
 // --------------------------------------------------------------- math policy
 template <class R> struct M;
 template <> struct M<double> {
-  static __device__ __forceinline__ double log(double x) { return ::log(x); }
-  static __device__ __forceinline__ double exp(double x) { return ::exp(x); }
+  static __device__ __forceinline__ double log(double x) { return dlog(x); }
+  static __device__ __forceinline__ double exp(double x) { return dexp(x); }
   static __device__ __forceinline__ double sqrt(double x) { return ::sqrt(x); }
-  static __device__ __forceinline__ double pow(double x, double y) { return ::pow(x, y); }
-  static __device__ __forceinline__ double cbrt(double x) { return ::pow(x, 1.0 / 3.0); }
-  static __device__ __forceinline__ void sincos(double x, double *s, double *c)
-  {
-    *s = ::sin(x);
-    *c = ::cos(x);
-  }
+  static __device__ __forceinline__ double pow(double x, double y) { return dpow(x, y); }
+  static __device__ __forceinline__ double cbrt(double x) { return dpow(x, 1.0 / 3.0); }
+  static __device__ __forceinline__ void sincos(double x, double *s, double *c) { dsincos(x, s, c); }
   // sin/cos of 2 pi u
-  static __device__ __forceinline__ void sincos2pi(double u, double *s, double *c)
+  static __device__ __forceinline__ void sincos2pi(double u, double *s, double *c) { dsincos(kTwoPi * u, s, c); }
+  static __device__ __forceinline__ double cosr(double x)
   {
-    double phi = kTwoPi * u;
-    *s = ::sin(phi);
-    *c = ::cos(phi);
+    double s, c;
+    dsincos(x, &s, &c);
+    return c;
   }
-  static __device__ __forceinline__ double cosr(double x) { return ::cos(x); }
+  static __device__ __forceinline__ double sinr(double x)
+  {
+    double s, c;
+    dsincos(x, &s, &c);
+    return s;
+  }
 };
 template <> struct M<float> {
   static __device__ __forceinline__ float log(float x) { return __logf(x); }
@@ -70,6 +112,7 @@ template <> struct M<float> {
   static __device__ __forceinline__ void sincos(float x, float *s, float *c) { sincosf(x, s, c); }
   static __device__ __forceinline__ void sincos2pi(float u, float *s, float *c) { sincospif(2.0f * u, s, c); }
   static __device__ __forceinline__ float cosr(float x) { return __cosf(x); }
+  static __device__ __forceinline__ float sinr(float x) { return sinf(x); }
 };
 
 // ------------------------------------------------------------------ MRG32k3a
@@ -210,7 +253,7 @@ __device__ __forceinline__ double vec_value_ref(const Data &d, const VecDesc &v,
 {
   if (e <= v.emin) return __ldg(&d.y[v.off]);
   if (e >= v.emax) return __ldg(&d.y[v.off + v.n - 1]);
-  int bin = (int)(::log(e) / v.dbin - v.base);
+  int bin = (int)(dlog(e) / v.dbin - v.base);
   if (bin > v.n - 2) bin = v.n - 2;
   const double *x = d.x + v.off, *y = d.y + v.off, *d2 = d.d2 + v.off;
   if (bin > 0 && e < __ldg(&x[bin])) --bin;
@@ -570,10 +613,10 @@ template <class R> __device__ int bh_sample(Mrg &r, const ModelParams &p, Inter<
     epsil = epsil0 + (R(0.5) - epsil0) * r.u<R>();
   } else {
     double zi = (double)(int)(Z + 0.5);
-    R logZ3 = (R)(::log(zi) / 3.0);
+    R logZ3 = (R)(dlog(zi) / 3.0);
     R FZ = R(8) * logZ3;
     if (gE > R(50.0)) FZ += R(8) * (R)coulomb_factor((double)Z);
-    R Z3 = (R)::pow(zi, 1 / 3.0);
+    R Z3 = (R)dpow(zi, 1 / 3.0);
     R screenfac = R(136) * epsil0 / Z3;
     R screenmax = M<R>::exp((R(42.24) - FZ) / R(8.368)) - R(0.952);
     R screenmin = fmin(R(4) * screenfac, screenmax);
@@ -847,7 +890,7 @@ __device__ __forceinline__ double annih_xs_per_electron(double pi_rcl2, double k
   double ekin = fmax(eV, kin);
   double tau = ekin / kEMass, gam = tau + 1.0, gamma2 = gam * gam;
   double bg2 = tau * (tau + 2.0), bg = ::sqrt(bg2);
-  return pi_rcl2 * ((gamma2 + 4 * gam + 1.) * ::log(gam + bg) - (gam + 3.) * bg) / (bg2 * (gam + 1.));
+  return pi_rcl2 * ((gamma2 + 4 * gam + 1.) * dlog(gam + bg) - (gam + 3.) * bg) / (bg2 * (gam + 1.));
 }
 
 // The same cross section times the material's electron density (1/mm), in
@@ -904,7 +947,7 @@ __device__ __forceinline__ void helix_dostep(double kB2C, const double B[3], con
   double cx = vy * uz - vz * uy, cy = vz * ux - vx * uz, cz = vx * uy - vy * ux;
   double phi = -step * charge * Bmag * kB2C / momentum;
   double sinphi, cosphi;
-  sincos(phi, &sinphi, &cosphi);
+  dsincos(phi, &sinphi, &cosphi);
   np[0] = pos[0] + R * (cosphi - 1) * cx - R * sinphi * vx + step * UVdotUB * ux;
   np[1] = pos[1] + R * (cosphi - 1) * cy - R * sinphi * vy + step * UVdotUB * uy;
   np[2] = pos[2] + R * (cosphi - 1) * cz - R * sinphi * vz + step * UVdotUB * uz;

@@ -10,6 +10,9 @@
 namespace gx {
 
 struct Engine; // transport buffers, kept across calls (gx_transport.cu)
+namespace parity {
+struct Engine; // the same for the FP64 parity variant (gx_transport_parity.cu)
+}
 
 struct Ctx {
   int device = 0;
@@ -18,6 +21,7 @@ struct Ctx {
   Data *dev = nullptr;  // device copy
   std::vector<void *> owned;
   Engine *engine = nullptr;
+  parity::Engine *parity_engine = nullptr;
   // the CSG volume tree (gx_ctx_load_geometry): touchables, children, tally column of each
   CsgNode *csg_node = nullptr;
   int *csg_kids = nullptr, *csg_score = nullptr, *csg_slab = nullptr, *csg_cand = nullptr;
@@ -30,7 +34,16 @@ int cuda_error(cudaError_t e, const char *what);
 void jump_matrix(int comp, long long e, long long c, uint64_t out[9]);
 void mat_mul(const uint64_t A[9], const uint64_t B[9], uint64_t C[9], uint64_t m);
 void mat_vec(const uint64_t A[9], uint64_t v[3], uint64_t m);
+void build_jump_host(uint64_t h[2][64][9]);
 void release_engine(Ctx *c);
+int launch_substreams(const double seed[6], long long first, int n, uint32_t *d_states, cudaStream_t s);
+int get_jump_table(uint64_t **out);
+namespace parity {
+void release_engine(Ctx *c);
+int run_transport(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
+                  const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
+                  int *d_pstep, gx_transport_stats *stats, cudaStream_t s);
+} // namespace parity
 int refit_vector(Ctx *ctx, int table, int mat, const double *ynew);
 
 inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }

@@ -90,6 +90,23 @@ __global__ void k_rng_uniform(uint32_t *__restrict__ st, int n, int k, double *_
 static std::mutex g_jump_mu;
 static uint64_t *g_jump_dev[64] = {nullptr};
 
+// The skip-ahead table of the substream jumps: h[c][b] = A_c^(2^(76 + b))
+// mod m_c for the two components c of MRG32k3a, b = 0..63 (A^(2^76) is one
+// substream, MRG32k3a::AdvanceState(76, 0)).  The one host recipe of every
+// copy of the table on a device.
+void build_jump_host(uint64_t h[2][64][9])
+{
+  const uint64_t m[2] = {4294967087ULL, 4294944443ULL};
+  for (int c = 0; c < 2; ++c) {
+    uint64_t P[9];
+    jump_matrix(c, 76, 0, P); // A^(2^76)
+    for (int b = 0; b < 64; ++b) {
+      std::memcpy(h[c][b], P, sizeof(P));
+      mat_mul(P, P, P, m[c]);
+    }
+  }
+}
+
 int get_jump_table(uint64_t **out)
 {
   int dev = 0;
@@ -99,15 +116,7 @@ int get_jump_table(uint64_t **out)
   std::lock_guard<std::mutex> lk(g_jump_mu);
   if (!g_jump_dev[dev]) {
     uint64_t h[2][64][9];
-    const uint64_t m[2] = {4294967087ULL, 4294944443ULL};
-    for (int c = 0; c < 2; ++c) {
-      uint64_t P[9];
-      jump_matrix(c, 76, 0, P); // A^(2^76)
-      for (int b = 0; b < 64; ++b) {
-        std::memcpy(h[c][b], P, sizeof(P));
-        mat_mul(P, P, P, m[c]);
-      }
-    }
+    build_jump_host(h);
     uint64_t *d = nullptr;
     e = cudaMalloc((void **)&d, sizeof(h));
     if (e != cudaSuccess) return cuda_error(e, "cudaMalloc jump table");
@@ -299,6 +308,27 @@ using namespace gx;
   if (!(c)) return set_error(GX_ERR_ARG, "%s: null context", __func__);                                            \
   Ctx *C = reinterpret_cast<Ctx *>(c)
 
+// The elementary functions of the FP64 parity variant (gx_math.h), or CUDA's
+// own (lib = 1), one thread per argument.
+__global__ void k_math(int fn, int lib, int n, const double *__restrict__ x, const double *__restrict__ y,
+                       double *__restrict__ out)
+{
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double a = x[i], b = y ? y[i] : 0.0;
+  double r;
+  switch (fn) {
+  case 0: r = lib ? ::log(a) : gxm_log(a); break;
+  case 1: r = lib ? ::exp(a) : gxm_exp(a); break;
+  case 2: r = lib ? ::pow(a, b) : gxm_pow(a, b); break;
+  case 3: r = lib ? ::sin(a) : gxm_sin(a); break;
+  case 4: r = lib ? ::cos(a) : gxm_cos(a); break;
+  case 5: r = lib ? ::expm1(a) : gxm_expm1(a); break;
+  default: r = lib ? ::log1p(a) : gxm_log1p(a); break;
+  }
+  out[i] = r;
+}
+
 extern "C" {
 
 int gx_rng_substreams(const double seed[6], long long first, int n, uint32_t *d_states, gx_stream_t s)
@@ -482,6 +512,14 @@ int gx_helix_dostep(const double B[3], double kB2C, int n, const double *d_posx,
                  d_step, d_newposx, d_newposy, d_newposz, d_newdirx, d_newdiry, d_newdirz};
   if (n > 0) k_helix<<<grid_for(n), kBlock, 0, stream_of(s)>>>(a);
   return check_launch("k_helix");
+}
+
+int gx_math_eval(int fn, int lib, int n, const double *d_x, const double *d_y, double *d_out, gx_stream_t s)
+{
+  if (fn < 0 || fn > 6 || lib < 0 || lib > 1 || n < 0 || (n > 0 && (!d_x || !d_out)) || (fn == 2 && n > 0 && !d_y))
+    return set_error(GX_ERR_ARG, "gx_math_eval: bad args");
+  if (n > 0) k_math<<<grid_for(n), kBlock, 0, stream_of(s)>>>(fn, lib, n, d_x, d_y, d_out);
+  return check_launch("k_math");
 }
 
 } // extern "C"

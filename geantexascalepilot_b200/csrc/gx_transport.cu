@@ -16,6 +16,15 @@
 // The "plain" engine runs the same step code as one kernel over one mixed
 // store, launched and synchronised from the host every iteration, in FP64: the
 // straightforward GPU loop the batched engine is measured against.
+//
+// The FP64 parity variant: gx_transport_parity.cu compiles this file a second
+// time with GX_PARITY defined and without floating-point contraction, into
+// namespace gx::parity (FP64 only).  There the step takes the reference's
+// spline form for every table lookup, the reference's ionisation GPIL/DoIt,
+// the general helix step (ConstFieldHelixStepper::DoStep) with the
+// oracle's sub-step length, and the elementary functions of gx_math.h: the
+// same operations, in the same order and rounding, as the oracle's step loop,
+// so that the two agree track by track (gx_transport_config.fp64_parity).
 #include "gx_internal.cuh"
 
 #include <algorithm>
@@ -25,6 +34,14 @@
 #include <cstring>
 
 namespace gx {
+#ifdef GX_PARITY
+namespace parity {
+#define GX_ENGINE_OF(c) ((c)->parity_engine)
+#define GX_RELEASE_ENGINE(c) ::gx::parity::release_engine(c)
+#else
+#define GX_ENGINE_OF(c) ((c)->engine)
+#define GX_RELEASE_ENGINE(c) ::gx::release_engine(c)
+#endif
 
 // ------------------------------------------------------------------ layout
 template <class R> struct Store {
@@ -282,11 +299,23 @@ template <int K> __device__ __forceinline__ int nav_relocate(const Geom &g, int 
 }
 
 // ---------------------------------------------------------- cross sections
+// A table lookup of the step: the polynomial form (one record per bin); in
+// the parity variant the reference's spline form, as the oracle evaluates it.
+template <class R> __device__ __forceinline__ R tab_value(const Data &d, const VecDesc &v, R e)
+{
+#ifdef GX_PARITY
+  static_assert(sizeof(R) == 8, "the parity variant is FP64");
+  return vec_value_ref(d, v, e);
+#else
+  return vec_value_fast<R>(d, v, e);
+#endif
+}
+
 template <class R> __device__ __forceinline__ R lambda_tab(const Data &d, int t, int mat, R e)
 {
   const VecDesc &v = d.vec[t][mat];
   if ((double)e <= v.emin) return R(0);
-  return vec_value_fast<R>(d, v, e);
+  return tab_value<R>(d, v, e);
 }
 
 // Macroscopic cross sections (1/mm): gamma {Compton, conversion, photo-electric},
@@ -295,10 +324,10 @@ template <class R> __device__ __forceinline__ void cross_sections(const Data &d,
 {
   xs[0] = xs[1] = xs[2] = R(0);
   if (type == 0) {
-    xs[0] = (e < R(1)) ? vec_value_fast<R>(d, d.vec[GX_Lambda_compt][mat], e)
-                       : vec_value_fast<R>(d, d.vec[GX_LambdaPrim_compt][mat], e) / e;
+    xs[0] = (e < R(1)) ? tab_value<R>(d, d.vec[GX_Lambda_compt][mat], e)
+                       : tab_value<R>(d, d.vec[GX_LambdaPrim_compt][mat], e) / e;
     xs[1] = lambda_tab<R>(d, GX_Lambda_conv, mat, e);
-    xs[2] = (e >= R(0.2)) ? vec_value_fast<R>(d, d.vec[GX_LambdaPrim_phot][mat], e) / e
+    xs[2] = (e >= R(0.2)) ? tab_value<R>(d, d.vec[GX_LambdaPrim_phot][mat], e) / e
                           : (R)pe_xs_sandia(d, (int)d.mat_Z[mat], d.mat_density[mat], (double)e);
   } else if (type == 1) {
     xs[0] = lambda_tab<R>(d, GX_Lambda_eIoni_em, mat, e);
@@ -316,6 +345,9 @@ template <class R> __device__ __forceinline__ void cross_sections(const Data &d,
 // ProxyIonization::AlongStepGPIL in physics mode (Geant4 step function, length cut)
 template <class R> __device__ __forceinline__ R range_limit(const Data &d, int type, int mat, R e)
 {
+#ifdef GX_PARITY
+  return ioni_along_gpil_ref(d, 1, type == 2 ? 1 : -1, mat, e);
+#endif
   const R dR = R(0.2), finalRange = R(10.0);
   R range = vec_value_fast<R>(d, d.vec[type == 2 ? GX_Range_ep : GX_Range_em][mat], e);
   if (e < R(kMinE)) range *= e / R(kMinE);
@@ -329,6 +361,12 @@ template <class R> __device__ __forceinline__ R range_limit(const Data &d, int t
 // the loss exceeds 1%, i.e. near the end of the range) is evaluated in FP64.
 template <class R> __device__ __forceinline__ R along_loss(const Data &d, int type, int mat, double step, R &e)
 {
+#ifdef GX_PARITY
+  double edep = 0.0, ee = e;
+  ioni_along_doit_ref(d, 1, type == 2 ? 1 : -1, mat, step, ee, edep);
+  e = ee;
+  return edep;
+#endif
   bool ep = type == 2;
   R energy = e;
   R range = vec_value_fast<R>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], energy);
@@ -537,16 +575,16 @@ constexpr double kMscTauBig = 8.0, kMscTauSmall = 1.0e-16, kMscTauLim = 1.0e-6;
 // transport mean free path lambda1 (mm); 0 when the table has nothing
 template <class R> __device__ __forceinline__ R msc_lambda1(const Data &d, int type, int mat, R e)
 {
-  const R v = vec_value_fast<R>(d, d.vec[type == 2 ? GX_LambdaMod1_msc_ep : GX_LambdaMod1_msc_em][mat], e);
+  const R v = tab_value<R>(d, d.vec[type == 2 ? GX_LambdaMod1_msc_ep : GX_LambdaMod1_msc_em][mat], e);
   return v > R(0) ? e * e / v : R(0);
 }
 
 template <class R> __device__ __forceinline__ R msc_expm1(R x);
 template <> __device__ __forceinline__ float msc_expm1(float x) { return expm1f(x); }
-template <> __device__ __forceinline__ double msc_expm1(double x) { return ::expm1(x); }
+template <> __device__ __forceinline__ double msc_expm1(double x) { return dexpm1(x); }
 template <class R> __device__ __forceinline__ R msc_log1p(R x);
 template <> __device__ __forceinline__ float msc_log1p(float x) { return log1pf(x); }
-template <> __device__ __forceinline__ double msc_log1p(double x) { return ::log1p(x); }
+template <> __device__ __forceinline__ double msc_log1p(double x) { return dlog1p(x); }
 
 template <class R> __device__ __forceinline__ double msc_true_to_geom(double t, R lam)
 {
@@ -599,7 +637,7 @@ __device__ __forceinline__ R msc_cos_theta(Mrg &rng, const double *c, R t, R lam
   if (th0 > R(kPi / 6)) return msc_simple<R>(rng, xm, x2m);
   R x = th2 * (R(1) - th2 / R(12));
   if (th2 > R(0.01)) {
-    const R s = R(2) * sin(R(0.5) * th0);
+    const R s = R(2) * M<R>::sinr(R(0.5) * th0);
     x = s * s;
   }
   const R u = M<R>::exp(M<R>::log(tau) / R(6));
@@ -784,7 +822,7 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
   if ((K & kKindMsc) != 0 && charged) {
     const R lam0 = msc_lambda1<R>(d, t.type, mat, t.E);
     if (t.msc_r0 <= R(0)) {
-      R range = vec_value_fast<R>(d, d.vec[t.type == 2 ? GX_Range_ep : GX_Range_em][mat], t.E);
+      R range = tab_value<R>(d, d.vec[t.type == 2 ? GX_Range_ep : GX_Range_em][mat], t.E);
       if (t.E < R(kMinE)) range *= t.E / R(kMinE);
       t.msc_r0 = range > lam0 ? range : lam0;
     }
@@ -932,6 +970,27 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
   double step_gp = fmax(fmin(remaining, 1e-4), snext);
   R pt = p * M<R>::sqrt(fmax(R(1) - t.dir[2] * t.dir[2], R(0)));
   double step_field = 1.7976931348623157e308;
+#ifdef GX_PARITY
+  // the oracle's form: the sagitta length from the curvature, the general
+  // helix step, the direction renormalised by division
+  if (pt > 0.0) {
+    const double curv = 0.299792458 * fabs(g.Bz) / pt;
+    step_field = fmax(2.0 * ::sqrt(eps / curv), saf);
+  }
+  s = fmin(fmin(step_gp, step_field), remaining);
+  if (pt > 0.0) {
+    const double B[3] = {0.0, 0.0, g.Bz};
+    double np[3], nd[3];
+    helix_dostep(kB2C_mm, B, t.pos, t.dir, (double)charge, p, s, np, nd);
+    const double m = ::sqrt(nd[0] * nd[0] + nd[1] * nd[1] + nd[2] * nd[2]);
+    for (int k = 0; k < 3; ++k) {
+      t.pos[k] = np[k];
+      t.dir[k] = nd[k] / m;
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) t.pos[k] += s * dd[k];
+  }
+#else
   if (pt > R(0)) step_field = fmax(2.0 * (double)M<R>::sqrt(eps * pt / curv_per_pt), saf);
   s = fmin(fmin(step_gp, step_field), remaining);
   if (pt > R(0)) {
@@ -947,6 +1006,7 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
   } else {
     for (int k = 0; k < 3; ++k) t.pos[k] += s * dd[k];
   }
+#endif
   }
   c.total += s;
   c.remaining = remaining - s;
@@ -1723,7 +1783,7 @@ template <class R> static Store<R> carve(uintptr_t base, size_t &off, long long 
 
 void release_engine(Ctx *c)
 {
-  Engine *e = c->engine;
+  Engine *e = GX_ENGINE_OF(c);
   if (!e) return;
   if (e->graph) cudaGraphExecDestroy(e->graph);
   if (e->pool) cudaFree(e->pool);
@@ -1738,11 +1798,9 @@ void release_engine(Ctx *c)
   if (e->ev_j1) cudaEventDestroy(e->ev_j1);
   if (e->ev_j2) cudaEventDestroy(e->ev_j2);
   delete e;
-  c->engine = nullptr;
+  GX_ENGINE_OF(c) = nullptr;
 }
 
-int launch_substreams(const double seed[6], long long first, int n, uint32_t *d_states, cudaStream_t s);
-int get_jump_table(uint64_t **out);
 
 template <class R> struct Launch {
   Args<R> a;
@@ -1880,8 +1938,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   const int nstores = batched ? 3 : 1;
   long long cap = cfg->capacity > 0 ? cfg->capacity : (batched ? (1LL << 24) : (3LL << 24));
   long long stack_cap = std::max(cap, 1LL << 20);
-  Engine *&E = C->engine;
-  if (E && (E->precision != prec || E->engine != cfg->engine || E->cap != cap)) release_engine(C);
+  Engine *&E = GX_ENGINE_OF(C);
+  if (E && (E->precision != prec || E->engine != cfg->engine || E->cap != cap)) GX_RELEASE_ENGINE(C);
   cudaError_t err;
   if (!E) {
     E = new Engine();
@@ -1897,13 +1955,13 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       for (int k = 0; k < 8; ++k) carve<R>(0, bytes, cap, false);
     err = cudaMalloc(&E->pool, bytes);
     if (err != cudaSuccess) {
-      release_engine(C);
+      GX_RELEASE_ENGINE(C);
       return cuda_error(err, "transport track stores");
     }
     E->pool_bytes = bytes;
     if ((err = cudaMalloc((void **)&E->ctl, sizeof(Ctl))) != cudaSuccess ||
         (err = cudaMallocHost((void **)&E->h_ctl, sizeof(Ctl))) != cudaSuccess) {
-      release_engine(C);
+      GX_RELEASE_ENGINE(C);
       return cuda_error(err, "transport control block");
     }
     cudaStreamCreateWithFlags(&E->s1, cudaStreamNonBlocking);
@@ -2166,8 +2224,19 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   return GX_OK;
 }
 
+#ifdef GX_PARITY
+// The FP64 transport of gx_transport_run with gx_transport_config.fp64_parity
+int run_transport(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
+                  const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
+                  int *d_pstep, gx_transport_stats *stats, cudaStream_t s)
+{
+  return run<double>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_pstep, stats, s);
+}
+} // namespace parity
+#endif
 } // namespace gx
 
+#ifndef GX_PARITY
 using namespace gx;
 
 extern "C" {
@@ -2215,7 +2284,12 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
   if (cfg->geometry == 2 && nvol != C->csg_nscore)
     return set_error(GX_ERR_ARG, "gx_transport_run: nvol %d, the volume tree has %d scored touchables", nvol,
                      C->csg_nscore);
+  if (cfg->fp64_parity < 0 || cfg->fp64_parity > 1 || (cfg->fp64_parity && cfg->precision != 0))
+    return set_error(GX_ERR_ARG, "gx_transport_run: fp64_parity must be 0 or 1, and 1 needs precision 0");
   cudaSetDevice(C->device);
+  if (cfg->fp64_parity)
+    return parity::run_transport(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps,
+                                 stats, stream_of(s));
   if (cfg->precision == 1)
     return run<float>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
                       stream_of(s));
@@ -2292,10 +2366,16 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
 // Calls that overlap on the GPU (two streams, two host threads) race on it.
 // The first call on a device sets up that device (cudaGetSymbolAddress and
 // the skip-ahead table upload) and should come before any stream capture.
+// Every call synchronises its stream after each iteration (the host reads the
+// control block to decide whether to go on).  The set-up is kept for the life
+// of the process: a cudaDeviceReset while the library is loaded is not
+// supported (the array would come back zeroed without its skip-ahead table).
 namespace gx {
 
 constexpr long long kNoallocCapacity = 16384;
 constexpr int kNoallocMaxPrimaries = 4096;
+static_assert(kNoallocCapacity == GX_NOALLOC_CAPACITY && kNoallocMaxPrimaries == GX_NOALLOC_MAX_PRIMARIES,
+              "the limits of the allocation-free entry point must match gx_abi.h");
 constexpr size_t kNoallocStoreBytes = 128 * (size_t)kNoallocCapacity; // FP64 record with type field
 constexpr size_t kNoallocCtlBytes = 4096;
 constexpr size_t kNoallocCumEBytes = sizeof(double) * kNoallocMaxPrimaries;
@@ -2319,15 +2399,7 @@ static int noalloc_setup(int dev, unsigned char **out)
     cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return cuda_error(e, "gx_transport_run_noalloc: cudaGetSymbolAddress");
     uint64_t h[2][64][9];
-    const uint64_t m[2] = {4294967087ULL, 4294944443ULL};
-    for (int c = 0; c < 2; ++c) {
-      uint64_t P[9];
-      jump_matrix(c, 76, 0, P);
-      for (int b = 0; b < 64; ++b) {
-        std::memcpy(h[c][b], P, sizeof(P));
-        mat_mul(P, P, P, m[c]);
-      }
-    }
+    build_jump_host(h);
     unsigned char *base = (unsigned char *)p;
     e = cudaMemcpy(base + 3 * kNoallocStoreBytes + kNoallocCtlBytes + kNoallocCumEBytes, h, sizeof(h),
                    cudaMemcpyHostToDevice);
@@ -2488,3 +2560,4 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   if (hc.err_flags) return set_error(GX_ERR_ITERCAP, "gx_transport_run_noalloc: an iteration cap was hit");
   return GX_OK;
 }
+#endif // GX_PARITY

@@ -173,6 +173,15 @@ int gx_ioni_along_gpil(gx_ctx *ctx, int mode, int charge, const int *d_mat, cons
 int gx_ioni_along_doit(gx_ctx *ctx, int mode, int charge, const int *d_mat, const double *d_step, double *d_E,
                        double *d_edep, int n, gx_stream_t s);
 
+/* ------------------------------------------------ elementary functions */
+/* The elementary functions of the FP64 parity variant of the transport
+ * (gx_math.h: log, exp, pow, sin, cos, expm1, log1p from published methods,
+ * contraction-free, identical on the GPU and the CPU), or with lib = 1 CUDA's
+ * own, at n device arguments: fn 0 log, 1 exp, 2 pow(x, y), 3 sin, 4 cos,
+ * 5 expm1, 6 log1p.  No counterpart in the reference, whose std:: / VecCore
+ * math these stand in for; for testing the parity build. */
+int gx_math_eval(int fn, int lib, int n, const double *d_x, const double *d_y, double *d_out, gx_stream_t s);
+
 /* -------------------------------------------------------------- helix */
 /* ConstFieldHelixStepper::DoStepArr (ConstFieldHelixStepper.hpp:249-302):
  * SoA inputs and outputs; kB2C is the reference's -0.299792458e-3 for
@@ -275,6 +284,10 @@ typedef struct {
                               Runge-Kutta sub-steps, Bz ignored; 0: uniform Bz with the helix */
   int steps_per_launch_by_type[3]; /* batched engine: steps per transport launch for gamma, e-, e+
                               (0: from steps_per_launch; e+ a quarter of it, at least 1) */
+  int fp64_parity;         /* 1 (precision 0 only): the FP64 parity variant -- no contraction, the reference's
+                              spline and ionisation forms, the general helix step and the elementary functions
+                              of gx_math.h, the operations of the CPU oracle in its order, so that the two
+                              agree track by track; 0: the library's FP64 kernels */
 } gx_transport_config;
 
 typedef struct {
@@ -430,10 +443,14 @@ int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, cons
  * library (about 6.3 MB, held on every device that loads the library until the
  * process exits): at most GX_NOALLOC_MAX_PRIMARIES primaries per call, at most
  * GX_NOALLOC_CAPACITY tracks in flight plus as many deferred; larger inputs
- * are rejected with GX_ERR_ARG and a message.  precision must be 0 (FP64);
- * engine is ignored; d_edep is added to as in gx_transport_run.  Every call
- * shares the array; calls that overlap on the GPU race on it.  The first call
- * on a device sets that device up and should come before any stream capture. */
+ * are rejected with GX_ERR_ARG and a message; more tracks than that in flight
+ * and deferred at once end the call with GX_ERR_OVERFLOW (the tracks that did
+ * not fit are scored where they were).  precision must be 0 (FP64); engine is
+ * ignored; d_edep is added to as in gx_transport_run.  Every call shares the
+ * array; calls that overlap on the GPU race on it.  The first call on a device
+ * sets that device up and should come before any stream capture.  Each call
+ * synchronises its stream after every iteration.  A cudaDeviceReset while the
+ * library is loaded is not supported (the set-up is kept per process). */
 #define GX_NOALLOC_CAPACITY 16384
 #define GX_NOALLOC_MAX_PRIMARIES 4096
 int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type,

@@ -1,13 +1,14 @@
 #!/bin/sh
 # Builds oracle/_ref/libgxref.so from the reference's own hot-path sources,
-# compiled in place from a reference checkout (default: the path in
-# GX_REFERENCE_ROOT), through the headers in oracle/refshim.  Test
+# compiled in place from a reference checkout (the first argument, else
+# $GX_REFERENCE_ROOT, else a directory named `reference` beside the
+# repository), through the headers in oracle/refshim.  Test
 # infrastructure only: the library pins the oracle and generates the golden
 # vectors.  The reference's own build system is not used (it needs cmake and
 # its empty VecCore/VecGeom/PTL/timemory submodules).
 set -e
-REF=${1:-${GX_REFERENCE_ROOT:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
+REF=${1:-${GX_REFERENCE_ROOT:-$HERE/../../reference}}
 OUT="$HERE/_ref"
 SRC="$REF/source/Geant"
 if [ ! -d "$SRC" ]; then

@@ -18,7 +18,37 @@
 #ifndef GXO_H
 #define GXO_H
 
+#include <math.h>
 #include <stdint.h>
+
+/* The elementary functions of the per-step arithmetic (table lookups, models,
+ * multiple scattering, helix).  Default build (liboracle.so): the C library's,
+ * as the reference's std:: math -- this is the build pinned bit for bit
+ * against the reference.  Parity build (liboracle_gxm.so, -DGXO_OWN_MATH):
+ * the functions of gx_math.h, which the CUDA library's FP64 parity variant
+ * compiles too, so that the two round alike and agree track by track; that
+ * header is itself tested against the C library's functions to its stated
+ * error bounds.  Set-up constants (materials, table grids, the multiple-
+ * scattering material constants) stay on the C library in both builds, as in
+ * the CUDA library's host code. */
+#ifdef GXO_OWN_MATH
+#include "gx_math.h"
+#define gxo_log gxm_log
+#define gxo_exp gxm_exp
+#define gxo_pow gxm_pow
+#define gxo_sin gxm_sin
+#define gxo_cos gxm_cos
+#define gxo_expm1 gxm_expm1
+#define gxo_log1p gxm_log1p
+#else
+#define gxo_log log
+#define gxo_exp exp
+#define gxo_pow pow
+#define gxo_sin sin
+#define gxo_cos cos
+#define gxo_expm1 expm1
+#define gxo_log1p log1p
+#endif
 
 #ifdef __cplusplus
 extern "C" {

@@ -160,11 +160,11 @@ int gxo_kn_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   double E0_m = E0 / EMASS;
   double eps0 = 1. / (1. + 2. * E0_m);
   double epsilon0sq = eps0 * eps0;
-  double alpha1 = -log(eps0);
+  double alpha1 = -gxo_log(eps0);
   double alpha2 = 0.5 * (1. - epsilon0sq);
   do {
     if (alpha1 / (alpha1 + alpha2) > gxo_mrg_u01(r)) {
-      epsilon = exp(-alpha1 * gxo_mrg_u01(r));
+      epsilon = gxo_exp(-alpha1 * gxo_mrg_u01(r));
       epsilonsq = epsilon * epsilon;
     } else {
       epsilonsq = epsilon0sq + (1. - epsilon0sq) * gxo_mrg_u01(r);
@@ -177,7 +177,7 @@ int gxo_kn_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   double sinTheta = (sint2 < 0.0) ? 0.0 : sqrt(sint2);
   double phi = TWOPI * gxo_mrg_u01(r);
   double gE = epsilon * E0;
-  double gx = sinTheta * cos(phi), gy = sinTheta * sin(phi), gz = 1. - onecost;
+  double gx = sinTheta * gxo_cos(phi), gy = sinTheta * gxo_sin(phi), gz = 1. - onecost;
   gxo_rotate_to_lab(&gx, &gy, &gz, d0x, d0y, d0z);
   if (gE > low) {
     io->dir[0] = gx;
@@ -255,7 +255,7 @@ int gxo_sg_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   }
   double sint = sqrt((1 + cost) * (1 - cost));
   double phi = TWOPI * gxo_mrg_u01(r);
-  double xh = sint * cos(phi), yh = sint * sin(phi), zh = cost;
+  double xh = sint * gxo_cos(phi), yh = sint * gxo_sin(phi), zh = cost;
   gxo_rotate_to_lab(&xh, &yh, &zh, io->dir[0], io->dir[1], io->dir[2]);
   add_sec(io, 1, eE, xh, yh, zh);
   if (p->mode == GXO_MODE_PHYSICS) io->edep += gE - eE; /* binding energy, local */
@@ -268,11 +268,11 @@ int gxo_sg_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
 /* ScreenFunction1/2, ProxyBetheHeitler.hpp:184-210 */
 static double screen1(double s)
 {
-  return (s > 1.) ? 42.24 - 8.368 * log(s + 0.952) : 42.392 - s * (7.796 - 1.961 * s);
+  return (s > 1.) ? 42.24 - 8.368 * gxo_log(s + 0.952) : 42.392 - s * (7.796 - 1.961 * s);
 }
 static double screen2(double s)
 {
-  return (s > 1.) ? 42.24 - 8.368 * log(s + 0.952) : 41.405 - s * (5.828 - 0.8945 * s);
+  return (s > 1.) ? 42.24 - 8.368 * gxo_log(s + 0.952) : 41.405 - s * (5.828 - 0.8945 * s);
 }
 
 /* ProxyBetheHeitler::SampleSecondaries, ProxyBetheHeitler.hpp:64-182.  Quirk:
@@ -289,12 +289,12 @@ int gxo_bh_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   if (gE < Egsmall) {
     epsil = epsil0 + (0.5 - epsil0) * gxo_mrg_u01(r);
   } else {
-    double logZ3 = log(1.0 * (int)(Z + 0.5)) / 3.0;
+    double logZ3 = gxo_log(1.0 * (int)(Z + 0.5)) / 3.0;
     double FZ = 8. * logZ3;
     if (gE > 50. * MEV) FZ += 8. * gxo_coulomb_factor(Z);
-    double Z3 = pow(1.0 * (int)(Z + 0.5), 1 / 3.0);
+    double Z3 = gxo_pow(1.0 * (int)(Z + 0.5), 1 / 3.0);
     double screenfac = 136. * epsil0 / Z3;
-    double screenmax = exp((42.24 - FZ) / 8.368) - 0.952;
+    double screenmax = gxo_exp((42.24 - FZ) / 8.368) - 0.952;
     double screenmin = fmin(4. * screenfac, screenmax);
     double epsil1 = 0.5 - 0.5 * sqrt(1. - screenmin / screenmax);
     double epsilmin = fmax(epsil0, epsil1);
@@ -306,7 +306,7 @@ int gxo_bh_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
     double NormF2 = fmax(1.5 * F20, 0.);
     do {
       if (NormF1 / (NormF1 + NormF2) > gxo_mrg_u01(r)) {
-        epsil = 0.5 - epsilrange * pow(gxo_mrg_u01(r), 0.333333);
+        epsil = 0.5 - epsilrange * gxo_pow(gxo_mrg_u01(r), 0.333333);
         screenvar = screenfac / (epsil * (1 - epsil));
         greject = (screen1(screenvar) - FZ) / F10;
       } else {
@@ -320,18 +320,18 @@ int gxo_bh_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   double pTot = gE - eTot;
   double u1 = gxo_mrg_u01(r);
   double u2 = gxo_mrg_u01(r);
-  double aa0 = -log(u1 * u2);
+  double aa0 = -gxo_log(u1 * u2);
   double u = (0.25 > gxo_mrg_u01(r)) ? aa0 / 0.625 : aa0 / 1.875;
   double phi = TWOPI * gxo_mrg_u01(r);
-  double cosp = cos(phi), sinp = sin(phi);
+  double cosp = gxo_cos(phi), sinp = gxo_sin(phi);
   double cost = u * EMASS / eTot;
-  if (p->mode == GXO_MODE_PHYSICS) cost = cos(cost);
+  if (p->mode == GXO_MODE_PHYSICS) cost = gxo_cos(cost);
   double sint = sqrt((1. - cost) * (1. + cost));
   double xh = sint * cosp, yh = sint * sinp, zh = cost;
   gxo_rotate_to_lab(&xh, &yh, &zh, io->dir[0], io->dir[1], io->dir[2]);
   add_sec(io, 1, eTot - EMASS, xh, yh, zh);
   cost = u * EMASS / pTot;
-  if (p->mode == GXO_MODE_PHYSICS) cost = cos(cost);
+  if (p->mode == GXO_MODE_PHYSICS) cost = gxo_cos(cost);
   sint = sqrt((1. - cost) * (1. + cost));
   xh = -sint * cosp;
   yh = -sint * sinp;
@@ -354,15 +354,15 @@ static void sb_photon_direction(gxo_mrg_t *r, double energyIn, double *dx, doubl
   double signc = (c < 0) ? -1 : 1;
   double a = fabs(c);
   double delta = 0.5 * (sqrt(4.0 + a * a) + a);
-  double cofA = -signc * pow(delta, 1.0 / 3.0);
+  double cofA = -signc * gxo_pow(delta, 1.0 / 3.0);
   double cosTheta = cofA - 1.0 / cofA;
   double tau = energyIn / EMASS;
   double beta = sqrt(tau * (tau + 2.0)) / (tau + 1.0);
   cosTheta = (cosTheta + beta) / (1.0 + cosTheta * beta);
   double sinTheta = sqrt((1.0 - cosTheta) * (1.0 + cosTheta));
   double phi = TWOPI * gxo_mrg_u01(r);
-  *dx = sinTheta * cos(phi);
-  *dy = sinTheta * sin(phi);
+  *dx = sinTheta * gxo_cos(phi);
+  *dy = sinTheta * gxo_sin(phi);
   *dz = cosTheta;
 }
 
@@ -378,9 +378,9 @@ int gxo_sb_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   const gxo_sb_t *T = p->sb;
   double totalEnergy = kin + EMASS;
   double densityCorr = p->density_factor * totalEnergy * totalEnergy;
-  double xmin = log(cut * cut + densityCorr);
-  double xmax = log(emax * emax + densityCorr);
-  double y = log(kin / MEV);
+  double xmin = gxo_log(cut * cut + densityCorr);
+  double xmax = gxo_log(emax * emax + densityCorr);
+  double y = gxo_log(kin / MEV);
   double x0 = cut / kin;
   double vmax = gxo_sb_value(T, x0, y) * 1.02;
   double epeaklimit = 300 * MEV, elowlimit = 10 * KEV;
@@ -392,7 +392,7 @@ int gxo_sb_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
   double gE = 0, v;
   do {
     double auxrand = gxo_mrg_u01(r);
-    double x = exp(xmin + auxrand * (xmax - xmin)) - densityCorr;
+    double x = gxo_exp(xmin + auxrand * (xmax - xmin)) - densityCorr;
     if (x < 0.0) x = 0.0;
     gE = sqrt(x);
     double x1 = gE / kin;
@@ -444,7 +444,7 @@ static void delta_ray(gxo_mrg_t *r, gxo_inter_t *io, double kin, double x)
   if (cost > 1.0) cost = 1.0;
   double sint = sqrt((1.0 - cost) * (1. + cost));
   double phi = TWOPI * gxo_mrg_u01(r);
-  double xh = sint * cos(phi), yh = sint * sin(phi), zh = cost;
+  double xh = sint * gxo_cos(phi), yh = sint * gxo_sin(phi), zh = cost;
   gxo_rotate_to_lab(&xh, &yh, &zh, io->dir[0], io->dir[1], io->dir[2]);
   add_sec(io, 1, deltaKin, xh, yh, zh);
   io->E -= deltaKin;
@@ -530,7 +530,7 @@ double gxo_annih_xs_per_electron(double kin)
   double gamma2 = gam * gam;
   double bg2 = tau * (tau + 2.0);
   double bg = sqrt(bg2);
-  return g_pi_rcl2 * ((gamma2 + 4 * gam + 1.) * log(gam + bg) - (gam + 3.) * bg) / (bg2 * (gam + 1.));
+  return g_pi_rcl2 * ((gamma2 + 4 * gam + 1.) * gxo_log(gam + bg) - (gam + 3.) * bg) / (bg2 * (gam + 1.));
 }
 
 /* Two-photon annihilation (Geant4 eeToTwoGamma sampling, published algorithm).
@@ -544,7 +544,7 @@ int gxo_annih_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
     double cost = 2. * gxo_mrg_u01(r) - 1.;
     double sint = sqrt((1. - cost) * (1. + cost));
     double phi = TWOPI * gxo_mrg_u01(r);
-    double dx = sint * cos(phi), dy = sint * sin(phi), dz = cost;
+    double dx = sint * gxo_cos(phi), dy = sint * gxo_sin(phi), dz = cost;
     add_sec(io, 0, EMASS, dx, dy, dz);
     add_sec(io, 0, EMASS, -dx, -dy, -dz);
   } else {
@@ -558,7 +558,7 @@ int gxo_annih_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
     double epsilqot = epsilmax / epsilmin;
     double epsil, greject;
     do {
-      epsil = epsilmin * exp(log(epsilqot) * gxo_mrg_u01(r));
+      epsil = epsilmin * gxo_exp(gxo_log(epsilqot) * gxo_mrg_u01(r));
       greject = 1. - epsil + (2. * gam * epsil - 1.) / (epsil * tau2 * tau2);
     } while (greject < gxo_mrg_u01(r));
     double cost = (epsil * tau2 - 1.) / (epsil * sqg2m1);
@@ -568,7 +568,7 @@ int gxo_annih_sample(gxo_mrg_t *r, const gxo_model_params_t *p, gxo_inter_t *io)
     double phi = TWOPI * gxo_mrg_u01(r);
     double tot = kin + 2.0 * EMASS;
     double e1 = epsil * tot, e2 = (1. - epsil) * tot;
-    double dx = sint * cos(phi), dy = sint * sin(phi), dz = cost;
+    double dx = sint * gxo_cos(phi), dy = sint * gxo_sin(phi), dz = cost;
     gxo_rotate_to_lab(&dx, &dy, &dz, io->dir[0], io->dir[1], io->dir[2]);
     double pp = sqrt(kin * (kin + 2. * EMASS));
     double ex = pp * io->dir[0] - e1 * dx, ey = pp * io->dir[1] - e1 * dy, ez = pp * io->dir[2] - e1 * dz;
@@ -660,7 +660,7 @@ double gxo_post_step_gpil(gxo_mrg_t *r, double lambda, double pstep_prev, double
                           double *inv_lambda_saved)
 {
   if (*nil <= 0.0)
-    *nil = -log(gxo_mrg_u01(r));
+    *nil = -gxo_log(gxo_mrg_u01(r));
   else
     *nil -= pstep_prev / *inv_lambda_saved;
   double step = *nil / lambda;
@@ -718,7 +718,7 @@ void gxo_ioni_along_doit(const gxo_data_t *d, int mode, int charge, int mat, dou
       else if (range >= iv->emax)
         einv = iv->y[iv->n - 1];
       else {
-        int bin = (int)(log(range) / iv->dbin - iv->base);
+        int bin = (int)(gxo_log(range) / iv->dbin - iv->base);
         if (bin > 0 && range < iv->x[bin]) --bin;
         if (bin < 0) bin = 0;
         if (bin > iv->n - 2) bin = iv->n - 2;
@@ -766,7 +766,7 @@ static void helix_core(double kB2C, const double B[3], const double pos[3], cons
   unit3(&vx, &vy, &vz);
   double cx = vy * uz - vz * uy, cy = vz * ux - vx * uz, cz = vx * uy - vy * ux;
   double phi = -step * charge * Bmag * kB2C / momentum;
-  double sinphi = sin(phi), cosphi = cos(phi);
+  double sinphi = gxo_sin(phi), cosphi = gxo_cos(phi);
   np[0] = pos[0] + R * (cosphi - 1) * cx - R * sinphi * vx + step * UVdotUB * ux;
   np[1] = pos[1] + R * (cosphi - 1) * cy - R * sinphi * vy + step * UVdotUB * uy;
   np[2] = pos[2] + R * (cosphi - 1) * cz - R * sinphi * vz + step * UVdotUB * uz;

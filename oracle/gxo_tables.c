@@ -97,7 +97,7 @@ static int retrieve_vector(FILE *f, gxo_pvec_t *v)
 /* FindBinLocation, ProxyPhysicsVector.cu:388-394 */
 static int find_bin(const gxo_pvec_t *v, double e)
 {
-  int bin = (int)(log(e) / v->dbin - v->base);
+  int bin = (int)(gxo_log(e) / v->dbin - v->base);
   /* the reference reads outside the vector when the grid is not logarithmic
    * (InverseRange tables); the oracle keeps the bin inside it */
   if (bin > v->n - 2) bin = v->n - 2;

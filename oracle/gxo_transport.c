@@ -323,14 +323,14 @@ static double msc_range(const world_t *w, int type, int mat, double e)
 static double msc_true_to_geom(double t, double lam)
 {
   double tau = t / lam;
-  return tau < MSC_TAULIM ? t : -lam * expm1(-tau);
+  return tau < MSC_TAULIM ? t : -lam * gxo_expm1(-tau);
 }
 
 static double msc_geom_to_true(double z, double lam, double tmax)
 {
   double x = z / lam;
   if (x < MSC_TAULIM) return z;
-  double t = x < 1.0 ? -lam * log1p(-x) : tmax;
+  double t = x < 1.0 ? -lam * gxo_log1p(-x) : tmax;
   return t < tmax ? t : tmax;
 }
 
@@ -340,7 +340,7 @@ static double msc_simple(gxo_mrg_t *r, double xm, double x2m)
   double a = (2 * xm + 9 * x2m - 3) / (2 * xm - 3 * x2m + 1);
   double prob = (a + 2) * xm / a;
   double r0 = gxo_mrg_u01(r), r1 = gxo_mrg_u01(r);
-  if (r0 < prob) return -1 + 2 * exp(log(r1) / (a + 1));
+  if (r0 < prob) return -1 + 2 * gxo_exp(gxo_log(r1) / (a + 1));
   return -1 + 2 * r1;
 }
 
@@ -350,7 +350,7 @@ static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, dou
                             double e1)
 {
   double tau = t / lam0;
-  if (lam1 > 0.0 && fabs(lam1 - lam0) > 0.01 * lam0) tau = t * log(lam0 / lam1) / (lam0 - lam1);
+  if (lam1 > 0.0 && fabs(lam1 - lam0) > 0.01 * lam0) tau = t * gxo_log(lam0 / lam1) / (lam0 - lam1);
   if (tau >= MSC_TAUBIG) return -1 + 2 * gxo_mrg_u01(r);
   if (tau < MSC_TAUSMALL) return 1.0;
   double xm, x2m;
@@ -358,25 +358,25 @@ static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, dou
     xm = 1 - tau * (1 - 0.5 * tau);
     x2m = 1 - tau * (5 - 6.25 * tau) / 3;
   } else {
-    xm = exp(-tau);
-    x2m = (1 + 2 * exp(-2.5 * tau)) / 3;
+    xm = gxo_exp(-tau);
+    x2m = (1 + 2 * gxo_exp(-2.5 * tau)) / 3;
   }
   if (1.0 - e1 / e0 > 0.5) return msc_simple(r, xm, x2m);
   /* Highland-type width with the model's Z-dependent correction; 1 / (beta c p)
    * taken at the geometric mean of the start and end energies */
   double inv0 = (e0 + EMASS) / (e0 * (e0 + 2 * EMASS)), inv1 = (e1 + EMASS) / (e1 * (e1 + 2 * EMASS));
   double y = t / m->X0;
-  double th0 = 13.6 * sqrt(y) * sqrt(inv0 * inv1) * (m->th1 + m->th2 * log(y));
+  double th0 = 13.6 * sqrt(y) * sqrt(inv0 * inv1) * (m->th1 + m->th2 * gxo_log(y));
   double th2 = th0 * th0;
   if (th2 < MSC_TAUSMALL) return 1.0;
   if (th0 > PI / 6) return msc_simple(r, xm, x2m);
   double x = th2 * (1 - th2 / 12);
   if (th2 > 0.01) {
-    double s = 2 * sin(0.5 * th0);
+    double s = 2 * gxo_sin(0.5 * th0);
     x = s * s;
   }
-  double u = exp(log(tau) / 6);
-  double xsi = m->ca + u * (m->cb + m->cc * u) + m->cd * log((t / tau) / m->X0);
+  double u = gxo_exp(gxo_log(tau) / 6);
+  double xsi = m->ca + u * (m->cb + m->cc * u) + m->cd * gxo_log((t / tau) / m->X0);
   if (xsi < 1.9) xsi = 1.9;
   double c = xsi;
   if (fabs(c - 3) < 0.001)
@@ -384,12 +384,12 @@ static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, dou
   else if (fabs(c - 2) < 0.001)
     c = 2.001;
   double c1 = c - 1;
-  double ea = exp(-xsi), eaa = 1 - ea;
+  double ea = gxo_exp(-xsi), eaa = 1 - ea;
   double xmean1 = 1 - (1 - (1 + xsi) * ea) * x / eaa;
   if (xmean1 <= 0.999 * xm) return msc_simple(r, xm, x2m);
   double x0 = 1 - xsi * x;
   double b = 1 + (c - xsi) * x, b1 = b + 1, bx = c * x;
-  double d = exp(c1 * log(bx)) / exp(c1 * log(b1));
+  double d = gxo_exp(c1 * gxo_log(bx)) / gxo_exp(c1 * gxo_log(b1));
   double xmean2 = (x0 + d - (bx - b1 * d) / (c - 2)) / (1 - d);
   double f1x0 = ea / eaa, f2x0 = c1 / (c * (1 - d));
   double prob = f2x0 / (f1x0 + f2x0);
@@ -403,13 +403,13 @@ static double msc_cos_theta(gxo_mrg_t *r, const struct msc_mat *m, double t, dou
   }
   double r0 = gxo_mrg_u01(r), r1 = gxo_mrg_u01(r);
   if (r0 < qprob) {
-    if (r1 < prob) return 1 + log(ea + gxo_mrg_u01(r) * eaa) * x;
+    if (r1 < prob) return 1 + gxo_log(ea + gxo_mrg_u01(r) * eaa) * x;
     double var = (1 - d) * gxo_mrg_u01(r);
     if (var < 0.01 * d) {
       var /= d * c1;
       return -1 + var * (1 - 0.5 * var * c) * (2 + (c - xsi) * x);
     }
-    return 1 + x * (c - xsi - c * exp(-log(var + d) / c1));
+    return 1 + x * (c - xsi - c * gxo_exp(-gxo_log(var + d) / c1));
   }
   return -1 + 2 * r1;
 }
@@ -424,7 +424,7 @@ static int msc_deflect(const world_t *w, track_t *tr, int mat, double t, double 
   if (ct < -1.0) ct = -1.0;
   double st = sqrt((1 - ct) * (1 + ct));
   double phi = TWOPI * gxo_mrg_u01(&tr->rng);
-  double u = st * cos(phi), v = st * sin(phi), z = ct;
+  double u = st * gxo_cos(phi), v = st * gxo_sin(phi), z = ct;
   gxo_rotate_to_lab(&u, &v, &z, tr->dir[0], tr->dir[1], tr->dir[2]);
   tr->dir[0] = u;
   tr->dir[1] = v;
@@ -641,7 +641,7 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
   double xs[3];
   cross_sections(w, tr->type, mat, tr->E, xs);
   for (int i = 0; i < np; ++i)
-    if (tr->nil[i] <= 0.0) tr->nil[i] = -log(gxo_mrg_u01(&tr->rng));
+    if (tr->nil[i] <= 0.0) tr->nil[i] = -gxo_log(gxo_mrg_u01(&tr->rng));
   double pstep = DBL_MAX;
   int sel = -1;
   for (int i = 0; i < np; ++i)
@@ -736,7 +736,7 @@ static int one_step(const world_t *w, track_t *tr, stack_t *st, tally_t *t)
         const double saf = rmax2 > 0.0 ? safety(w, tr->vol, tr->pos) : 0.0;
         if (saf > MSC_TMIN) {
           double r = fmin(0.73 * sqrt(rmax2), 0.99 * saf);
-          double u = cos(phi), v = sin(phi), z = 0.0;
+          double u = gxo_cos(phi), v = gxo_sin(phi), z = 0.0;
           gxo_rotate_to_lab(&u, &v, &z, d0, d1, d2);
           tr->pos[0] += r * u;
           tr->pos[1] += r * v;

@@ -28,6 +28,14 @@ def oracle():
 
 
 @pytest.fixture(scope="session")
+def oracle_gxm():
+    """The oracle's parity build (gx_math.h's elementary functions)."""
+    _ensure_oracle()
+    from oracle_ctypes import ORACLE_GXM_SO, Oracle
+    return Oracle(ORACLE_GXM_SO)
+
+
+@pytest.fixture(scope="session")
 def golden():
     import numpy as np
     d = os.path.join(HERE, "golden")

@@ -7,7 +7,8 @@ field map at run time from
 ``source/Geant/proxy/test/BasicCpuTransport/data/`` (see
 ``source/Geant/proxy/src/ProxyDataManager.cu:49-122`` and
 ``source/Geant/proxy/ProxySeltzerBerger.hpp:134-152``).  This script copies
-the subset this framework loads into this directory, unchanged, and extracts
+the subset this framework loads into the package's data directory
+(``geantexascalepilot_b200/data``), unchanged, and extracts
 the atomic-shell and Sandia photo-absorption arrays that the reference keeps
 as C++ data tables in ``source/Geant/proxy/ProxySandiaData.hpp`` into a plain
 text file (``sandia.dat``) so that nothing here has to include reference code.
@@ -22,7 +23,8 @@ import re
 import shutil
 import sys
 
-HERE = os.path.dirname(os.path.abspath(__file__))
+HERE = os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                    "geantexascalepilot_b200", "data")
 
 TABLES = [
     "DEDX.eBrem.e-.asc", "DEDX.eBrem.e+.asc", "DEDX.eIoni.e-.asc", "DEDX.eIoni.e+.asc",

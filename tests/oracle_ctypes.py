@@ -14,9 +14,19 @@ import numpy as np
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 DATA_DIR = os.path.join(REPO, "geantexascalepilot_b200", "data")
 ORACLE_SO = os.path.join(REPO, "oracle", "liboracle.so")
+# the parity build: the same oracle with the elementary functions of the CUDA
+# library's FP64 parity variant (gx_math.h), for track-by-track comparisons
+ORACLE_GXM_SO = os.path.join(REPO, "oracle", "liboracle_gxm.so")
 REF_SO = os.path.join(REPO, "oracle", "_ref", "libgxref.so")
-REF_DATA_CWD = os.path.join(os.environ.get("GX_REFERENCE_ROOT", "/root/reference"),
-                            "source/Geant/proxy/test/BasicCpuTransport")
+
+
+def reference_root():
+    """The reference checkout: $GX_REFERENCE_ROOT, else a directory named
+    `reference` beside this repository."""
+    return os.environ.get("GX_REFERENCE_ROOT", os.path.join(os.path.dirname(REPO), "reference"))
+
+
+REF_DATA_CWD = os.path.join(reference_root(), "source/Geant/proxy/test/BasicCpuTransport")
 
 P = C.c_void_p
 D = C.c_double
@@ -99,9 +109,24 @@ class Oracle:
         lib.gxo_transport_flat.argtypes = [P, C.POINTER(Config), I, C.POINTER(I), C.POINTER(D), C.POINTER(D),
                                            C.POINTER(D), C.POINTER(I), C.POINTER(D), I, C.POINTER(D),
                                            C.POINTER(C.c_longlong), C.POINTER(I)]
+        for f in ("gxo_gxm_eval", "gxo_libm_eval"):
+            getattr(lib, f).argtypes = [I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
         self.data = lib.gxo_data_load(datadir.encode())
         if not self.data:
             raise RuntimeError("oracle could not load physics data from %s" % datadir)
+
+    # --------------------------------------------- elementary functions
+    MATH_FUNCS = {"log": 0, "exp": 1, "pow": 2, "sin": 3, "cos": 4, "expm1": 5, "log1p": 6}
+
+    def math_eval(self, name, x, y=None, libm=False):
+        """gx_math.h's function `name` (libm=False) or the C library's, at x
+        (and y for pow)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.ascontiguousarray(np.zeros_like(x) if y is None else y, dtype=np.float64)
+        out = np.zeros_like(x)
+        f = self.lib.gxo_libm_eval if libm else self.lib.gxo_gxm_eval
+        f(self.MATH_FUNCS[name], len(x), dp(x), dp(y), dp(out))
+        return out
 
     # ------------------------------------------------------------ RNG
     def mrg_draws(self, states, k):
