@@ -13,5 +13,6 @@ from .api import (ANNIHILATION, BETHE_HEITLER, BHABHA, ELECTRON, GAMMA, KLEIN_NI
                   ProxyMollerScattering, ProxyPhotoElectric, ProxySauterGavrila, ProxySeltzerBerger, autotune,
                   cut_convert, default_config, egamma_gun, hepevt_load, hepevt_read, math_eval, pdg_to_type,
                   set_direction_xyz,
-                  spot_gun, transport, transport_host, transport_noalloc)
+                  spot_gun, transport, transport_host, transport_noalloc, TrackSoA, gpil, propagate, along_step,
+                  post_step, transport_tracks)
 from . import configs, geometry, sharding  # noqa: F401

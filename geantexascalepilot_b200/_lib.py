@@ -46,6 +46,15 @@ class TransportConfig(C.Structure):
                 ("field_map", I), ("steps_per_launch_by_type", I * 3), ("fp64_parity", I)]
 
 
+class TrackSoAStruct(C.Structure):
+    """gx_track_soa (include/gx_abi.h): device pointers of the SoA fields."""
+    _fields_ = ([("n", I), ("capacity", I)] +
+                [(f, P) for f in ("type", "status", "event", "primary", "volume", "next_volume", "process",
+                                  "boundary", "x", "y", "z", "dx", "dy", "dz", "ekin", "nil0", "nil1", "nil2",
+                                  "lambda_inv0", "lambda_inv1", "lambda_inv2", "pstep", "step", "snext", "safety",
+                                  "msc_range", "rng")])
+
+
 class TransportStats(C.Structure):
     _fields_ = [("steps", LL), ("substeps", LL), ("tracks", LL), ("secondaries", LL * 3), ("n_pair", LL),
                 ("n_annih", LL), ("errors", LL), ("escaped", D), ("iterations", LL), ("peak_in_flight", LL),
@@ -120,6 +129,13 @@ _SIGS = {
     "gx_ioni_along_doit": (I, [P, I, I, P, P, P, P, I, P]),
     "gx_helix_dostep": (I, [PD, D, I] + [P] * 15 + [P]),
     "gx_math_eval": (I, [I, I, I, P, P, P, P]),
+    "gx_gpil": (I, [P, C.POINTER(TransportConfig), C.POINTER(TrackSoAStruct), P]),
+    "gx_propagate": (I, [P, C.POINTER(TransportConfig), C.POINTER(TrackSoAStruct), P]),
+    "gx_along_step": (I, [P, C.POINTER(TransportConfig), C.POINTER(TrackSoAStruct), P, I, P]),
+    "gx_post_step": (I, [P, C.POINTER(TransportConfig), C.POINTER(TrackSoAStruct), C.POINTER(TrackSoAStruct), P, I,
+                         P]),
+    "gx_transport_tracks": (I, [P, C.POINTER(TransportConfig), C.POINTER(TrackSoAStruct), I,
+                                C.POINTER(TrackSoAStruct), P, I, C.POINTER(TransportStats), P]),
     "gx_transport_config_default": (None, [C.POINTER(TransportConfig)]),
     "gx_transport_run": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P, C.POINTER(TransportStats), P]),
     "gx_transport_run_host": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, P, I, P,

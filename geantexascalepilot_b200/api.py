@@ -14,7 +14,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from ._lib import AutotuneReport, GunParams, GxError, ModelParams, TransportConfig, TransportStats, check, lib
+from ._lib import (AutotuneReport, GunParams, GxError, ModelParams, TrackSoAStruct, TransportConfig, TransportStats,
+                   check, lib)
 
 # physics-table ids (ProxyPhysicsTableIndex.hpp:23-45)
 TABLES = ["DEDX.eBrem.e-", "DEDX.eBrem.e+", "DEDX.eIoni.e-", "DEDX.eIoni.e+", "InverseRange.eIoni.e-",
@@ -306,6 +307,125 @@ class ConstFieldHelixStepper:
         check(lib.gx_helix_dostep(self.B, self.kB2C, n, *[_ptr(c) for c in cols], _ptr(q), _ptr(p), _ptr(s),
                                   *[_ptr(o) for o in outs], _stream()))
         return torch.stack(outs[:3], 1), torch.stack(outs[3:], 1)
+
+
+# ------------------------------------------------------- tracks in SoA form
+TRACK_ALIVE, TRACK_KILLED, TRACK_INTERACT, TRACK_EXITED = 0, 1, 2, 3
+
+
+class TrackSoA:
+    """A batch of tracks in SoA form (gx_track_soa): the hot fields of the
+    reference's TrackState as the arrays of a TrackCollection
+    (source/Geant/track/TrackState.hpp:30-232, TrackCollection.hpp:23-42),
+    one CUDA tensor per field, `capacity` entries, the first `n` tracks.
+    rng holds the MRG32k3a states as six planes of `capacity` uint32 words."""
+
+    INT_FIELDS = ("type", "status", "event", "primary", "volume", "next_volume", "process", "boundary")
+    DBL_FIELDS = ("x", "y", "z", "dx", "dy", "dz", "ekin", "nil0", "nil1", "nil2", "lambda_inv0", "lambda_inv1",
+                  "lambda_inv2", "pstep", "step", "snext", "safety", "msc_range")
+
+    def __init__(self, capacity, device="cuda"):
+        self.capacity = int(capacity)
+        self.n = 0
+        for f in self.INT_FIELDS:
+            setattr(self, f, torch.zeros(self.capacity, dtype=torch.int32, device=device))
+        for f in self.DBL_FIELDS:
+            setattr(self, f, torch.zeros(self.capacity, dtype=torch.float64, device=device))
+        self.rng = torch.zeros(6 * self.capacity, dtype=torch.int32, device=device)
+
+    @classmethod
+    def from_primaries(cls, cfg, types, E, pos, direction, events=None, capacity=None, first_substream=None):
+        """Primaries as tracks: stream = substream (first_substream + i) of
+        cfg.seed (cfg.first_substream by default), NIL to be drawn, volume to
+        be located -- the state gx_transport_run gives a primary."""
+        n = len(types)
+        t = cls(capacity or n)
+        t.n = n
+        t.type[:n] = torch.as_tensor(np.asarray(types), dtype=torch.int32)
+        t.status[:n] = TRACK_ALIVE
+        if events is not None:
+            t.event[:n] = torch.as_tensor(np.asarray(events), dtype=torch.int32)
+        t.primary[:n] = torch.arange(n, dtype=torch.int32)
+        t.volume[:n] = -2
+        p = np.asarray(pos, dtype=np.float64).reshape(n, 3)
+        d = np.asarray(direction, dtype=np.float64).reshape(n, 3)
+        for k, f in enumerate(("x", "y", "z")):
+            getattr(t, f)[:n] = torch.as_tensor(p[:, k])
+        for k, f in enumerate(("dx", "dy", "dz")):
+            getattr(t, f)[:n] = torch.as_tensor(d[:, k])
+        t.ekin[:n] = torch.as_tensor(np.asarray(E, dtype=np.float64))
+        for f in ("nil0", "nil1", "nil2", "msc_range"):
+            getattr(t, f)[:n] = -1.0
+        first = cfg.first_substream if first_substream is None else first_substream
+        st = torch.zeros(6 * n, dtype=torch.int32, device="cuda")
+        check(lib.gx_rng_substreams((C.c_double * 6)(*cfg.seed), int(first), n, _ptr(st), _stream()))
+        t.rng.view(6, t.capacity)[:, :n] = st.view(6, n)
+        return t
+
+    def struct(self):
+        s = TrackSoAStruct()
+        s.n, s.capacity = self.n, self.capacity
+        for f in self.INT_FIELDS + self.DBL_FIELDS + ("rng",):
+            setattr(s, f, getattr(self, f).data_ptr())
+        return s
+
+    def numpy(self):
+        """The first n tracks as host arrays (rng as n x 6 uint32 words)."""
+        n = self.n
+        out = {f: getattr(self, f)[:n].cpu().numpy() for f in self.INT_FIELDS + self.DBL_FIELDS}
+        out["rng"] = self.rng.view(6, self.capacity)[:, :n].cpu().numpy().view(np.uint32).T.copy()
+        return out
+
+
+def _stage(fn, dm, cfg, tracks, *extra):
+    s = tracks.struct()
+    check(fn(dm.handle, C.byref(cfg), C.byref(s), *extra))
+    return s
+
+
+def gpil(dm, cfg, tracks):
+    """gx_gpil: PostStepGPIL of the discrete processes, range limit and
+    FindNextBoundary for the ALIVE tracks (FP64; cfg.fp64_parity selects the
+    parity variant)."""
+    _stage(lib.gx_gpil, dm, cfg, tracks, _stream())
+
+
+def propagate(dm, cfg, tracks):
+    """gx_propagate: the move by the proposed step (straight or helix)."""
+    _stage(lib.gx_propagate, dm, cfg, tracks, _stream())
+
+
+def along_step(dm, cfg, tracks, edep):
+    """gx_along_step: NIL update, continuous loss into edep [nevents, nvol],
+    outcome of the step."""
+    _stage(lib.gx_along_step, dm, cfg, tracks, _ptr(edep), edep.shape[1], _stream())
+
+
+def post_step(dm, cfg, tracks, secondaries, edep):
+    """gx_post_step: the interactions of the INTERACT tracks; secondaries of
+    track i at entries 2i, 2i+1 of `secondaries` (capacity >= 2 n)."""
+    t, sec = tracks.struct(), secondaries.struct()
+    check(lib.gx_post_step(dm.handle, C.byref(cfg), C.byref(t), C.byref(sec), _ptr(edep), edep.shape[1],
+                           _stream()))
+    secondaries.n = sec.n
+
+
+def transport_tracks(dm, cfg, tracks, max_iterations=0, out=None, edep=None, nvol=None):
+    """gx_transport_tracks: the engine started from `tracks`, stopped after
+    max_iterations iterations (0: to completion); returns (out TrackSoA with
+    the tracks still alive, edep, stats)."""
+    if nvol is None:
+        nvol = 2 * cfg.nlayers if cfg.geometry == 1 else 1
+    if edep is None:
+        edep = torch.zeros((cfg.nevents, nvol), dtype=torch.float64, device="cuda")
+    if out is None:
+        out = TrackSoA(max(1024, 64 * max(1, tracks.n)))
+    si, so = tracks.struct(), out.struct()
+    st = TransportStats()
+    check(lib.gx_transport_tracks(dm.handle, C.byref(cfg), C.byref(si), int(max_iterations), C.byref(so),
+                                  _ptr(edep), nvol, C.byref(st), _stream()))
+    out.n = so.n
+    return out, edep, st.as_dict()
 
 
 MATH_FUNCS = {"log": 0, "exp": 1, "pow": 2, "sin": 3, "cos": 4, "expm1": 5, "log1p": 6}

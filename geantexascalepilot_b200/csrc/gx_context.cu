@@ -222,7 +222,7 @@ static void material(Data &d, int m, double Z, double A, double density, double 
   d.mat_Z[m] = Z;
   d.mat_density[m] = density;
   d.mat_nel[m] = Z * n_atoms;
-  d.mat_dfactor[m] = d.mat_nel[m] * 4.0 * kPi * rcl * lc * lc; // Migdal constant x n_el
+  d.mat_dfactor[m] = d.mat_nel[m] * (4.0 * kPi * rcl * lc * lc); // n_el x the Migdal constant
   // radiation length (ProxyMaterial::ComputeDerivedQuantities, ProxyMaterial.cu:133-150)
   const double radinv = n_atoms * lrad_tsai_factor(Z, alpha, rcl);
   // the Urban model's Z-dependent constants: the theta0 correction and the

@@ -27,6 +27,7 @@ struct Ctx {
   int *csg_kids = nullptr, *csg_score = nullptr, *csg_slab = nullptr, *csg_cand = nullptr;
   double *csg_planes = nullptr;
   int csg_n = 0, csg_nscore = 0;
+  double *stage_scratch = nullptr; // escaped energy of the stage calls (gx_along_step)
 };
 
 int set_error(int code, const char *fmt, ...);
@@ -38,7 +39,15 @@ void build_jump_host(uint64_t h[2][64][9]);
 void release_engine(Ctx *c);
 int launch_substreams(const double seed[6], long long first, int n, uint32_t *d_states, cudaStream_t s);
 int get_jump_table(uint64_t **out);
+int run_stage(int stage, Ctx *C, const gx_transport_config *cfg, gx_track_soa *t, gx_track_soa *sec, double *d_edep,
+              int nvol, cudaStream_t s);
+int run_tracks(Ctx *C, const gx_transport_config *cfg, const gx_track_soa *in, int max_iter, gx_track_soa *out,
+               double *d_edep, int nvol, gx_transport_stats *stats, cudaStream_t s);
 namespace parity {
+int run_stage(int stage, Ctx *C, const gx_transport_config *cfg, gx_track_soa *t, gx_track_soa *sec, double *d_edep,
+              int nvol, cudaStream_t s);
+int run_tracks(Ctx *C, const gx_transport_config *cfg, const gx_track_soa *in, int max_iter, gx_track_soa *out,
+               double *d_edep, int nvol, gx_transport_stats *stats, cudaStream_t s);
 void release_engine(Ctx *c);
 int run_transport(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
                   const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,

@@ -83,11 +83,21 @@ struct Ctl {
   unsigned long long stat[kNStat];
   double escaped;
   double retired;     // energy deposited or escaped so far (the rest is still carried by tracks)
+  long long extracted; // tracks written out by gx_transport_tracks
   const double *cumE; // inclusive prefix sum of the primary energies
   double wave_energy; // energy carried by live tracks before more primaries are injected, at most
   long long refill_below, stack_cap;
   long long qcount[3][3]; // records in the interaction buffers [particle][process]
   long long take[3];      // tracks of the current stores handed out to the transport kernels
+};
+
+// Tracks handed in as a gx_track_soa (gx_transport_tracks) instead of
+// primaries: injected with their state as it is.
+struct SoaIn {
+  const int *type, *status, *event, *primary, *volume;
+  const double *x, *y, *z, *dx, *dy, *dz, *ekin, *nil0, *nil1, *nil2, *msc;
+  const uint32_t *rng;
+  long long cap;
 };
 
 struct Prims {
@@ -96,6 +106,8 @@ struct Prims {
   double seed[6];
   long long first_substream;
   const uint64_t *jump;
+  int from_soa; // 1: inject the tracks of soa
+  SoaIn soa;
 };
 
 template <class R> struct Args {
@@ -756,12 +768,13 @@ template <class R> struct GammaXs {
   int have; // bit 0: lead (material 1), bit 1: argon (material 2)
 };
 
-// GPIL and step limit.  Returns true when the step continues with helix
-// sub-steps (a charged track in a field), false when it is complete.  gx,
-// when given, caches a photon's cross sections per material.
+// GPIL and step limit (PostStepGPIL of the discrete processes, the range and
+// multiple-scattering limits): returns the step to move (geometric length),
+// and sets the step context.  gx, when given, caches a photon's cross
+// sections per material.
 template <class R, int K>
-__device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c,
-                                           GammaXs<R> *gx = nullptr)
+__device__ __forceinline__ R step_gpil(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c,
+                                       GammaXs<R> *gx = nullptr)
 {
   const int mat = vol_material(g, t.vol);
   const int np = (t.type == 1) ? 2 : 3;
@@ -842,7 +855,16 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
   c.newvol = t.vol;
   c.crossed = false;
   c.nsub = 0;
-  if (charged && (g.Bz != 0.0 || g.field_map)) {
+  return pstep;
+}
+
+// The start of the move by pstep: true when the step continues with helix
+// sub-steps (a charged track in a field); otherwise the straight move to pstep
+// or the first boundary is made here and false returned.
+template <class R, int K>
+__device__ __forceinline__ bool step_move_begin(const Geom &g, Track<R> &t, StepCtx<R> &c, R pstep)
+{
+  if (t.type != 0 && (g.Bz != 0.0 || g.field_map)) {
     c.remaining = (double)pstep;
     c.total = 0.0;
     return true;
@@ -871,6 +893,17 @@ __device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R
     for (int k = 0; k < 3; ++k) t.pos[k] += ps * dir[k];
   }
   return false;
+}
+
+// GPIL, step limit and the start of the move.  Returns true when the step
+// continues with helix sub-steps (a charged track in a field), false when it
+// is complete.
+template <class R, int K>
+__device__ __forceinline__ bool step_begin(const Data &d, const Geom &g, Track<R> &t, StepCtx<R> &c,
+                                           GammaXs<R> *gx = nullptr)
+{
+  const R pstep = step_gpil<R, K>(d, g, t, c, gx);
+  return step_move_begin<R, K>(g, t, c, pstep);
 }
 
 // One helix sub-step in Bz (FieldPropagationHandler::Propagate /
@@ -1612,15 +1645,16 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
 
 // Inclusive prefix sum of the primary energies, one block: each thread scans a
 // contiguous chunk, the chunk totals are scanned in shared memory.
+// status (optional): only the entries with status GX_TRACK_ALIVE count.
 __global__ void __launch_bounds__(1024) k_prefix_energy(const double *__restrict__ E, long long n,
-                                                        double *__restrict__ out)
+                                                        double *__restrict__ out, const int *__restrict__ status)
 {
   __shared__ double part[1024];
   int t = threadIdx.x, nt = blockDim.x;
   long long chunk = (n + nt - 1) / nt;
   long long b = t * chunk, e = min(n, b + chunk);
   double s = 0.0;
-  for (long long i = b; i < e; ++i) s += E[i];
+  for (long long i = b; i < e; ++i) s += (!status || status[i] == GX_TRACK_ALIVE) ? E[i] : 0.0;
   part[t] = s;
   __syncthreads();
   if (t == 0)
@@ -1628,7 +1662,7 @@ __global__ void __launch_bounds__(1024) k_prefix_energy(const double *__restrict
   __syncthreads();
   double run = t > 0 ? part[t - 1] : 0.0;
   for (long long i = b; i < e; ++i) {
-    run += E[i];
+    run += (!status || status[i] == GX_TRACK_ALIVE) ? E[i] : 0.0;
     out[i] = run;
   }
 }
@@ -1673,29 +1707,55 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
     }
     long long pi = ctl->prim_next + j;
     Track<R> t;
-    t.type = a.p.type[pi];
-    t.E = (R)a.p.E[pi];
-    for (int k = 0; k < 3; ++k) {
-      t.pos[k] = a.p.pos[3 * pi + k];
-      t.dir[k] = (R)a.p.dir[3 * pi + k];
-    }
-    double dd[3] = {a.p.dir[3 * pi], a.p.dir[3 * pi + 1], a.p.dir[3 * pi + 2]};
-    t.vol = a.g.geometry == 2 ? csg_locate(a.g.csg, 0, t.pos, dd, kCsgTol) : locate(a.g, t.pos, dd);
-    t.nil[0] = t.nil[1] = t.nil[2] = R(-1);
-    t.msc_r0 = R(-1);
-    t.event = a.p.event ? a.p.event[pi] : 0;
-    t.prim = (int)pi;
-    unsigned long long kk = (unsigned long long)(a.p.first_substream + pi);
-    uint64_t v1[3] = {(uint64_t)a.p.seed[0], (uint64_t)a.p.seed[1], (uint64_t)a.p.seed[2]};
-    uint64_t v2[3] = {(uint64_t)a.p.seed[3], (uint64_t)a.p.seed[4], (uint64_t)a.p.seed[5]};
-    for (int b = 0; kk != 0 && b < 64; ++b, kk >>= 1)
-      if (kk & 1ULL) {
-        jump_matvec(a.p.jump + 9 * b, v1, 4294967087ULL);
-        jump_matvec(a.p.jump + 9 * (64 + b), v2, 4294944443ULL);
+    if (a.p.from_soa) {
+      // a track handed in with its state
+      const SoaIn &q = a.p.soa;
+      if (q.status[pi] != GX_TRACK_ALIVE) continue;
+      t.type = q.type[pi];
+      t.E = (R)q.ekin[pi];
+      t.pos[0] = q.x[pi];
+      t.pos[1] = q.y[pi];
+      t.pos[2] = q.z[pi];
+      t.dir[0] = (R)q.dx[pi];
+      t.dir[1] = (R)q.dy[pi];
+      t.dir[2] = (R)q.dz[pi];
+      t.nil[0] = (R)q.nil0[pi];
+      t.nil[1] = (R)q.nil1[pi];
+      t.nil[2] = (R)q.nil2[pi];
+      t.msc_r0 = q.msc ? (R)q.msc[pi] : R(-1);
+      t.rng.load(q.rng, q.cap, pi);
+      t.vol = q.volume[pi];
+      if (t.vol < -1) {
+        double dd[3] = {q.dx[pi], q.dy[pi], q.dz[pi]};
+        t.vol = a.g.geometry == 2 ? csg_locate(a.g.csg, 0, t.pos, dd, kCsgTol) : locate(a.g, t.pos, dd);
       }
-    for (int k = 0; k < 3; ++k) {
-      t.rng.s[k] = (double)v1[k];
-      t.rng.s[3 + k] = (double)v2[k];
+      t.event = q.event ? q.event[pi] : 0;
+      t.prim = q.primary ? q.primary[pi] : -1;
+    } else {
+      t.type = a.p.type[pi];
+      t.E = (R)a.p.E[pi];
+      for (int k = 0; k < 3; ++k) {
+        t.pos[k] = a.p.pos[3 * pi + k];
+        t.dir[k] = (R)a.p.dir[3 * pi + k];
+      }
+      double dd[3] = {a.p.dir[3 * pi], a.p.dir[3 * pi + 1], a.p.dir[3 * pi + 2]};
+      t.vol = a.g.geometry == 2 ? csg_locate(a.g.csg, 0, t.pos, dd, kCsgTol) : locate(a.g, t.pos, dd);
+      t.nil[0] = t.nil[1] = t.nil[2] = R(-1);
+      t.msc_r0 = R(-1);
+      t.event = a.p.event ? a.p.event[pi] : 0;
+      t.prim = (int)pi;
+      unsigned long long kk = (unsigned long long)(a.p.first_substream + pi);
+      uint64_t v1[3] = {(uint64_t)a.p.seed[0], (uint64_t)a.p.seed[1], (uint64_t)a.p.seed[2]};
+      uint64_t v2[3] = {(uint64_t)a.p.seed[3], (uint64_t)a.p.seed[4], (uint64_t)a.p.seed[5]};
+      for (int b = 0; kk != 0 && b < 64; ++b, kk >>= 1)
+        if (kk & 1ULL) {
+          jump_matvec(a.p.jump + 9 * b, v1, 4294967087ULL);
+          jump_matvec(a.p.jump + 9 * (64 + b), v2, 4294944443ULL);
+        }
+      for (int k = 0; k < 3; ++k) {
+        t.rng.s[k] = (double)v1[k];
+        t.rng.s[3 + k] = (double)v2[k];
+      }
     }
     atomicAdd(&ctl->stat[S_TRACKS], 1ULL);
     if (t.vol < 0) {
@@ -1928,10 +1988,82 @@ template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaS
   }
 }
 
+// Copy the tracks of a store (or stack), or the not yet injected tracks of a
+// handed-in batch, into a caller's gx_track_soa at slots taken from a counter.
+template <class R>
+__global__ void k_extract(Store<R> src, long long n, int ptype, Ctl *ctl, gx_track_soa out)
+{
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    Track<R> t;
+    load_track(src, i, ptype, t);
+    const long long j = (long long)atomicAdd((unsigned long long *)&ctl->extracted, 1ULL);
+    if (j >= out.capacity) continue;
+    out.type[j] = t.type;
+    out.status[j] = GX_TRACK_ALIVE;
+    if (out.event) out.event[j] = t.event;
+    if (out.primary) out.primary[j] = t.prim;
+    out.volume[j] = t.vol;
+    out.next_volume[j] = t.vol;
+    out.process[j] = -1;
+    out.boundary[j] = 0;
+    out.x[j] = t.pos[0];
+    out.y[j] = t.pos[1];
+    out.z[j] = t.pos[2];
+    out.dx[j] = (double)t.dir[0];
+    out.dy[j] = (double)t.dir[1];
+    out.dz[j] = (double)t.dir[2];
+    out.ekin[j] = (double)t.E;
+    out.nil0[j] = (double)t.nil[0];
+    out.nil1[j] = (double)t.nil[1];
+    out.nil2[j] = (double)t.nil[2];
+    out.lambda_inv0[j] = out.lambda_inv1[j] = out.lambda_inv2[j] = 0.0;
+    out.pstep[j] = out.step[j] = out.snext[j] = out.safety[j] = 0.0;
+    if (out.msc_range) out.msc_range[j] = (double)t.msc_r0;
+    t.rng.store(out.rng, out.capacity, j);
+  }
+}
+
+__global__ void k_extract_pending(SoaIn in, long long first, long long n, Ctl *ctl, gx_track_soa out)
+{
+  for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    const long long i = first + k;
+    if (in.status[i] != GX_TRACK_ALIVE) continue;
+    const long long j = (long long)atomicAdd((unsigned long long *)&ctl->extracted, 1ULL);
+    if (j >= out.capacity) continue;
+    out.type[j] = in.type[i];
+    out.status[j] = GX_TRACK_ALIVE;
+    if (out.event) out.event[j] = in.event ? in.event[i] : 0;
+    if (out.primary) out.primary[j] = in.primary ? in.primary[i] : -1;
+    out.volume[j] = in.volume[i];
+    out.next_volume[j] = in.volume[i];
+    out.process[j] = -1;
+    out.boundary[j] = 0;
+    out.x[j] = in.x[i];
+    out.y[j] = in.y[i];
+    out.z[j] = in.z[i];
+    out.dx[j] = in.dx[i];
+    out.dy[j] = in.dy[i];
+    out.dz[j] = in.dz[i];
+    out.ekin[j] = in.ekin[i];
+    out.nil0[j] = in.nil0[i];
+    out.nil1[j] = in.nil1[i];
+    out.nil2[j] = in.nil2[i];
+    out.lambda_inv0[j] = out.lambda_inv1[j] = out.lambda_inv2[j] = 0.0;
+    out.pstep[j] = out.step[j] = out.snext[j] = out.safety[j] = 0.0;
+    if (out.msc_range) out.msc_range[j] = in.msc ? in.msc[i] : -1.0;
+#pragma unroll
+    for (int w = 0; w < 6; ++w) out.rng[w * out.capacity + j] = in.rng[w * in.cap + i];
+  }
+}
+
+// The transport loop.  tin (optional): transport these tracks instead of the
+// primaries; max_iter > 0: stop after that many iterations and write every
+// track still alive to tout.
 template <class R>
 static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
                const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
-               int *d_pstep, gx_transport_stats *stats, cudaStream_t s)
+               int *d_pstep, gx_transport_stats *stats, cudaStream_t s, const gx_track_soa *tin = nullptr,
+               int max_iter = 0, gx_track_soa *tout = nullptr)
 {
   const int prec = std::is_same<R, float>::value ? 1 : 0;
   const bool batched = cfg->engine == 1;
@@ -2030,6 +2162,12 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   for (int k = 0; k < 6; ++k) L.a.p.seed[k] = cfg->seed[k];
   L.a.p.first_substream = cfg->first_substream;
   L.a.p.jump = jt;
+  if (tin) {
+    L.a.p.from_soa = 1;
+    L.a.p.soa = SoaIn{tin->type, tin->status, tin->event, tin->primary, tin->volume, tin->x, tin->y, tin->z,
+                      tin->dx, tin->dy, tin->dz, tin->ekin, tin->nil0, tin->nil1, tin->nil2, tin->msc_range,
+                      tin->rng, (long long)tin->capacity};
+  }
   L.a.edep = d_edep;
   L.a.pstep = d_pstep;
   if (cfg->geometry == 2) {
@@ -2064,7 +2202,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       return cuda_error(err, "transport primary energies");
     E->cumE_cap = nprim;
   }
-  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, E->cumE);
+  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(tin ? tin->ekin : d_E, nprim, E->cumE, tin ? tin->status : nullptr);
   Ctl h;
   std::memset(&h, 0, sizeof(h));
   h.nprim = nprim;
@@ -2081,7 +2219,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
   cudaEventRecord(t0, s);
-  const long long max_iter = 2000000LL;
+  const long long kMaxIter = 2000000LL;
   long long iters = 0;
   // the kernels read their arguments from a device copy (indexing a kernel
   // parameter by a run-time value would copy the whole block to local memory)
@@ -2091,9 +2229,9 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     return cuda_error(err, "transport arguments upload");
   double step_ms[3] = {0, 0, 0}, transport_ms[3] = {0, 0, 0};
   long long step_launches[3] = {0, 0, 0};
-  if (!batched || cfg->profile) {
-    // plain loop (and the profiling pass): launch, synchronise, look at the
-    // counters, every iteration
+  if (!batched || cfg->profile || max_iter > 0) {
+    // plain loop (and the profiling pass, and runs stopped after a number of
+    // iterations): launch, synchronise, look at the counters, every iteration
     cudaEvent_t ea[3], em[3], eb[3];
     for (int q = 0; q < 3; ++q) {
       cudaEventCreate(&ea[q]);
@@ -2132,7 +2270,8 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         }
       ++iters;
       if (E->h_ctl->in_flight == 0 && E->h_ctl->pending == 0) break;
-      if (iters > max_iter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
+      if (max_iter > 0 && iters >= max_iter) break;
+      if (iters > kMaxIter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
     }
     for (int q = 0; q < 3; ++q) {
       cudaEventDestroy(ea[q]);
@@ -2174,7 +2313,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport graph");
       iters += G;
       if (E->h_ctl->in_flight == 0 && E->h_ctl->pending == 0) break;
-      if (iters > max_iter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
+      if (iters > kMaxIter) return set_error(GX_ERR_ITERCAP, "transport: iteration cap");
     }
   }
   if (cfg->geometry == 2) {
@@ -2183,6 +2322,31 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         E->vtally, C->csg_score, C->csg_n, C->csg_nscore, nt, d_edep);
   }
   k_count_new_tracks<<<1, 1, 0, s>>>(E->ctl);
+  if (tout) {
+    // the tracks still alive: carry out the refill plan the last iteration
+    // made (deferred tracks back into the stores, the next primaries in), then
+    // write out the stores, the stacks and what was never injected
+    const Args<R> *A = (const Args<R> *)E->dargs;
+    k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
+    k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
+    cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
+    if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport hand-over");
+    const Ctl hc = *E->h_ctl;
+    const int par = hc.parity;
+    const int ptype_of[3] = {batched ? 0 : 3, batched ? 1 : 3, batched ? 2 : 3};
+    for (int q = 0; q < nstores; ++q) {
+      const long long nc = std::min(hc.count[par][q], cap), ns = std::min(hc.stack_count[q], stack_cap);
+      if (nc > 0) k_extract<R><<<(int)std::min<long long>((nc + 255) / 256, 4096), 256, 0, s>>>(
+          L.a.st[par][q], nc, ptype_of[q], E->ctl, *tout);
+      if (ns > 0) k_extract<R><<<(int)std::min<long long>((ns + 255) / 256, 4096), 256, 0, s>>>(
+          L.a.stack[q], ns, ptype_of[q], E->ctl, *tout);
+    }
+    if (tin && hc.prim_next < hc.nprim) {
+      const long long np = hc.nprim - hc.prim_next;
+      k_extract_pending<<<(int)std::min<long long>((np + 255) / 256, 4096), 256, 0, s>>>(L.a.p.soa, hc.prim_next,
+                                                                                        np, E->ctl, *tout);
+    }
+  }
   cudaEventRecord(t1, s);
   cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
   if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport end");
@@ -2217,11 +2381,286 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     stats->bytes_per_track = (long long)(3 * sizeof(double) + 8 * sizeof(R) + 6 * sizeof(uint32_t) +
                                          3 * sizeof(int) + (batched ? 0 : sizeof(int)));
   }
+  if (tout) tout->n = (int)std::min<long long>(c.extracted, INT32_MAX);
   if (c.err_flags & kErrEvent)
     return set_error(GX_ERR_ARG, "transport: a primary's event index is outside [0, nevents = %d)", cfg->nevents);
   if (c.err_flags & kErrOverflow) return set_error(GX_ERR_OVERFLOW, "transport: track stores and stacks full");
+  if (tout && c.extracted > tout->capacity)
+    return set_error(GX_ERR_OVERFLOW, "gx_transport_tracks: %lld tracks alive, the output holds %d", c.extracted,
+                     tout->capacity);
   if (c.err_flags) return set_error(GX_ERR_ITERCAP, "transport: an iteration cap was hit (flags %d)", c.err_flags);
   return GX_OK;
+}
+
+
+// ------------------------------------------------- the stages of one step
+// gx_gpil, gx_propagate, gx_along_step, gx_post_step: OneStep cut at the
+// points where the reference's process interface hands over (GPIL, the move,
+// the along-step DoIt, the post-step DoIt), one thread per track of a
+// caller's gx_track_soa, FP64; the state carried from one stage to the next
+// is the SoA's (lambda_inv*, pstep, process, step, boundary, next_volume).
+// Multiple scattering is not offered stage by stage (its along-step state is
+// not part of the SoA); K: kKindFieldMap or 0.
+struct StageArgs {
+  const Data *d;
+  Geom g;
+  gx_track_soa t, sec;
+  double *edep;
+  double *escaped;
+};
+
+__device__ __forceinline__ void soa_load(const gx_track_soa &s, int i, Track<double> &t)
+{
+  t.type = s.type[i];
+  t.pos[0] = s.x[i];
+  t.pos[1] = s.y[i];
+  t.pos[2] = s.z[i];
+  t.dir[0] = s.dx[i];
+  t.dir[1] = s.dy[i];
+  t.dir[2] = s.dz[i];
+  t.E = s.ekin[i];
+  t.nil[0] = s.nil0[i];
+  t.nil[1] = s.nil1[i];
+  t.nil[2] = s.nil2[i];
+  t.msc_r0 = s.msc_range ? s.msc_range[i] : -1.0;
+  t.rng.load(s.rng, s.capacity, i);
+  t.vol = s.volume[i];
+  t.event = s.event ? s.event[i] : 0;
+  t.prim = s.primary ? s.primary[i] : -1;
+}
+
+// the state a stage may change
+__device__ __forceinline__ void soa_store(const gx_track_soa &s, int i, const Track<double> &t)
+{
+  s.x[i] = t.pos[0];
+  s.y[i] = t.pos[1];
+  s.z[i] = t.pos[2];
+  s.dx[i] = t.dir[0];
+  s.dy[i] = t.dir[1];
+  s.dz[i] = t.dir[2];
+  s.ekin[i] = t.E;
+  s.nil0[i] = t.nil[0];
+  s.nil1[i] = t.nil[1];
+  s.nil2[i] = t.nil[2];
+  if (s.msc_range) s.msc_range[i] = t.msc_r0;
+  t.rng.store(s.rng, s.capacity, i);
+  s.volume[i] = t.vol;
+}
+
+// the step context of a track from its SoA fields (after gx_gpil)
+__device__ __forceinline__ void soa_ctx(const gx_track_soa &s, int i, const Track<double> &t, StepCtx<double> &c)
+{
+  c.xs0 = s.lambda_inv0[i];
+  c.xs1 = s.lambda_inv1[i];
+  c.xs2 = s.lambda_inv2[i];
+  c.sel = s.process[i];
+  c.vol0 = t.vol;
+  c.newvol = t.vol;
+  c.crossed = false;
+  c.nsub = 0;
+  c.remaining = 0.0;
+  c.total = 0.0;
+  c.lam0 = 0.0;
+  c.e0 = t.E;
+  c.ttrue = 0.0;
+}
+
+__device__ __forceinline__ void stage_local(Local &L, const StageArgs &a)
+{
+  L.sm_edep = nullptr;
+  L.g_edep = a.edep;
+  L.sm_esc = a.escaped;
+  L.nvol = a.g.nvol;
+  L.nevents = a.g.nevents;
+  L.sm_bins = 0;
+  L.retired = 0.0;
+  L.err = 0;
+#pragma unroll
+  for (int k = 0; k < kNStat; ++k) L.st[k] = 0;
+}
+
+template <int K> __global__ void __launch_bounds__(128) k_stage_gpil(StageArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.t.n || a.t.status[i] != GX_TRACK_ALIVE) return;
+  Track<double> t;
+  soa_load(a.t, i, t);
+  if (t.vol < -1) t.vol = locate(a.g, t.pos, t.dir);
+  if (t.vol < 0) { // outside the world
+    a.t.volume[i] = t.vol;
+    a.t.status[i] = GX_TRACK_EXITED;
+    return;
+  }
+  StepCtx<double> c;
+  const double ps = step_gpil<double, K>(*a.d, a.g, t, c);
+  soa_store(a.t, i, t);
+  a.t.pstep[i] = ps;
+  a.t.process[i] = c.sel;
+  a.t.lambda_inv0[i] = c.xs0;
+  a.t.lambda_inv1[i] = c.xs1;
+  a.t.lambda_inv2[i] = c.xs2;
+  a.t.safety[i] = nav_safety<K>(a.g, t.vol, t.pos);
+  int plane;
+  a.t.snext[i] = fmin(nav_distance<K>(a.g, t.vol, t.pos, t.dir, ps, plane), ps);
+}
+
+template <int K> __global__ void __launch_bounds__(128) k_stage_propagate(StageArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.t.n || a.t.status[i] != GX_TRACK_ALIVE) return;
+  Track<double> t;
+  soa_load(a.t, i, t);
+  StepCtx<double> c;
+  soa_ctx(a.t, i, t, c);
+  Local L;
+  stage_local(L, a);
+  if (step_move_begin<double, K>(a.g, t, c, a.t.pstep[i]))
+    while (!field_substep<double, K>(*a.d, a.g, t, c, L)) {
+    }
+  soa_store(a.t, i, t);
+  a.t.step[i] = c.total;
+  a.t.boundary[i] = c.crossed ? 1 : 0;
+  a.t.next_volume[i] = c.crossed ? c.newvol : t.vol;
+}
+
+template <int K> __global__ void __launch_bounds__(128) k_stage_along(StageArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.t.n || a.t.status[i] != GX_TRACK_ALIVE) return;
+  Track<double> t;
+  soa_load(a.t, i, t);
+  StepCtx<double> c;
+  soa_ctx(a.t, i, t, c);
+  c.crossed = a.t.boundary[i] != 0;
+  c.newvol = a.t.next_volume[i];
+  c.total = a.t.step[i];
+  Local L;
+  stage_local(L, a);
+  int proc = -1;
+  const int r = step_end<double, K>(*a.d, a.g, t, c, L, &proc);
+  soa_store(a.t, i, t);
+  a.t.process[i] = (r == kInteract) ? proc : -1;
+  a.t.status[i] = (r == kInteract) ? GX_TRACK_INTERACT
+                  : (r == kAlive)  ? GX_TRACK_ALIVE
+                  : (c.crossed && c.newvol == -1) ? GX_TRACK_EXITED
+                                                  : GX_TRACK_KILLED;
+}
+
+template <int K> __global__ void __launch_bounds__(128) k_stage_post(StageArgs a)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.t.n) return;
+  int nsec = 0;
+  if (a.t.status[i] == GX_TRACK_INTERACT) {
+    Track<double> t;
+    soa_load(a.t, i, t);
+    Secs<double> sec;
+    sec.n = 0;
+    Local L;
+    stage_local(L, a);
+    run_model(*a.d, a.g, t, a.t.process[i], sec, L);
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      if (k >= sec.n) break;
+      Track<double> ch;
+      ch.type = sec.type[k];
+      ch.pos[0] = t.pos[0];
+      ch.pos[1] = t.pos[1];
+      ch.pos[2] = t.pos[2];
+      ch.dir[0] = sec.dir[k][0];
+      ch.dir[1] = sec.dir[k][1];
+      ch.dir[2] = sec.dir[k][2];
+      ch.E = sec.E[k];
+      ch.nil[0] = ch.nil[1] = ch.nil[2] = -1.0;
+      ch.msc_r0 = -1.0;
+      t.rng.seed_child(ch.rng);
+      ch.vol = t.vol;
+      ch.event = t.event;
+      ch.prim = -1;
+      const int j = 2 * i + k;
+      soa_store(a.sec, j, ch);
+      a.sec.type[j] = ch.type;
+      a.sec.status[j] = GX_TRACK_ALIVE;
+      if (a.sec.event) a.sec.event[j] = ch.event;
+      if (a.sec.primary) a.sec.primary[j] = -1;
+      a.sec.next_volume[j] = ch.vol;
+      a.sec.process[j] = -1;
+      a.sec.boundary[j] = 0;
+      a.sec.lambda_inv0[j] = a.sec.lambda_inv1[j] = a.sec.lambda_inv2[j] = 0.0;
+      a.sec.pstep[j] = a.sec.step[j] = a.sec.snext[j] = a.sec.safety[j] = 0.0;
+      ++nsec;
+    }
+    soa_store(a.t, i, t);
+    a.t.process[i] = -1;
+    a.t.status[i] = t.E > 0.0 ? GX_TRACK_ALIVE : GX_TRACK_KILLED;
+  }
+  for (int k = nsec; k < 2; ++k) {
+    a.sec.status[2 * i + k] = GX_TRACK_KILLED;
+    a.sec.type[2 * i + k] = -1;
+  }
+}
+
+// Geometry and options of a transport configuration, for the kernels.
+static void make_geom(const Ctx *C, const gx_transport_config *cfg, int nvol, Geom &g)
+{
+  std::memset(&g, 0, sizeof(g));
+  g.geometry = cfg->geometry;
+  g.axis = cfg->axis;
+  g.nlayers = cfg->nlayers;
+  g.box_mat = cfg->box_mat;
+  g.charged_local = cfg->charged_local;
+  g.nvol = nvol;
+  g.nevents = cfg->nevents;
+  g.t_abs = cfg->t_abs;
+  g.pitch = cfg->t_abs + cfg->t_gap;
+  g.x0 = -0.5 * cfg->nlayers * g.pitch;
+  g.total = cfg->nlayers * g.pitch;
+  g.half_trans = cfg->half_trans;
+  g.Bz = cfg->Bz;
+  g.msc = cfg->msc;
+  g.field_map = cfg->field_map;
+  for (int k = 0; k < 3; ++k) {
+    g.box_half[k] = cfg->box_half[k];
+    g.box_centre[k] = cfg->box_centre[k];
+  }
+}
+
+// One stage (0 gpil, 1 propagate, 2 along, 3 post) over a track SoA.
+int run_stage(int stage, Ctx *C, const gx_transport_config *cfg, gx_track_soa *t, gx_track_soa *sec, double *d_edep,
+              int nvol, cudaStream_t s)
+{
+  StageArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.d = C->dev;
+  make_geom(C, cfg, nvol, a.g);
+  a.t = *t;
+  if (sec) a.sec = *sec;
+  a.edep = d_edep;
+  a.escaped = C->stage_scratch;
+  if (t->n <= 0) return GX_OK;
+  const int grid = (t->n + 127) / 128;
+  const bool fm = cfg->field_map != 0;
+  switch (stage) {
+  case 0: (fm ? k_stage_gpil<kKindFieldMap> : k_stage_gpil<0>)<<<grid, 128, 0, s>>>(a); break;
+  case 1: (fm ? k_stage_propagate<kKindFieldMap> : k_stage_propagate<0>)<<<grid, 128, 0, s>>>(a); break;
+  case 2: (fm ? k_stage_along<kKindFieldMap> : k_stage_along<0>)<<<grid, 128, 0, s>>>(a); break;
+  default: (fm ? k_stage_post<kKindFieldMap> : k_stage_post<0>)<<<grid, 128, 0, s>>>(a); break;
+  }
+  const cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GX_OK : cuda_error(e, "gx stage launch");
+}
+
+// gx_transport_tracks in this variant (FP64 here, or FP32-mixed)
+int run_tracks(Ctx *C, const gx_transport_config *cfg, const gx_track_soa *in, int max_iter, gx_track_soa *out,
+               double *d_edep, int nvol, gx_transport_stats *stats, cudaStream_t s)
+{
+#ifndef GX_PARITY
+  if (cfg->precision == 1)
+    return run<float>(C, cfg, in->n, nullptr, nullptr, nullptr, nullptr, nullptr, d_edep, nvol, nullptr, stats, s, in,
+                      max_iter, out);
+#endif
+  return run<double>(C, cfg, in->n, nullptr, nullptr, nullptr, nullptr, nullptr, d_edep, nvol, nullptr, stats, s, in,
+                     max_iter, out);
 }
 
 #ifdef GX_PARITY
@@ -2258,6 +2697,39 @@ void gx_transport_config_default(gx_transport_config *c)
   c->engine = 1;
 }
 
+// The checks of a transport configuration shared by the entry points.
+static int check_config(const Ctx *C, const gx_transport_config *cfg, int nvol, const char *who)
+{
+  if (cfg->geometry == 1 && (cfg->nlayers <= 0 || cfg->t_abs <= 0 || cfg->t_gap <= 0 || cfg->half_trans <= 0 ||
+                             nvol < 2 * cfg->nlayers))
+    return set_error(GX_ERR_ARG, "%s: bad calorimeter (nvol must be >= 2 nlayers)", who);
+  if (cfg->axis < 0 || cfg->axis > 2 || cfg->precision < 0 || cfg->precision > 1 || cfg->engine < 0 ||
+      cfg->engine > 1 || cfg->nevents < 1)
+    return set_error(GX_ERR_ARG, "%s: bad config", who);
+  if (cfg->box_mat < 0 || cfg->box_mat > 2) return set_error(GX_ERR_ARG, "%s: bad box material", who);
+  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
+    return set_error(GX_ERR_ARG, "%s: block_size must be a multiple of 32, at most 256", who);
+  if (cfg->field_map && !C->host.fmap)
+    return set_error(GX_ERR_ARG, "%s: field_map = 1 without a field map (gx_ctx_load_field_map)", who);
+  if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "%s: bad geometry", who);
+  if (cfg->msc < 0 || cfg->msc > 2) return set_error(GX_ERR_ARG, "%s: msc must be 0, 1 or 2", who);
+  if (cfg->geometry == 2 && !C->csg_node)
+    return set_error(GX_ERR_ARG, "%s: geometry 2 without a volume tree (gx_ctx_load_geometry)", who);
+  if (cfg->geometry == 2 && nvol != C->csg_nscore)
+    return set_error(GX_ERR_ARG, "%s: nvol %d, the volume tree has %d scored touchables", who, nvol, C->csg_nscore);
+  if (cfg->fp64_parity < 0 || cfg->fp64_parity > 1 || (cfg->fp64_parity && cfg->precision != 0))
+    return set_error(GX_ERR_ARG, "%s: fp64_parity must be 0 or 1, and 1 needs precision 0", who);
+  return GX_OK;
+}
+
+// The arrays every stage and the hand-over read or write.
+static bool soa_complete(const gx_track_soa *t)
+{
+  return t && t->n >= 0 && t->capacity >= t->n && t->type && t->status && t->volume && t->next_volume && t->process &&
+         t->boundary && t->x && t->y && t->z && t->dx && t->dy && t->dz && t->ekin && t->nil0 && t->nil1 && t->nil2 &&
+         t->lambda_inv0 && t->lambda_inv1 && t->lambda_inv2 && t->pstep && t->step && t->snext && t->safety && t->rng;
+}
+
 int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
                      const double *d_pos, const double *d_dir, const int *d_event, double *d_edep, int nvol,
                      int *d_primary_steps, gx_transport_stats *stats, gx_stream_t s)
@@ -2265,27 +2737,9 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
   if (!ctx || !cfg) return set_error(GX_ERR_ARG, "gx_transport_run: null argument");
   if (nprim < 0 || (nprim > 0 && (!d_type || !d_E || !d_pos || !d_dir)) || !d_edep || nvol <= 0)
     return set_error(GX_ERR_ARG, "gx_transport_run: bad arguments");
-  if (cfg->geometry == 1 && (cfg->nlayers <= 0 || cfg->t_abs <= 0 || cfg->t_gap <= 0 || cfg->half_trans <= 0 ||
-                             nvol < 2 * cfg->nlayers))
-    return set_error(GX_ERR_ARG, "gx_transport_run: bad calorimeter (nvol must be >= 2 nlayers)");
-  if (cfg->axis < 0 || cfg->axis > 2 || cfg->precision < 0 || cfg->precision > 1 || cfg->engine < 0 ||
-      cfg->engine > 1 || cfg->nevents < 1)
-    return set_error(GX_ERR_ARG, "gx_transport_run: bad config");
-  if (cfg->box_mat < 0 || cfg->box_mat > 2) return set_error(GX_ERR_ARG, "gx_transport_run: bad box material");
-  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
-    return set_error(GX_ERR_ARG, "gx_transport_run: block_size must be a multiple of 32, at most 256");
   Ctx *C = reinterpret_cast<Ctx *>(ctx);
-  if (cfg->field_map && !C->host.fmap)
-    return set_error(GX_ERR_ARG, "gx_transport_run: field_map = 1 without a field map (gx_ctx_load_field_map)");
-  if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "gx_transport_run: bad geometry");
-  if (cfg->msc < 0 || cfg->msc > 2) return set_error(GX_ERR_ARG, "gx_transport_run: msc must be 0, 1 or 2");
-  if (cfg->geometry == 2 && !C->csg_node)
-    return set_error(GX_ERR_ARG, "gx_transport_run: geometry 2 without a volume tree (gx_ctx_load_geometry)");
-  if (cfg->geometry == 2 && nvol != C->csg_nscore)
-    return set_error(GX_ERR_ARG, "gx_transport_run: nvol %d, the volume tree has %d scored touchables", nvol,
-                     C->csg_nscore);
-  if (cfg->fp64_parity < 0 || cfg->fp64_parity > 1 || (cfg->fp64_parity && cfg->precision != 0))
-    return set_error(GX_ERR_ARG, "gx_transport_run: fp64_parity must be 0 or 1, and 1 needs precision 0");
+  int rc = check_config(C, cfg, nvol, "gx_transport_run");
+  if (rc) return rc;
   cudaSetDevice(C->device);
   if (cfg->fp64_parity)
     return parity::run_transport(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps,
@@ -2295,6 +2749,68 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
                       stream_of(s));
   return run<double>(C, cfg, nprim, d_type, d_E, d_pos, d_dir, d_event, d_edep, nvol, d_primary_steps, stats,
                      stream_of(s));
+}
+
+static int stage_entry(int stage, gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *t, gx_track_soa *sec,
+                       double *d_edep, int nvol, gx_stream_t s, const char *who)
+{
+  if (!ctx || !cfg || !soa_complete(t)) return set_error(GX_ERR_ARG, "%s: null argument or incomplete track SoA", who);
+  if (stage >= 2 && (!d_edep || nvol <= 0)) return set_error(GX_ERR_ARG, "%s: no tally", who);
+  if (stage == 3 && (!soa_complete(sec) || sec->capacity < 2 * t->n))
+    return set_error(GX_ERR_ARG, "%s: the secondaries' SoA needs capacity 2 n", who);
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  int rc = check_config(C, cfg, nvol > 0 ? nvol : 2 * cfg->nlayers, who);
+  if (rc) return rc;
+  if (cfg->msc || cfg->geometry == 2)
+    return set_error(GX_ERR_ARG, "%s: the stage calls take msc = 0 and geometry 0 or 1 (use gx_transport_tracks)", who);
+  cudaSetDevice(C->device);
+  if (!C->stage_scratch) {
+    cudaError_t e = cudaMalloc((void **)&C->stage_scratch, 8 * sizeof(double));
+    if (e != cudaSuccess) return cuda_error(e, "stage scratch");
+    C->owned.push_back(C->stage_scratch);
+    cudaMemset(C->stage_scratch, 0, 8 * sizeof(double));
+  }
+  if (stage == 3) sec->n = 2 * t->n;
+  if (cfg->fp64_parity) return parity::run_stage(stage, C, cfg, t, sec, d_edep, nvol, stream_of(s));
+  return run_stage(stage, C, cfg, t, sec, d_edep, nvol, stream_of(s));
+}
+
+int gx_gpil(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_stream_t s)
+{
+  return stage_entry(0, ctx, cfg, tracks, nullptr, nullptr, 0, s, "gx_gpil");
+}
+
+int gx_propagate(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_stream_t s)
+{
+  return stage_entry(1, ctx, cfg, tracks, nullptr, nullptr, 0, s, "gx_propagate");
+}
+
+int gx_along_step(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, double *d_edep, int nvol,
+                  gx_stream_t s)
+{
+  return stage_entry(2, ctx, cfg, tracks, nullptr, d_edep, nvol, s, "gx_along_step");
+}
+
+int gx_post_step(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_track_soa *secondaries,
+                 double *d_edep, int nvol, gx_stream_t s)
+{
+  return stage_entry(3, ctx, cfg, tracks, secondaries, d_edep, nvol, s, "gx_post_step");
+}
+
+int gx_transport_tracks(gx_ctx *ctx, const gx_transport_config *cfg, const gx_track_soa *in, int max_iterations,
+                        gx_track_soa *out, double *d_edep, int nvol, gx_transport_stats *stats, gx_stream_t s)
+{
+  if (!ctx || !cfg || !soa_complete(in) || !soa_complete(out) || !d_edep || nvol <= 0 || max_iterations < 0)
+    return set_error(GX_ERR_ARG, "gx_transport_tracks: bad arguments");
+  if (in->rng == out->rng || in->x == out->x || in->status == out->status)
+    return set_error(GX_ERR_ARG, "gx_transport_tracks: in and out share arrays");
+  Ctx *C = reinterpret_cast<Ctx *>(ctx);
+  int rc = check_config(C, cfg, nvol, "gx_transport_tracks");
+  if (rc) return rc;
+  cudaSetDevice(C->device);
+  out->n = 0;
+  if (cfg->fp64_parity) return parity::run_tracks(C, cfg, in, max_iterations, out, d_edep, nvol, stats, stream_of(s));
+  return run_tracks(C, cfg, in, max_iterations, out, d_edep, nvol, stats, stream_of(s));
 }
 
 int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *h_type,
@@ -2513,7 +3029,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   if ((err = cudaMemcpyAsync(ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
       (err = cudaStreamSynchronize(s)) != cudaSuccess)
     return cuda_error(err, "gx_transport_run_noalloc: control block");
-  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, cumE);
+  if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, cumE, nullptr);
   k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
   Ctl hc;
   long long iters = 0;

@@ -406,6 +406,112 @@ int gx_hepevt_load(const char *path, int mode, int max_events, const double vert
                    double *d_E, double *d_pos, double *d_dir, int *d_event, int *n_prim, int *n_events,
                    int *n_skipped, gx_stream_t s);
 
+/* ------------------------------------------------- tracks in SoA form */
+/* A batch of tracks: the hot fields of the reference's TrackState
+ * (source/Geant/track/TrackState.hpp:30-232) as the arrays of a
+ * TrackCollection (source/Geant/track/TrackCollection.hpp:23-42), one entry
+ * per track in every array.  All arrays are device arrays of `capacity`
+ * entries owned by the caller; entries 0 .. n-1 are tracks.  Units mm, MeV.
+ * The fields, with the TrackState member each stands for:
+ *   type          particle: 0 gamma, 1 e-, 2 e+ (fPhysicsState.fParticleType)
+ *   status        GX_TRACK_* (fStatus)
+ *   event         event index, a row of the tally (fHistoryState.fEvent)
+ *   primary       index of the primary this track is, -1 for a secondary
+ *                 (fHistoryState.fPrimaryIndx)
+ *   volume        volume holding the track (layered calorimeter: 2 layer +
+ *                 slab; box: 0; CSG tree: the touchable), -1 outside, < -1
+ *                 "locate it" (fGeometryState.fPath)
+ *   next_volume   volume after the step (fGeometryState.fNextpath)
+ *   process       discrete process that limits the step, -1 none
+ *                 (fPhysicsState.fProcess): gamma 0 Compton, 1 conversion,
+ *                 2 photo-electric; e-/e+ 0 ionisation, 1 brems, e+
+ *                 2 annihilation
+ *   boundary      1 when the step ends on a boundary (fGeometryState.fBoundary)
+ *   x, y, z       position (fPos)          dx, dy, dz  unit direction (fDir)
+ *   ekin          kinetic energy (fPhysicsState.fEkin)
+ *   nil0..2       number of interaction lengths left of each discrete process,
+ *                 <= 0: draw a new one (fPhysicsProcessState[i].fNumOfInteractLengthLeft)
+ *   lambda_inv0..2  its macroscopic cross section at the step start, 1/mm
+ *                 (fPhysicsProcessState[i].fMacroscopicCrossSection)
+ *   pstep         proposed physics step (fPhysicsState.fPstep)
+ *   step          length of the last step taken (fStep)
+ *   snext         distance to the next boundary along the direction, up to
+ *                 pstep (fGeometryState.fSnext)
+ *   safety        isotropic safety (fGeometryState.fSafety)
+ *   msc_range     multiple scattering: range scale of the step limit in the
+ *                 current volume, <= 0 unset (no TrackState member: the
+ *                 reference has no multiple scattering)
+ *   rng           MRG32k3a state, six planes of `capacity` words (the
+ *                 reference keeps one generator per thread) */
+enum { GX_TRACK_ALIVE = 0, GX_TRACK_KILLED = 1, GX_TRACK_INTERACT = 2, GX_TRACK_EXITED = 3 };
+typedef struct {
+  int n, capacity;
+  int *type, *status, *event, *primary, *volume, *next_volume, *process, *boundary;
+  double *x, *y, *z, *dx, *dy, *dz, *ekin;
+  double *nil0, *nil1, *nil2, *lambda_inv0, *lambda_inv1, *lambda_inv2;
+  double *pstep, *step, *snext, *safety, *msc_range;
+  uint32_t *rng;
+} gx_track_soa;
+
+/* The four stages of one step of the reference's OneStep / InnerStep
+ * (source/Geant/proxy/test/test_BasicCpuTransport.cpp:358-497), one thread per
+ * track, for the tracks of `tracks` with status GX_TRACK_ALIVE (gx_post_step:
+ * GX_TRACK_INTERACT), in FP64 (cfg->fp64_parity selects the parity variant).
+ * cfg gives the geometry, field and physics options; multiple scattering
+ * (cfg->msc) is not offered stage by stage (use gx_transport_tracks).
+ *   gx_gpil        PostStepGPIL of every discrete process (NIL drawn when
+ *                  <= 0; ProxyEmProcess.hpp:122-151), the ionisation range
+ *                  limit (ProxyIonization.hpp:108-128), FindNextBoundary
+ *                  (geometry/NavigationInterface.hpp:63-98): writes
+ *                  lambda_inv*, nil*, pstep, process, snext, safety.
+ *   gx_propagate   LinearPropagationHandler / FieldPropagationHandler::
+ *                  Propagate (core/src/LinearPropagationHandler.cpp:12-56,
+ *                  magneticfield/src/FieldPropagationHandler.cpp:87-360): moves
+ *                  the track by pstep or to the first boundary; writes x..dz,
+ *                  step, boundary, next_volume.
+ *   gx_along_step  NIL update by step x lambda_inv, ProxyIonization::
+ *                  AlongStepDoIt (ProxyIonization.hpp:130-168) scored into
+ *                  d_edep[event * nvol + volume], then the outcome: status
+ *                  KILLED (stopped, or left the world: EXITED, energy kept in
+ *                  ekin), INTERACT (process set; a stopped e+ annihilates at
+ *                  rest, process 2) or ALIVE (volume = next_volume).
+ *   gx_post_step   PostStepDoIt (ProxyEmProcess.hpp:153-163): NIL of the
+ *                  process reset and its model sampled; the track is updated in
+ *                  place (KILLED when absorbed), its secondaries are written to
+ *                  `secondaries` at entries 2i and 2i+1 (status ALIVE, fresh
+ *                  NIL, streams seeded from the parent's; unused entries
+ *                  KILLED with type -1), and deposits scored; secondaries->
+ *                  capacity must be at least 2 tracks->n (secondaries->n is
+ *                  set to 2 tracks->n).
+ * Replace the reference's GPU launch wrappers (GPILGammaProcess,
+ * StepGammaProcess and the electron ones, source/Geant/kernel/
+ * KernelPhysicsProcess.cuh:22-36). */
+int gx_gpil(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_stream_t s);
+int gx_propagate(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_stream_t s);
+int gx_along_step(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, double *d_edep, int nvol,
+                  gx_stream_t s);
+int gx_post_step(gx_ctx *ctx, const gx_transport_config *cfg, gx_track_soa *tracks, gx_track_soa *secondaries,
+                 double *d_edep, int nvol, gx_stream_t s);
+
+/* The engine of gx_transport_run started from tracks instead of primaries:
+ * the tracks of `in` (status ALIVE; entries with other status are skipped)
+ * are injected as they are -- position, direction, energy, NIL, stream,
+ * volume (< -1: located) -- and transported with their secondaries for at
+ * most max_iterations iterations of the engine (0: to completion; one
+ * iteration is one step of every track in flight with the plain engine,
+ * up to steps_per_launch with the batched one), deposits added to d_edep.
+ * Every track still alive then -- in flight, deferred, or not yet injected --
+ * is written to `out` (out->n set; status ALIVE), so a caller can hand tracks
+ * over and take them back: transporting `out` afterwards, here or in the
+ * reference's host loop, continues each track exactly where it stopped (the
+ * results do not depend on where the hand-over happens).  More tracks than
+ * out->capacity: the first capacity are written and GX_ERR_OVERFLOW is
+ * returned with out->n = the number alive.  Synchronous.  `in` and `out` must
+ * not share arrays.  No counterpart in the reference (its TrackCollection is
+ * host-side only). */
+int gx_transport_tracks(gx_ctx *ctx, const gx_transport_config *cfg, const gx_track_soa *in, int max_iterations,
+                        gx_track_soa *out, double *d_edep, int nvol, gx_transport_stats *stats, gx_stream_t s);
+
 /* Launch-setting sweep of the batched engine.  No counterpart in the
  * reference (its kernels take nblocks / nthreads from the caller,
  * source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).  Transports the given

@@ -282,6 +282,17 @@ typedef struct {
 int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
                   const gxo_primary_t *prims, gxo_result_t *res);
 /* flat-array front end for ctypes */
+/* Tracks in flat arrays (pos, dir, nil: n x 3; rng: n x 6 state doubles;
+ * event, primary, msc optional), status 0 alive. */
+typedef struct {
+  int n;
+  int *type, *status, *event, *primary, *volume;
+  double *pos, *dir, *ekin, *nil, *msc, *rng;
+} gxo_tracks_t;
+int gxo_step_tracks(const gxo_data_t *d, const gxo_config_t *cfg, gxo_tracks_t *t, gxo_tracks_t *sec,
+                    double *edep, int nvol, double *escaped, long long *counters);
+int gxo_transport_tracks(const gxo_data_t *d, const gxo_config_t *cfg, const gxo_tracks_t *t, double *edep, int nvol,
+                         double *escaped, long long *counters);
 int gxo_transport_flat(const gxo_data_t *d, const gxo_config_t *cfg, int nprim,
                        const int *type, const double *E, const double *pos, const double *dir,
                        const int *event, double *edep, int nvol, double *escaped,

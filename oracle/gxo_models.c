@@ -594,7 +594,10 @@ double gxo_pe_xs_sandia(const gxo_data_t *d, int Z, double density, double e)
   while (row > first && ekev < d->sandia[row][0]) --row;
   if (ekev < d->sandia[row][0]) return 0.0;
   const double *a = d->sandia[row];
-  double s = a[1] / ekev + a[2] / (ekev * ekev) + a[3] / (ekev * ekev * ekev) + a[4] / (ekev * ekev * ekev * ekev);
+  /* a1/E + a2/E^2 + a3/E^3 + a4/E^4 as a polynomial in 1/E (Horner), the
+   * CUDA library's form, so that both round alike */
+  double i1 = 1.0 / ekev;
+  double s = i1 * (a[1] + i1 * (a[2] + i1 * (a[3] + i1 * a[4])));
   return fmax(s, 0.0) * density * 0.1; /* cm2/g * g/cm3 = 1/cm -> 1/mm */
 }
 

@@ -788,11 +788,109 @@ double gxo_msc_lambda1(const gxo_data_t *d, int type, int mat, double e)
 double gxo_msc_true_to_geom(double t, double lam) { return msc_true_to_geom(t, lam); }
 double gxo_msc_geom_to_true(double z, double lam, double tmax) { return msc_geom_to_true(z, lam, tmax); }
 
+/* ------------------------------------------------ tracks handed in or out */
+static void track_in(const world_t *w, const gxo_tracks_t *a, int i, track_t *tr)
+{
+  memset(tr, 0, sizeof(*tr));
+  tr->type = a->type[i];
+  tr->E = a->ekin[i];
+  for (int k = 0; k < 3; ++k) {
+    tr->pos[k] = a->pos[3 * i + k];
+    tr->dir[k] = a->dir[3 * i + k];
+    tr->nil[k] = a->nil[3 * i + k];
+  }
+  tr->msc_r0 = a->msc ? a->msc[i] : -1.0;
+  memcpy(tr->rng.s, &a->rng[6 * i], sizeof(tr->rng.s));
+  tr->vol = a->volume[i];
+  if (tr->vol < -1) tr->vol = locate(w, tr->pos, tr->dir);
+  tr->event = a->event ? a->event[i] : 0;
+  tr->primary = -1;
+}
+
+static void track_out(const track_t *tr, gxo_tracks_t *a, int i, int status)
+{
+  a->type[i] = tr->type;
+  a->status[i] = status;
+  if (a->event) a->event[i] = tr->event;
+  if (a->primary) a->primary[i] = -1;
+  a->volume[i] = tr->vol;
+  a->ekin[i] = tr->E;
+  for (int k = 0; k < 3; ++k) {
+    a->pos[3 * i + k] = tr->pos[k];
+    a->dir[3 * i + k] = tr->dir[k];
+    a->nil[3 * i + k] = tr->nil[k];
+  }
+  if (a->msc) a->msc[i] = tr->msc_r0;
+  memcpy(&a->rng[6 * i], tr->rng.s, sizeof(tr->rng.s));
+}
+
+static void world_init(world_t *w, const gxo_data_t *d, const gxo_config_t *cfg)
+{
+  memset(w, 0, sizeof(*w));
+  w->d = d;
+  w->c = cfg;
+  w->pitch = cfg->t_abs + cfg->t_gap;
+  gxo_material_make(1.0, 1.01, 1.e-25, &w->mat[0]);
+  gxo_material_make(82.0, 207.2, 11.35, &w->mat[1]);
+  gxo_material_make(18.0, 39.95, 1.396, &w->mat[2]);
+  for (int m = 0; m < 3; ++m) msc_material(w->mat[m].Z, w->mat[m].radlen, &w->msc[m]);
+}
+
+/* One OneStep of every track of t with status 0 (alive), in order, single
+ * thread: the step-by-step counterpart of the CUDA library's stage calls
+ * (gx_gpil .. gx_post_step).  A track's secondaries go to sec entries 2i,
+ * 2i+1 in the order they are made (status 0; unused entries status 1, type
+ * -1); t's status becomes 0 alive, 1 finished, 3 left the world (its energy
+ * kept).  counters: steps, substeps, secondaries (gamma, e-, e+), pairs,
+ * annihilations, errors. */
+int gxo_step_tracks(const gxo_data_t *d, const gxo_config_t *cfg, gxo_tracks_t *t, gxo_tracks_t *sec,
+                    double *edep, int nvol, double *escaped, long long *counters)
+{
+  world_t w;
+  world_init(&w, d, cfg);
+  tally_t ta;
+  memset(&ta, 0, sizeof(ta));
+  ta.edep = edep;
+  ta.nvol = nvol;
+  stack_t st = {0, 0, 0};
+  for (int i = 0; i < t->n; ++i) {
+    int nsec = 0;
+    if (t->status[i] == 0) {
+      track_t tr;
+      track_in(&w, t, i, &tr);
+      st.n = 0;
+      int alive = (tr.vol >= 0) ? one_step(&w, &tr, &st, &ta) : 0;
+      track_out(&tr, t, i, alive ? 0 : (tr.vol < 0 ? 3 : 1));
+      for (int k = 0; k < st.n && k < 2; ++k) {
+        track_out(&st.a[k], sec, 2 * i + k, 0);
+        nsec++;
+      }
+    }
+    for (int k = nsec; k < 2; ++k) {
+      sec->status[2 * i + k] = 1;
+      sec->type[2 * i + k] = -1;
+    }
+  }
+  sec->n = 2 * t->n;
+  free(st.a);
+  *escaped = ta.escaped;
+  counters[0] = ta.steps;
+  counters[1] = ta.substeps;
+  counters[2] = ta.sec[0];
+  counters[3] = ta.sec[1];
+  counters[4] = ta.sec[2];
+  counters[5] = ta.npair;
+  counters[6] = ta.nannih;
+  counters[7] = ta.errors;
+  return 0;
+}
+
 /* -------------------------------------------------------------- runner */
 typedef struct {
   world_t *w;
   int nprim;
   const gxo_primary_t *prims;
+  const gxo_tracks_t *tracks; /* instead of prims: tracks handed in with their state */
   int tid, nthreads;
   tally_t t;
   double seedcopy[6];
@@ -804,19 +902,24 @@ static void *worker(void *arg)
   world_t *w = j->w;
   stack_t st = {0, 0, 0};
   for (int i = j->tid; i < j->nprim; i += j->nthreads) {
-    const gxo_primary_t *pr = &j->prims[i];
     track_t tr;
-    memset(&tr, 0, sizeof(tr));
-    tr.type = pr->type;
-    tr.E = pr->E;
-    memcpy(tr.pos, pr->pos, sizeof(tr.pos));
-    memcpy(tr.dir, pr->dir, sizeof(tr.dir));
-    tr.vol = locate(w, tr.pos, tr.dir);
-    tr.nil[0] = tr.nil[1] = tr.nil[2] = -1.0;
-    tr.msc_r0 = -1.0;
-    gxo_mrg_substreams(w->c->seed, w->c->first_substream + i, 1, tr.rng.s);
-    tr.event = pr->event;
-    tr.primary = i;
+    if (j->tracks) {
+      if (j->tracks->status[i] != 0) continue;
+      track_in(w, j->tracks, i, &tr);
+    } else {
+      const gxo_primary_t *pr = &j->prims[i];
+      memset(&tr, 0, sizeof(tr));
+      tr.type = pr->type;
+      tr.E = pr->E;
+      memcpy(tr.pos, pr->pos, sizeof(tr.pos));
+      memcpy(tr.dir, pr->dir, sizeof(tr.dir));
+      tr.vol = locate(w, tr.pos, tr.dir);
+      tr.nil[0] = tr.nil[1] = tr.nil[2] = -1.0;
+      tr.msc_r0 = -1.0;
+      gxo_mrg_substreams(w->c->seed, w->c->first_substream + i, 1, tr.rng.s);
+      tr.event = pr->event;
+      tr.primary = i;
+    }
     if (tr.vol < 0) {
       j->t.escaped += tr.E;
       continue;
@@ -840,18 +943,11 @@ static void *worker(void *arg)
   return NULL;
 }
 
-int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const gxo_primary_t *prims,
-                  gxo_result_t *res)
+static int transport_jobs(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const gxo_primary_t *prims,
+                          const gxo_tracks_t *tracks, gxo_result_t *res)
 {
   world_t w;
-  memset(&w, 0, sizeof(w));
-  w.d = d;
-  w.c = cfg;
-  w.pitch = cfg->t_abs + cfg->t_gap;
-  gxo_material_make(1.0, 1.01, 1.e-25, &w.mat[0]);
-  gxo_material_make(82.0, 207.2, 11.35, &w.mat[1]);
-  gxo_material_make(18.0, 39.95, 1.396, &w.mat[2]);
-  for (int m = 0; m < 3; ++m) msc_material(w.mat[m].Z, w.mat[m].radlen, &w.msc[m]);
+  world_init(&w, d, cfg);
   int nt = cfg->nthreads > 0 ? cfg->nthreads : 1;
   int nvol = res->nvol;
   if (cfg->geometry == 2 && (!cfg->csg || nvol != cfg->csg->nscore)) return -1;
@@ -862,6 +958,7 @@ int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const
     jobs[k].w = &w;
     jobs[k].nprim = nprim;
     jobs[k].prims = prims;
+    jobs[k].tracks = tracks;
     jobs[k].tid = k;
     jobs[k].nthreads = nt;
     jobs[k].t.nvol = nvol;
@@ -890,6 +987,36 @@ int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const
   free(jobs);
   free(th);
   return 0;
+}
+
+int gxo_transport(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const gxo_primary_t *prims,
+                  gxo_result_t *res)
+{
+  return transport_jobs(d, cfg, nprim, prims, NULL, res);
+}
+
+/* The tracks of t with status 0, handed in with their state, transported to
+ * completion with their secondaries (the oracle's side of the hand-over of
+ * gx_transport_tracks); counters as gxo_transport_flat's. */
+int gxo_transport_tracks(const gxo_data_t *d, const gxo_config_t *cfg, const gxo_tracks_t *t, double *edep, int nvol,
+                         double *escaped, long long *counters)
+{
+  gxo_result_t r;
+  memset(&r, 0, sizeof(r));
+  r.edep = edep;
+  r.nvol = nvol;
+  int rc = transport_jobs(d, cfg, t->n, NULL, t, &r);
+  *escaped = r.escaped;
+  counters[0] = r.steps;
+  counters[1] = r.substeps;
+  counters[2] = r.tracks;
+  counters[3] = r.secondaries[0];
+  counters[4] = r.secondaries[1];
+  counters[5] = r.secondaries[2];
+  counters[6] = r.n_pair;
+  counters[7] = r.n_annih;
+  counters[8] = r.errors;
+  return rc;
 }
 
 int gxo_transport_flat(const gxo_data_t *d, const gxo_config_t *cfg, int nprim, const int *type,

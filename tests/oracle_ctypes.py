@@ -67,6 +67,46 @@ _SB_SIZE = (32 + 57 + 57 * 32) * 8
 _SB_OFF = _NTABLES * _NMAT * _PVEC_SIZE + (4 * _NMAT) * 8 * 2 + 12 * 8
 
 
+class TracksStruct(C.Structure):
+    _fields_ = [("n", I)] + [(f, P) for f in ("type", "status", "event", "primary", "volume", "pos", "dir", "ekin",
+                                              "nil", "msc", "rng")]
+
+
+class Tracks:
+    """Tracks for the oracle in flat host arrays (pos, dir, nil n x 3; rng
+    n x 6 MRG32k3a state doubles)."""
+
+    def __init__(self, n):
+        self.n = n
+        for f in ("type", "status", "event", "primary", "volume"):
+            setattr(self, f, np.zeros(n, np.int32))
+        for f, shape in (("pos", (n, 3)), ("dir", (n, 3)), ("nil", (n, 3)), ("rng", (n, 6)), ("ekin", (n,)),
+                         ("msc", (n,))):
+            setattr(self, f, np.zeros(shape))
+
+    @classmethod
+    def from_soa(cls, d):
+        """From TrackSoA.numpy() of the CUDA library's SoA."""
+        n = len(d["type"])
+        t = cls(n)
+        for f in ("type", "status", "event", "primary", "volume"):
+            getattr(t, f)[:] = d[f]
+        t.pos[:] = np.stack([d["x"], d["y"], d["z"]], 1)
+        t.dir[:] = np.stack([d["dx"], d["dy"], d["dz"]], 1)
+        t.nil[:] = np.stack([d["nil0"], d["nil1"], d["nil2"]], 1)
+        t.ekin[:] = d["ekin"]
+        t.msc[:] = d["msc_range"]
+        t.rng[:] = d["rng"].astype(np.float64)
+        return t
+
+    def struct(self):
+        s = TracksStruct()
+        s.n = self.n
+        for f in ("type", "status", "event", "primary", "volume", "pos", "dir", "ekin", "nil", "msc", "rng"):
+            setattr(s, f, getattr(self, f).ctypes.data)
+        return s
+
+
 class Oracle:
     def __init__(self, path=ORACLE_SO, datadir=DATA_DIR):
         if not os.path.exists(path):
@@ -109,6 +149,10 @@ class Oracle:
         lib.gxo_transport_flat.argtypes = [P, C.POINTER(Config), I, C.POINTER(I), C.POINTER(D), C.POINTER(D),
                                            C.POINTER(D), C.POINTER(I), C.POINTER(D), I, C.POINTER(D),
                                            C.POINTER(C.c_longlong), C.POINTER(I)]
+        lib.gxo_step_tracks.argtypes = [P, C.POINTER(Config), C.POINTER(TracksStruct), C.POINTER(TracksStruct),
+                                        C.POINTER(D), I, C.POINTER(D), C.POINTER(C.c_longlong)]
+        lib.gxo_transport_tracks.argtypes = [P, C.POINTER(Config), C.POINTER(TracksStruct), C.POINTER(D), I,
+                                             C.POINTER(D), C.POINTER(C.c_longlong)]
         for f in ("gxo_gxm_eval", "gxo_libm_eval"):
             getattr(lib, f).argtypes = [I, I, C.POINTER(D), C.POINTER(D), C.POINTER(D)]
         self.data = lib.gxo_data_load(datadir.encode())
@@ -235,6 +279,33 @@ class Oracle:
                  "errors"]
         res = dict(zip(names, [int(c) for c in counters]))
         res.update(edep=edep, escaped=esc.value, primary_steps=psteps)
+        return res
+
+    def step_tracks(self, cfg, tracks, edep):
+        """One OneStep of every alive track (in place); returns (secondaries
+        Tracks at 2i, 2i+1, escaped energy, counters dict)."""
+        sec = Tracks(2 * tracks.n)
+        esc = D(0.0)
+        counters = np.zeros(8, dtype=np.int64)
+        ts, ss = tracks.struct(), sec.struct()
+        self.lib.gxo_step_tracks(self.data, C.byref(cfg), C.byref(ts), C.byref(ss), dp(edep), edep.shape[-1],
+                                 C.byref(esc), lp(counters))
+        names = ["steps", "substeps", "sec_gamma", "sec_electron", "sec_positron", "n_pair", "n_annih", "errors"]
+        return sec, esc.value, dict(zip(names, [int(c) for c in counters]))
+
+    def transport_tracks(self, cfg, tracks, nvol, nevents=1):
+        """The alive tracks of `tracks` to completion; returns a result dict
+        like transport()'s."""
+        edep = np.zeros((nevents, nvol))
+        esc = D(0.0)
+        counters = np.zeros(9, dtype=np.int64)
+        ts = tracks.struct()
+        assert self.lib.gxo_transport_tracks(self.data, C.byref(cfg), C.byref(ts), dp(edep), nvol, C.byref(esc),
+                                             lp(counters)) == 0
+        names = ["steps", "substeps", "tracks", "sec_gamma", "sec_electron", "sec_positron", "n_pair", "n_annih",
+                 "errors"]
+        res = dict(zip(names, [int(c) for c in counters]))
+        res.update(edep=edep, escaped=esc.value)
         return res
 
     # ------------------------------------------------------------ field map
