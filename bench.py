@@ -47,7 +47,8 @@ sys.path.insert(0, REPO)
 
 METRIC = "track-steps/s on 1 B200: FP32-mixed vs FP64 GPU, ≤0.5% per-layer Edep diff"
 UNIT = "track-steps/s"
-LAUNCH_KEYS = ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy")
+LAUNCH_KEYS = ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy",
+               "interaction_interval")
 NSUB = 10  # sub-batches of a batch for the per-layer standard deviations
 
 

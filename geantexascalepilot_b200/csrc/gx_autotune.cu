@@ -1,14 +1,18 @@
 // gx_autotune.cu -- launch-setting sweep for the batched transport engine.
 //
-// The step kernels are register-heavy (110-130 registers per thread), so the
-// useful block sizes are 64-256 threads (a 512- or 1024-thread block would
-// need at most 128 or 64 registers per thread and spill); the grid is a
-// multiple of the SM count.  The sweep is coordinate descent: block size x
-// resident blocks per SM first, then the steps a track may take per transport
-// launch, then the number of iterations per CUDA-graph launch, then the refill
-// threshold, then the primary energy per injection wave.  Each candidate transports the caller's primaries completely; its
-// score is track-steps per millisecond of device time, the best of `repeats`
-// runs (the first run of a new launch shape also captures its graph).
+// The step kernels are register-heavy (110-130 registers per thread); block
+// sizes of 64-256 threads run the kernels compiled for them, 512 and 1024
+// threads (for the uniform field, layered geometry and no multiple
+// scattering) the variants held to 64 registers per thread, which spill; the
+// grid is a multiple of the SM count.  The sweep is coordinate descent: block
+// size x resident blocks per SM first, then the steps a track may take per
+// transport launch, then the number of iterations per CUDA-graph launch, then
+// the refill threshold, then the primary energy per injection wave, then the
+// compaction interval (how many iterations interacting tracks wait in their
+// buffers before the interaction kernels compact them back into the stores).
+// Each candidate transports the caller's primaries completely; its score is
+// track-steps per millisecond of device time, the best of `repeats` runs (the
+// first run of a new launch shape also captures its graph).
 #include "gx_internal.cuh"
 
 #include <cstring>
@@ -20,6 +24,7 @@ struct Trial {
   int block, bpsm, steps, graph_iters;
   long long refill_below;
   double wave_energy;
+  int interval;
 };
 
 } // namespace
@@ -53,7 +58,8 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
                 base.blocks_per_sm > 0 ? base.blocks_per_sm : kDefaultBlocksPerSM,
                 base.steps_per_launch > 0 ? base.steps_per_launch : kDefaultStepsPerLaunch,
                 base.graph_iters > 0 ? base.graph_iters : 16,
-                base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy};
+                base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy,
+                base.interaction_interval > 0 ? base.interaction_interval : 1};
 
   auto measure = [&](const Trial &t) -> double {
     gx_transport_config c = base;
@@ -63,6 +69,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     c.graph_iters = t.graph_iters;
     c.refill_below = t.refill_below;
     c.wave_energy = t.wave_energy;
+    c.interaction_interval = t.interval;
     double best_ms = 0.0, rate = 0.0;
     for (int r = 0; r < repeats; ++r) {
       cudaMemsetAsync(edep, 0, nt * sizeof(double), s);
@@ -84,6 +91,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
       rep->graph_iters[ntrials] = t.graph_iters;
       rep->refill_below[ntrials] = t.refill_below;
       rep->wave_energy[ntrials] = t.wave_energy;
+      rep->interaction_interval[ntrials] = t.interval;
       rep->kernel_ms[ntrials] = best_ms;
       rep->steps_per_ms[ntrials] = rate;
     }
@@ -100,10 +108,13 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     }
   };
 
-  const int blocks[] = {64, 128, 256};
+  // blocks above 256 threads only where their kernel variants exist
+  const bool wide_ok = base.geometry != 2 && !base.msc && !base.field_map && !base.fp64_parity;
+  const int blocks[] = {64, 128, 256, 512, 1024};
   const int bpsms[] = {1, 2, 4, 8};
   for (int b : blocks)
     for (int p : bpsms) {
+      if (b > 256 && (!wide_ok || b * p > 4096)) continue;
       Trial t = best;
       t.block = b;
       t.bpsm = p;
@@ -135,6 +146,12 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     t.wave_energy = m * wave0;
     consider(t);
   }
+  const Trial after_wave = best;
+  for (int k : {2, 4, 8}) {
+    Trial t = after_wave;
+    t.interval = k;
+    consider(t);
+  }
   cudaFree(edep);
   if (rep) rep->trials = ntrials < GX_AUTOTUNE_MAX_TRIALS ? ntrials : GX_AUTOTUNE_MAX_TRIALS;
   if (rc) return rc;
@@ -145,5 +162,6 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   cfg->graph_iters = best.graph_iters;
   cfg->refill_below = best.refill_below;
   cfg->wave_energy = best.wave_energy;
+  cfg->interaction_interval = best.interval;
   return GX_OK;
 }

@@ -1538,11 +1538,17 @@ template <class R, int PT, int K> __global__ void __maxnreg__(168) k_transport_c
 {
   transport_body<R, PT, K>(A);
 }
+// Variants for 512- and 1024-thread blocks (the launch-setting sweep): held
+// to the 64 registers per thread a 1024-thread block leaves, they spill.
+template <class R, int PT, int K> __global__ void __launch_bounds__(1024, 1) k_transport_wide(const Args<R> *__restrict__ A)
+{
+  transport_body<R, PT, K>(A);
+}
 
 // Post-step interaction of process PROC for the buffered tracks of type PT:
 // one model per kernel, so a warp runs one sampling algorithm; survivor and
 // secondaries go to the next stores.
-template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMinBlocks<R>) k_interact(const Args<R> *__restrict__ A)
+template <class R, int PT, int PROC> __device__ __forceinline__ void interact_body(const Args<R> *__restrict__ A)
 {
   extern __shared__ double sm_edep[];
   __shared__ unsigned long long sm_stat[kNStat];
@@ -1576,15 +1582,34 @@ template <class R, int PT, int PROC> __global__ void __launch_bounds__(256, kMin
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
 }
 
+template <class R, int PT, int PROC>
+__global__ void __launch_bounds__(256, kMinBlocks<R>) k_interact(const Args<R> *__restrict__ A)
+{
+  interact_body<R, PT, PROC>(A);
+}
+template <class R, int PT, int PROC>
+__global__ void __launch_bounds__(1024, 1) k_interact_wide(const Args<R> *__restrict__ A)
+{
+  interact_body<R, PT, PROC>(A);
+}
+
 // End of an iteration: the next stores become current, the refill plan for
-// the following iteration is made.  One thread.
-__global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores)
+// the following iteration is made.  One thread.  interacted: the interaction
+// kernels ran in this iteration (their buffers are emptied); otherwise the
+// tracks waiting in them count as pending.
+__global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores, int interacted)
 {
   int par = ctl->parity, np = par ^ 1;
   const long long cap[3] = {cap0, cap1, cap2};
   const long long refill_below = ctl->refill_below, stack_cap = ctl->stack_cap;
+  long long buffered = 0;
   for (int q = 0; q < 3; ++q) {
-    for (int p = 0; p < 3; ++p) ctl->qcount[q][p] = 0;
+    for (int p = 0; p < 3; ++p) {
+      if (interacted)
+        ctl->qcount[q][p] = 0;
+      else
+        buffered += ctl->qcount[q][p];
+    }
     ctl->take[q] = 0;
   }
   long long fl = 0;
@@ -1599,7 +1624,7 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
   ctl->iterations++;
   // refill plan: deferred tracks first (most recent first), then primaries
   long long budget = refill_below - fl;
-  long long pend = ctl->nprim - ctl->prim_next;
+  long long pend = ctl->nprim - ctl->prim_next + buffered;
   for (int q = 0; q < nstores; ++q) {
     long long room = cap[q] - ctl->count[np][q];
     long long take = 0;
@@ -1774,8 +1799,9 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
   }
 }
 
-template <class R> __global__ void k_refill(Args<R> a) { refill_body(a); }
-template <class R> __global__ void k_refill_p(const Args<R> *__restrict__ A) { refill_body(*A); }
+// launched with the step kernels' block size, up to 1024 threads
+template <class R> __global__ void __launch_bounds__(1024) k_refill(Args<R> a) { refill_body(a); }
+template <class R> __global__ void __launch_bounds__(1024) k_refill_p(const Args<R> *__restrict__ A) { refill_body(*A); }
 
 // Bookkeeping after a refill: the primary cursor.  One thread.
 __global__ void k_refill_done(Ctl *ctl)
@@ -1919,7 +1945,35 @@ template <class R> static void (*step_kernel_p(int kind))(const Args<R> *)
   }
 }
 
-template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent)
+// The step kernels of one type for a launch: blocks above 256 threads take the
+// wide variants (kernel kind 0 only, FP32 and FP64 library kernels).
+template <class R, int PT> static void (*transport_for(const Launch<R> &L))(const Args<R> *)
+{
+#ifndef GX_PARITY
+  if (L.block > 256) return k_transport_wide<R, PT, 0>;
+#endif
+  return transport_kernel<R, PT>(kernel_kind(L.a.g));
+}
+template <class R, int PT, int PROC> static void (*interact_for(const Launch<R> &L))(const Args<R> *)
+{
+#ifndef GX_PARITY
+  if (L.block > 256) return k_interact_wide<R, PT, PROC>;
+#endif
+  return k_interact<R, PT, PROC>;
+}
+
+// One type's interaction kernels (gamma 3 processes, e- 2, e+ 3).
+template <class R, int PT> static void enqueue_interactions(const Launch<R> &L, const Args<R> *A, cudaStream_t s)
+{
+  interact_for<R, PT, 0>(L)<<<L.grid, L.block, L.smem, s>>>(A);
+  interact_for<R, PT, 1>(L)<<<L.grid, L.block, L.smem, s>>>(A);
+  if (PT != 1) interact_for<R, PT, 2>(L)<<<L.grid, L.block, L.smem, s>>>(A);
+}
+
+// One iteration.  interact: this iteration runs the interaction kernels (the
+// compaction interval: otherwise the interacting tracks wait in their buffers).
+template <class R>
+static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, bool concurrent, bool interact = true)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
   if (L.a.nstores == 1) {
@@ -1927,7 +1981,7 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
     k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
     step_kernel_p<R>(kernel_kind(L.a.g))<<<L.grid, L.block, L.smem, s>>>(A);
-    k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
+    k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores, 1);
     return;
   }
   k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
@@ -1941,50 +1995,40 @@ template <class R> static void enqueue_iteration(const Launch<R> &L, Engine *e, 
     se = e->s1;
     sp = e->s2;
   }
-  const int kind = kernel_kind(L.a.g);
-  transport_kernel<R, 0>(kind)<<<L.grid, L.block, L.smem, sg>>>(A);
-  k_interact<R, 0, 0><<<L.grid, L.block, L.smem, sg>>>(A);
-  k_interact<R, 0, 1><<<L.grid, L.block, L.smem, sg>>>(A);
-  k_interact<R, 0, 2><<<L.grid, L.block, L.smem, sg>>>(A);
-  transport_kernel<R, 1>(kind)<<<L.grid, L.block, L.smem, se>>>(A);
-  k_interact<R, 1, 0><<<L.grid, L.block, L.smem, se>>>(A);
-  k_interact<R, 1, 1><<<L.grid, L.block, L.smem, se>>>(A);
-  transport_kernel<R, 2>(kind)<<<L.grid, L.block, L.smem, sp>>>(A);
-  k_interact<R, 2, 0><<<L.grid, L.block, L.smem, sp>>>(A);
-  k_interact<R, 2, 1><<<L.grid, L.block, L.smem, sp>>>(A);
-  k_interact<R, 2, 2><<<L.grid, L.block, L.smem, sp>>>(A);
+  transport_for<R, 0>(L)<<<L.grid, L.block, L.smem, sg>>>(A);
+  if (interact) enqueue_interactions<R, 0>(L, A, sg);
+  transport_for<R, 1>(L)<<<L.grid, L.block, L.smem, se>>>(A);
+  if (interact) enqueue_interactions<R, 1>(L, A, se);
+  transport_for<R, 2>(L)<<<L.grid, L.block, L.smem, sp>>>(A);
+  if (interact) enqueue_interactions<R, 2>(L, A, sp);
   if (concurrent) {
     cudaEventRecord(e->ev_j1, e->s1);
     cudaEventRecord(e->ev_j2, e->s2);
     cudaStreamWaitEvent(s, e->ev_j1, 0);
     cudaStreamWaitEvent(s, e->ev_j2, 0);
   }
-  k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
+  k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
+                           interact ? 1 : 0);
 }
 
 // One particle type's step (transport + its interactions), for the profiling
 // pass; `mid` is recorded between the transport kernel and the interactions.
-template <class R> static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q, cudaEvent_t mid)
+template <class R>
+static void enqueue_type(const Launch<R> &L, Engine *e, cudaStream_t s, int q, cudaEvent_t mid, bool interact = true)
 {
   const Args<R> *A = (const Args<R> *)e->dargs;
-  const int kind = kernel_kind(L.a.g);
   if (q == 0) {
-    transport_kernel<R, 0>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_for<R, 0>(L)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
-    k_interact<R, 0, 0><<<L.grid, L.block, L.smem, s>>>(A);
-    k_interact<R, 0, 1><<<L.grid, L.block, L.smem, s>>>(A);
-    k_interact<R, 0, 2><<<L.grid, L.block, L.smem, s>>>(A);
+    if (interact) enqueue_interactions<R, 0>(L, A, s);
   } else if (q == 1) {
-    transport_kernel<R, 1>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_for<R, 1>(L)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
-    k_interact<R, 1, 0><<<L.grid, L.block, L.smem, s>>>(A);
-    k_interact<R, 1, 1><<<L.grid, L.block, L.smem, s>>>(A);
+    if (interact) enqueue_interactions<R, 1>(L, A, s);
   } else {
-    transport_kernel<R, 2>(kind)<<<L.grid, L.block, L.smem, s>>>(A);
+    transport_for<R, 2>(L)<<<L.grid, L.block, L.smem, s>>>(A);
     cudaEventRecord(mid, s);
-    k_interact<R, 2, 0><<<L.grid, L.block, L.smem, s>>>(A);
-    k_interact<R, 2, 1><<<L.grid, L.block, L.smem, s>>>(A);
-    k_interact<R, 2, 2><<<L.grid, L.block, L.smem, s>>>(A);
+    if (interact) enqueue_interactions<R, 2>(L, A, s);
   }
 }
 
@@ -2214,7 +2258,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
   if (err != cudaSuccess) return cuda_error(err, "transport control init");
   // first refill plan
-  k_finish<<<1, 1, 0, s>>>(E->ctl, cap, cap, cap, nstores);
+  k_finish<<<1, 1, 0, s>>>(E->ctl, cap, cap, cap, nstores, 1);
   cudaEvent_t t0, t1;
   cudaEventCreate(&t0);
   cudaEventCreate(&t1);
@@ -2229,6 +2273,10 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     return cuda_error(err, "transport arguments upload");
   double step_ms[3] = {0, 0, 0}, transport_ms[3] = {0, 0, 0};
   long long step_launches[3] = {0, 0, 0};
+  // the compaction interval: the interaction kernels run (and their buffers
+  // are emptied into the stores) every `every` iterations; one iteration for
+  // the plain loop and for runs that hand their tracks over at the end
+  const int every = (batched && !tout && cfg->interaction_interval > 1) ? cfg->interaction_interval : 1;
   if (!batched || cfg->profile || max_iter > 0) {
     // plain loop (and the profiling pass, and runs stopped after a number of
     // iterations): launch, synchronise, look at the counters, every iteration
@@ -2249,13 +2297,14 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
                 (const Args<R> *)E->dargs);
             cudaEventRecord(em[q], s);
           } else {
-            enqueue_type(L, E, s, q, em[q]);
+            enqueue_type(L, E, s, q, em[q], (iters + 1) % every == 0);
           }
           cudaEventRecord(eb[q], s);
         }
-        k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores);
+        k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores,
+                                 (iters + 1) % every == 0 ? 1 : 0);
       } else {
-        enqueue_iteration(L, E, s, false);
+        enqueue_iteration(L, E, s, false, (iters + 1) % every == 0);
       }
       cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s);
       if ((err = cudaStreamSynchronize(s)) != cudaSuccess) return cuda_error(err, "transport iteration");
@@ -2280,10 +2329,11 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     }
   } else {
     int G = cfg->graph_iters > 0 ? cfg->graph_iters : 16;
+    G = ((G + every - 1) / every) * every; // whole compaction intervals
     // (re)capture the iteration graph when its launch shape or its kernels
     // (field kind, geometry kind) change; the arguments themselves are read
     // from the device copy uploaded above
-    int shape[6] = {G, L.block, L.grid, L.smem, kernel_kind(L.a.g), 0};
+    int shape[6] = {G, L.block, L.grid, L.smem, kernel_kind(L.a.g), every};
     std::vector<char> key(sizeof(shape) + 2 * sizeof(void *));
     const void *ptrs[2] = {E->dargs, E->ctl};
     std::memcpy(key.data(), shape, sizeof(shape));
@@ -2298,7 +2348,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
       cudaGraph_t graph;
       if ((err = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
         return cuda_error(err, "graph capture");
-      for (int k = 0; k < G; ++k) enqueue_iteration(L, E, cs, true);
+      for (int k = 0; k < G; ++k) enqueue_iteration(L, E, cs, true, (k + 1) % every == 0);
       cudaMemcpyAsync(E->h_ctl, E->ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, cs);
       if ((err = cudaStreamEndCapture(cs, &graph)) != cudaSuccess) return cuda_error(err, "graph capture end");
       err = cudaGraphInstantiate(&E->graph, graph, 0);
@@ -2707,8 +2757,14 @@ static int check_config(const Ctx *C, const gx_transport_config *cfg, int nvol, 
       cfg->engine > 1 || cfg->nevents < 1)
     return set_error(GX_ERR_ARG, "%s: bad config", who);
   if (cfg->box_mat < 0 || cfg->box_mat > 2) return set_error(GX_ERR_ARG, "%s: bad box material", who);
-  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 256))
-    return set_error(GX_ERR_ARG, "%s: block_size must be a multiple of 32, at most 256", who);
+  if (cfg->block_size && (cfg->block_size % 32 || cfg->block_size > 1024))
+    return set_error(GX_ERR_ARG, "%s: block_size must be a multiple of 32, at most 1024", who);
+  if (cfg->block_size > 256 && (cfg->engine != 1 || cfg->fp64_parity || cfg->geometry == 2 || cfg->msc ||
+                                cfg->field_map))
+    return set_error(GX_ERR_ARG, "%s: blocks above 256 threads are for the batched engine with the uniform field, "
+                                 "layered geometry and no multiple scattering", who);
+  if (cfg->interaction_interval < 0 || cfg->interaction_interval > 64)
+    return set_error(GX_ERR_ARG, "%s: interaction_interval must be 0 .. 64", who);
   if (cfg->field_map && !C->host.fmap)
     return set_error(GX_ERR_ARG, "%s: field_map = 1 without a field map (gx_ctx_load_field_map)", who);
   if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "%s: bad geometry", who);
@@ -3030,7 +3086,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
       (err = cudaStreamSynchronize(s)) != cudaSuccess)
     return cuda_error(err, "gx_transport_run_noalloc: control block");
   if (nprim > 0) k_prefix_energy<<<1, 1024, 0, s>>>(d_E, nprim, cumE, nullptr);
-  k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
+  k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, 1);
   Ctl hc;
   long long iters = 0;
   for (;;) {
@@ -3038,7 +3094,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
     k_refill_done<<<1, 1, 0, s>>>(ctl);
     (cfg->msc ? (cfg->field_map ? k_step<double, 3, 5> : k_step<double, 3, 4>)
               : (cfg->field_map ? k_step<double, 3, 1> : k_step<double, 3, 0>))<<<L.grid, L.block, L.smem, s>>>(L.a);
-    k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1);
+    k_finish<<<1, 1, 0, s>>>(ctl, cap, cap, cap, 1, 1);
     if ((err = cudaGetLastError()) != cudaSuccess) return cuda_error(err, "gx_transport_run_noalloc: launch");
     if ((err = cudaMemcpyAsync(&hc, ctl, sizeof(Ctl), cudaMemcpyDeviceToHost, s)) != cudaSuccess ||
         (err = cudaStreamSynchronize(s)) != cudaSuccess)

@@ -70,7 +70,9 @@ def main(argv=None):
         out["field_map"] = "cms"
     if a.autotune:
         cfg.profile = 0
-        out["autotune"] = gx.autotune(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)[0]
+        trials = gx.autotune(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)
+        out["autotune"] = trials[0]
+        out["autotune_trials"] = trials
         cfg.profile = int(a.profile)
     for _ in range(a.repeat):
         edep, st, _ = gx.transport(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)

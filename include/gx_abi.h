@@ -266,7 +266,8 @@ typedef struct {
   /* engine */
   int precision;           /* 0 FP64, 1 FP32-mixed */
   int engine;              /* 0 plain loop (one mixed queue, host-driven), 1 batched (per-type queues, graph) */
-  int block_size;          /* threads per block (0: default) */
+  int block_size;          /* threads per block (0: default); above 256 (up to 1024) only for the batched
+                              engine with the uniform field, layered geometry and no multiple scattering */
   int blocks_per_sm;       /* resident blocks per SM for the grid (0: default) */
   long long capacity;      /* track slots per particle type (0: default) */
   long long refill_below;  /* inject / refill when fewer tracks than this are in flight (0: default) */
@@ -284,6 +285,10 @@ typedef struct {
                               Runge-Kutta sub-steps, Bz ignored; 0: uniform Bz with the helix */
   int steps_per_launch_by_type[3]; /* batched engine: steps per transport launch for gamma, e-, e+
                               (0: from steps_per_launch; e+ a quarter of it, at least 1) */
+  int interaction_interval; /* batched engine: the compaction interval -- tracks that reach an interaction wait
+                              in their per-process buffers and the interaction kernels, which compact their
+                              survivors and secondaries back into the stores, run every this many iterations
+                              (0 or 1: every iteration).  Results do not depend on it. */
   int fp64_parity;         /* 1 (precision 0 only): the FP64 parity variant -- no contraction, the reference's
                               spline and ionisation forms, the general helix step and the elementary functions
                               of gx_math.h, the operations of the CPU oracle in its order, so that the two
@@ -516,16 +521,19 @@ int gx_transport_tracks(gx_ctx *ctx, const gx_transport_config *cfg, const gx_tr
  * reference (its kernels take nblocks / nthreads from the caller,
  * source/Geant/kernel/KernelPhysicsProcess.cuh:22-36).  Transports the given
  * primaries (the whole batch, or a representative subset of it) once per
- * candidate: block size {64, 128, 256} x resident blocks per SM {1, 2, 4, 8},
- * then steps per track and transport launch {1, 16, 64, 1024}, then
- * iterations per CUDA-graph launch {4, 8, 32, 64}, then the refill
- * threshold {1/8, 1/4, 3/4 of the capacity}, then the primary energy per
- * injection wave {1/4, 1/2, 2 x the default}, each coordinate from the best so
- * far.  Score: track-steps per millisecond of device time, best of `repeats`
- * runs (at least 1; the first run of a new launch shape includes its graph
- * capture).  Writes the winner into cfg->block_size, blocks_per_sm,
- * steps_per_launch, graph_iters, refill_below and wave_energy; report (optional) lists every
- * trial.  cfg->engine must be 1; the precision and capacity are kept. */
+ * candidate: block size {64, 128, 256, 512, 1024} (512 and 1024 with the
+ * uniform field, layered geometry and no multiple scattering, at most 4096
+ * threads per SM) x resident blocks per SM {1, 2, 4, 8}, then steps per track
+ * and transport launch {1, 16, 64, 1024}, then iterations per CUDA-graph
+ * launch {4, 8, 32, 64}, then the refill threshold {1/8, 1/4, 3/4 of the
+ * capacity}, then the primary energy per injection wave {1/4, 1/2, 2 x the
+ * default}, then the compaction interval (interaction_interval) {2, 4, 8},
+ * each coordinate from the best so far.  Score: track-steps per millisecond of
+ * device time, best of `repeats` runs (at least 1; the first run of a new
+ * launch shape includes its graph capture).  Writes the winner into
+ * cfg->block_size, blocks_per_sm, steps_per_launch, graph_iters,
+ * refill_below, wave_energy and interaction_interval; report (optional) lists
+ * every trial.  cfg->engine must be 1; the precision and capacity are kept. */
 #define GX_AUTOTUNE_MAX_TRIALS 64
 typedef struct {
   int trials, best; /* number of trials listed; index of the winner */
@@ -533,6 +541,7 @@ typedef struct {
   int steps_per_launch[GX_AUTOTUNE_MAX_TRIALS], graph_iters[GX_AUTOTUNE_MAX_TRIALS];
   long long refill_below[GX_AUTOTUNE_MAX_TRIALS];
   double wave_energy[GX_AUTOTUNE_MAX_TRIALS];
+  int interaction_interval[GX_AUTOTUNE_MAX_TRIALS];
   double kernel_ms[GX_AUTOTUNE_MAX_TRIALS];    /* device time, best of the repeats (0: did not complete) */
   double steps_per_ms[GX_AUTOTUNE_MAX_TRIALS]; /* track-steps per device millisecond */
 } gx_autotune_report;
