@@ -509,6 +509,8 @@ int gx_ctx_destroy(gx_ctx *ctx)
   release_engine(c);
   parity::release_engine(c);
   for (void *p : c->owned) cudaFree(p);
+  if (c->host_buf) cudaFree(c->host_buf);
+  if (c->host_stream) cudaStreamDestroy(c->host_stream);
   delete c;
   return GX_OK;
 }

@@ -132,6 +132,17 @@ struct Mrg {
 #pragma unroll
     for (int k = 0; k < 6; ++k) st[k * n + i] = (uint32_t)s[k];
   }
+  // the state as six words (a track carries it so: 6 registers, not 12)
+  __device__ __forceinline__ void from_words(const uint32_t w[6])
+  {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s[k] = (double)w[k];
+  }
+  __device__ __forceinline__ void to_words(uint32_t w[6]) const
+  {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[k] = (uint32_t)s[k];
+  }
   // draw numerator z in [1, m1]
   __device__ __forceinline__ double next()
   {

@@ -28,6 +28,10 @@ struct Ctx {
   double *csg_planes = nullptr;
   int csg_n = 0, csg_nscore = 0;
   double *stage_scratch = nullptr; // escaped energy of the stage calls (gx_along_step)
+  // gx_transport_run_host: its stream and device staging buffer, kept across calls
+  cudaStream_t host_stream = nullptr;
+  void *host_buf = nullptr;
+  size_t host_buf_bytes = 0;
 };
 
 int set_error(int code, const char *fmt, ...);

@@ -407,8 +407,25 @@ template <class R> struct Track {
   int type, vol, event, prim;
   double pos[3];
   R dir[3], E, nil[3];
-  R msc_r0; // multiple scattering: range scale of the step limit in this volume (<= 0: unset)
-  Mrg rng;
+  R msc_r0;       // multiple scattering: range scale of the step limit in this volume (<= 0: unset)
+  uint32_t rs[6]; // MRG32k3a state words; draws go through a Mrg made from them (rng / set_rng)
+  __device__ __forceinline__ Mrg rng() const
+  {
+    Mrg m;
+    m.from_words(rs);
+    return m;
+  }
+  __device__ __forceinline__ void set_rng(const Mrg &m) { m.to_words(rs); }
+  __device__ __forceinline__ void load_rng(const uint32_t *st, long long n, long long i)
+  {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) rs[k] = __ldg(&st[k * n + i]);
+  }
+  __device__ __forceinline__ void store_rng(uint32_t *st, long long n, long long i) const
+  {
+#pragma unroll
+    for (int k = 0; k < 6; ++k) st[k * n + i] = rs[k];
+  }
 };
 
 struct Local {
@@ -515,27 +532,29 @@ __device__ __forceinline__ void run_model(const Data &d, const Geom &g, Track<R>
   io.status = 0;
   io.nsec = 0;
   int err = 0;
+  Mrg rng = t.rng();
   if (t.type == 0) {
     if (proc == 0)
-      kn_sample(t.rng, mp, io, &err);
+      kn_sample(rng, mp, io, &err);
     else if (proc == 1) {
-      bh_sample(t.rng, mp, io, &err);
+      bh_sample(rng, mp, io, &err);
       if (io.nsec == 2) L.st[S_PAIR]++;
     } else
-      sg_sample(t.rng, d, mp, io, &err);
+      sg_sample(rng, d, mp, io, &err);
   } else if (proc == 0) {
     mp.cut = d.cut_energy[1][mat];
     if (t.type == 1)
-      mb_sample(t.rng, mp, io, &err);
+      mb_sample(rng, mp, io, &err);
     else
-      bhabha_sample(t.rng, mp, io, &err);
+      bhabha_sample(rng, mp, io, &err);
   } else if (proc == 1) {
     mp.cut = d.cut_energy[0][mat];
-    sb_sample(t.rng, mp, io, &err);
+    sb_sample(rng, mp, io, &err);
   } else {
-    annih_sample(t.rng, io, &err);
+    annih_sample(rng, io, &err);
     L.st[S_ANNIH]++;
   }
+  t.set_rng(rng);
   if (err) {
     L.err |= err;
     L.st[S_ERR]++;
@@ -695,11 +714,16 @@ template <class R>
 __device__ __forceinline__ bool msc_deflect(const Data &d, Track<R> &t, int mat, R step, R lam0, R e0, R &sp, R &cp)
 {
   const R lam1 = msc_lambda1<R>(d, t.type, mat, t.E);
-  R ct = msc_cos_theta<R>(t.rng, d.mat_msc[mat], step, lam0, lam1, e0, t.E);
-  if (!(ct < R(1))) return false;
+  Mrg rng = t.rng();
+  R ct = msc_cos_theta<R>(rng, d.mat_msc[mat], step, lam0, lam1, e0, t.E);
+  if (!(ct < R(1))) {
+    t.set_rng(rng);
+    return false;
+  }
   if (ct < R(-1)) ct = R(-1);
   const R st = M<R>::sqrt((R(1) - ct) * (R(1) + ct));
-  M<R>::sincos2pi(t.rng.template u<R>(), &sp, &cp);
+  M<R>::sincos2pi(rng.template u<R>(), &sp, &cp);
+  t.set_rng(rng);
   R u = st * cp, v = st * sp, w = ct;
   rotate_to_lab(u, v, w, t.dir[0], t.dir[1], t.dir[2]);
   t.dir[0] = u;
@@ -807,9 +831,17 @@ __device__ __forceinline__ R step_gpil(const Data &d, const Geom &g, Track<R> &t
   c.xs2 = xs[2];
   // loops over the three process slots are unrolled with the bound as a guard,
   // so xs[] and nil[] are indexed by constants and stay in registers
+  bool draw = false;
 #pragma unroll
   for (int i = 0; i < 3; ++i)
-    if (i < np && t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(t.rng.template u<R>());
+    if (i < np && t.nil[i] <= R(0)) draw = true;
+  if (draw) {
+    Mrg rng = t.rng();
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+      if (i < np && t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(rng.template u<R>());
+    t.set_rng(rng);
+  }
   R pstep = R(3.0e38);
   int sel = -1;
 #pragma unroll
@@ -1176,7 +1208,7 @@ template <class R> __device__ __forceinline__ void load_track(const Store<R> &s,
   t.nil[1] = s.n1[i];
   t.nil[2] = s.n2[i];
   t.msc_r0 = s.r0[i];
-  t.rng.load(s.rng, s.cap, i);
+  t.load_rng(s.rng, s.cap, i);
   t.vol = s.vol[i];
   t.event = s.event[i];
   t.prim = s.prim[i];
@@ -1195,7 +1227,7 @@ template <class R> __device__ __forceinline__ void store_track(const Store<R> &s
   s.n1[i] = t.nil[1];
   s.n2[i] = t.nil[2];
   s.r0[i] = t.msc_r0;
-  t.rng.store(s.rng, s.cap, i);
+  t.store_rng(s.rng, s.cap, i);
   s.vol[i] = t.vol;
   s.event[i] = t.event;
   s.prim[i] = t.prim;
@@ -1322,6 +1354,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
   for (int q = 0; q < 3; ++q)
     next[q] = (q < a.nstores) ? warp_reserve((unsigned long long *)&ctl->count[par ^ 1][q], cnt[q]) : 0;
   if (!active) return;
+  Mrg rng = t.rng();
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     if (k >= sec.n) break;
@@ -1336,7 +1369,9 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
     c.E = sec.E[k];
     c.nil[0] = c.nil[1] = c.nil[2] = R(-1);
     c.msc_r0 = R(-1);
-    t.rng.seed_child(c.rng);
+    Mrg cr;
+    rng.seed_child(cr);
+    c.set_rng(cr);
     c.vol = t.vol;
     c.event = t.event;
     c.prim = -1;
@@ -1349,6 +1384,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
     L.st[S_SEC2] = sc[2];
     L.st[S_WRITE0 + SRC]++;
   }
+  t.set_rng(rng);
   if (alive) {
     const int q = mixed ? 0 : t.type;
     put_track(a, q, take3(next, q, 1LL), t, L);
@@ -1748,7 +1784,7 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
       t.nil[1] = (R)q.nil1[pi];
       t.nil[2] = (R)q.nil2[pi];
       t.msc_r0 = q.msc ? (R)q.msc[pi] : R(-1);
-      t.rng.load(q.rng, q.cap, pi);
+      t.load_rng(q.rng, q.cap, pi);
       t.vol = q.volume[pi];
       if (t.vol < -1) {
         double dd[3] = {q.dx[pi], q.dy[pi], q.dz[pi]};
@@ -1778,8 +1814,8 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
           jump_matvec(a.p.jump + 9 * (64 + b), v2, 4294944443ULL);
         }
       for (int k = 0; k < 3; ++k) {
-        t.rng.s[k] = (double)v1[k];
-        t.rng.s[3 + k] = (double)v2[k];
+        t.rs[k] = (uint32_t)v1[k];
+        t.rs[3 + k] = (uint32_t)v2[k];
       }
     }
     atomicAdd(&ctl->stat[S_TRACKS], 1ULL);
@@ -1967,7 +2003,7 @@ template <class R, int PT> static void enqueue_interactions(const Launch<R> &L, 
 {
   interact_for<R, PT, 0>(L)<<<L.grid, L.block, L.smem, s>>>(A);
   interact_for<R, PT, 1>(L)<<<L.grid, L.block, L.smem, s>>>(A);
-  if (PT != 1) interact_for<R, PT, 2>(L)<<<L.grid, L.block, L.smem, s>>>(A);
+  if constexpr (PT != 1) interact_for<R, PT, 2>(L)<<<L.grid, L.block, L.smem, s>>>(A);
 }
 
 // One iteration.  interact: this iteration runs the interaction kernels (the
@@ -2063,7 +2099,7 @@ __global__ void k_extract(Store<R> src, long long n, int ptype, Ctl *ctl, gx_tra
     out.lambda_inv0[j] = out.lambda_inv1[j] = out.lambda_inv2[j] = 0.0;
     out.pstep[j] = out.step[j] = out.snext[j] = out.safety[j] = 0.0;
     if (out.msc_range) out.msc_range[j] = (double)t.msc_r0;
-    t.rng.store(out.rng, out.capacity, j);
+    t.store_rng(out.rng, out.capacity, j);
   }
 }
 
@@ -2473,7 +2509,7 @@ __device__ __forceinline__ void soa_load(const gx_track_soa &s, int i, Track<dou
   t.nil[1] = s.nil1[i];
   t.nil[2] = s.nil2[i];
   t.msc_r0 = s.msc_range ? s.msc_range[i] : -1.0;
-  t.rng.load(s.rng, s.capacity, i);
+  t.load_rng(s.rng, s.capacity, i);
   t.vol = s.volume[i];
   t.event = s.event ? s.event[i] : 0;
   t.prim = s.primary ? s.primary[i] : -1;
@@ -2493,7 +2529,7 @@ __device__ __forceinline__ void soa_store(const gx_track_soa &s, int i, const Tr
   s.nil1[i] = t.nil[1];
   s.nil2[i] = t.nil[2];
   if (s.msc_range) s.msc_range[i] = t.msc_r0;
-  t.rng.store(s.rng, s.capacity, i);
+  t.store_rng(s.rng, s.capacity, i);
   s.volume[i] = t.vol;
 }
 
@@ -2609,6 +2645,7 @@ template <int K> __global__ void __launch_bounds__(128) k_stage_post(StageArgs a
     Local L;
     stage_local(L, a);
     run_model(*a.d, a.g, t, a.t.process[i], sec, L);
+    Mrg rng = t.rng();
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
       if (k >= sec.n) break;
@@ -2623,7 +2660,9 @@ template <int K> __global__ void __launch_bounds__(128) k_stage_post(StageArgs a
       ch.E = sec.E[k];
       ch.nil[0] = ch.nil[1] = ch.nil[2] = -1.0;
       ch.msc_r0 = -1.0;
-      t.rng.seed_child(ch.rng);
+      Mrg cr;
+      rng.seed_child(cr);
+      ch.set_rng(cr);
       ch.vol = t.vol;
       ch.event = t.event;
       ch.prim = -1;
@@ -2640,6 +2679,7 @@ template <int K> __global__ void __launch_bounds__(128) k_stage_post(StageArgs a
       a.sec.pstep[j] = a.sec.step[j] = a.sec.snext[j] = a.sec.safety[j] = 0.0;
       ++nsec;
     }
+    t.set_rng(rng);
     soa_store(a.t, i, t);
     a.t.process[i] = -1;
     a.t.status[i] = t.E > 0.0 ? GX_TRACK_ALIVE : GX_TRACK_KILLED;
@@ -2873,49 +2913,47 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
                           const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
                           double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats)
 {
-  if (!ctx || !cfg || nprim < 0 || !h_edep || nvol <= 0) return set_error(GX_ERR_ARG, "gx_transport_run_host: bad arguments");
+  if (!ctx || !cfg || nprim < 0 || !h_edep || nvol <= 0 || (nprim > 0 && (!h_type || !h_E || !h_pos || !h_dir)))
+    return set_error(GX_ERR_ARG, "gx_transport_run_host: bad arguments");
   Ctx *C = reinterpret_cast<Ctx *>(ctx);
   cudaSetDevice(C->device);
-  size_t n = (size_t)(nprim > 0 ? nprim : 1), nt = (size_t)cfg->nevents * nvol;
-  int *dt = nullptr, *dev = nullptr, *dps = nullptr;
-  double *dE = nullptr, *dp = nullptr, *dd = nullptr, *ded = nullptr;
-  cudaStream_t s;
-  cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
-  cudaError_t e = cudaSuccess;
-  int rc = GX_OK;
-  if ((e = cudaMallocAsync((void **)&dt, n * sizeof(int), s)) || (e = cudaMallocAsync((void **)&dE, n * sizeof(double), s)) ||
-      (e = cudaMallocAsync((void **)&dp, 3 * n * sizeof(double), s)) ||
-      (e = cudaMallocAsync((void **)&dd, 3 * n * sizeof(double), s)) ||
-      (e = cudaMallocAsync((void **)&ded, nt * sizeof(double), s)))
-    rc = cuda_error(e, "gx_transport_run_host alloc");
-  if (!rc && h_event && (e = cudaMallocAsync((void **)&dev, n * sizeof(int), s))) rc = cuda_error(e, "alloc");
-  if (!rc && h_primary_steps && (e = cudaMallocAsync((void **)&dps, n * sizeof(int), s))) rc = cuda_error(e, "alloc");
-  if (!rc && nprim > 0) {
+  const size_t n = (size_t)(nprim > 0 ? nprim : 1), nt = (size_t)cfg->nevents * nvol;
+  // one staging buffer and one stream kept by the context, grown when a call
+  // needs more: no allocation, no stream creation per call
+  auto pad = [](size_t b) { return (b + 255) & ~size_t(255); };
+  const size_t b_int = pad(n * sizeof(int)), b_dbl = pad(n * sizeof(double)), b_vec = pad(3 * n * sizeof(double));
+  const size_t need = 3 * b_int + 2 * b_vec + b_dbl + pad(nt * sizeof(double));
+  cudaError_t e;
+  if (!C->host_stream && (e = cudaStreamCreateWithFlags(&C->host_stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return cuda_error(e, "gx_transport_run_host: stream");
+  if (need > C->host_buf_bytes) {
+    if (C->host_buf) cudaFree(C->host_buf);
+    C->host_buf = nullptr;
+    C->host_buf_bytes = 0;
+    if ((e = cudaMalloc(&C->host_buf, need)) != cudaSuccess) return cuda_error(e, "gx_transport_run_host: staging");
+    C->host_buf_bytes = need;
+  }
+  cudaStream_t s = C->host_stream;
+  char *b = (char *)C->host_buf;
+  int *dt = (int *)b, *dev = (int *)(b + b_int), *dps = (int *)(b + 2 * b_int);
+  double *dp = (double *)(b + 3 * b_int), *dd = (double *)(b + 3 * b_int + b_vec);
+  double *dE = (double *)(b + 3 * b_int + 2 * b_vec), *ded = (double *)(b + 3 * b_int + 2 * b_vec + b_dbl);
+  if (nprim > 0) {
     cudaMemcpyAsync(dt, h_type, nprim * sizeof(int), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dE, h_E, nprim * sizeof(double), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dp, h_pos, 3 * nprim * sizeof(double), cudaMemcpyHostToDevice, s);
     cudaMemcpyAsync(dd, h_dir, 3 * nprim * sizeof(double), cudaMemcpyHostToDevice, s);
-    if (dev) cudaMemcpyAsync(dev, h_event, nprim * sizeof(int), cudaMemcpyHostToDevice, s);
+    if (h_event) cudaMemcpyAsync(dev, h_event, nprim * sizeof(int), cudaMemcpyHostToDevice, s);
   }
-  if (!rc) {
-    cudaMemsetAsync(ded, 0, nt * sizeof(double), s);
-    if (dps) cudaMemsetAsync(dps, 0, n * sizeof(int), s);
-    rc = gx_transport_run(ctx, cfg, nprim, dt, dE, dp, dd, dev, ded, nvol, dps, stats, reinterpret_cast<gx_stream_t>(s));
-  }
+  cudaMemsetAsync(ded, 0, nt * sizeof(double), s);
+  if (h_primary_steps) cudaMemsetAsync(dps, 0, n * sizeof(int), s);
+  int rc = gx_transport_run(ctx, cfg, nprim, dt, dE, dp, dd, h_event ? dev : nullptr, ded, nvol,
+                            h_primary_steps ? dps : nullptr, stats, reinterpret_cast<gx_stream_t>(s));
   if (!rc) {
     cudaMemcpyAsync(h_edep, ded, nt * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (dps) cudaMemcpyAsync(h_primary_steps, dps, nprim * sizeof(int), cudaMemcpyDeviceToHost, s);
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) rc = cuda_error(e, "gx_transport_run_host copy back");
+    if (h_primary_steps) cudaMemcpyAsync(h_primary_steps, dps, nprim * sizeof(int), cudaMemcpyDeviceToHost, s);
   }
-  cudaFreeAsync(dt, s);
-  cudaFreeAsync(dE, s);
-  cudaFreeAsync(dp, s);
-  cudaFreeAsync(dd, s);
-  cudaFreeAsync(ded, s);
-  if (dev) cudaFreeAsync(dev, s);
-  if (dps) cudaFreeAsync(dps, s);
-  cudaStreamSynchronize(s);
-  cudaStreamDestroy(s);
+  if ((e = cudaStreamSynchronize(s)) != cudaSuccess && !rc) rc = cuda_error(e, "gx_transport_run_host copy back");
   return rc;
 }
 

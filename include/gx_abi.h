@@ -329,7 +329,9 @@ int gx_transport_run(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, con
                      const double *d_E, const double *d_pos, const double *d_dir, const int *d_event,
                      double *d_edep, int nvol, int *d_primary_steps, gx_transport_stats *stats, gx_stream_t s);
 /* The same from host buffers: copies the primaries in and the tallies out
- * inside the call (h_edep is overwritten). */
+ * inside the call (h_edep is overwritten).  The context keeps the stream and
+ * the device staging buffer of these calls (grown when a call needs more), so
+ * a call allocates nothing once the context has seen its size.  Synchronous. */
 int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim, const int *h_type,
                           const double *h_E, const double *h_pos, const double *h_dir, const int *h_event,
                           double *h_edep, int nvol, int *h_primary_steps, gx_transport_stats *stats);

@@ -211,11 +211,14 @@ def test_wide_blocks_and_compaction_interval_leave_results_unchanged(dm, precisi
     runs = [run_gpu(dm, cfg, prims, nvol, precision=precision, primary_steps=True, block_size=b, blocks_per_sm=bp,
                     interaction_interval=k) for b, bp, k in ((512, 2, 0), (1024, 1, 0), (128, 4, 3), (1024, 2, 4))]
     cfg.block_size, cfg.blocks_per_sm, cfg.interaction_interval = 0, 0, 0
+    # FP64 to rounding of the sums; FP32-mixed to float rounding (the wide
+    # variants are compiled apart, their float operations may contract differently)
+    tol = 1e-9 if precision == 0 else 1e-5
     for e, st, ps in runs:
         assert st["errors"] == 0
         assert st["steps"] == ref[1]["steps"] and st["tracks"] == ref[1]["tracks"]
         assert np.array_equal(ps, ref[2])
-        np.testing.assert_allclose(e, ref[0], rtol=1e-9, atol=1e-9 * ref[0].max())
+        np.testing.assert_allclose(e, ref[0], rtol=tol, atol=tol * ref[0].max())
     assert runs[2][1]["iterations"] >= ref[1]["iterations"]
 
 
