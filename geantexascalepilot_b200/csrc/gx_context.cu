@@ -335,6 +335,7 @@ int load_data(const char *datadir, Ctx *ctx)
   double rcl, lc, alpha;
   em_constants(&rcl, &lc, &alpha);
   d.pi_rcl2 = kPi * rcl * rcl;
+  d.alpha = alpha;
   material(d, 0, 1.0, 1.01, 1.e-25, rcl, lc, alpha);   // Galactic
   material(d, 1, 82.0, 207.2, 11.35, rcl, lc, alpha);  // G4_Pb
   material(d, 2, 18.0, 39.95, 1.396, rcl, lc, alpha);  // G4_lAr

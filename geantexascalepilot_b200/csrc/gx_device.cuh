@@ -214,6 +214,7 @@ struct Data {
   // model's Z-dependent constants {X0, th1, th2, ca, cb, cc, cd}
   double mat_msc[kNMat][7];
   double pi_rcl2; // pi r_e^2, mm^2
+  double alpha;   // the fine-structure constant
   // field map (optional, gx_ctx_load_field_map): (Br, Bphi, Bz) on an r-z
   // lattice, r outer, each premultiplied by 1 / (dr dz) as the reference's
   // reader stores them; null when no map is loaded

@@ -56,6 +56,59 @@ def test_built_tables_match_shipped(dm, mat):
         np.testing.assert_allclose(built, y[sel], rtol=tol, err_msg=name)
 
 
+@pytest.mark.parametrize("mat", [1, 2])
+def test_built_pair_and_photoelectric_tables_within_their_model_bands(dm, mat):
+    """Tables the reference has no per-atom cross section for, built from the
+    samplers' own physics: pairs from the Bethe-Heitler differential cross
+    section with Tsai's screening and triplet terms -- within 6% of the shipped
+    Geant4 table from 50 MeV to 10 TeV, within 15% from 10 to 50 MeV (the Born
+    approximation); photo-electric from the Sandia parameterisation -- within
+    6% (lead) and 20% (argon, whose shipped table comes from another
+    photo-electric model) from 200 keV up."""
+    import geantexascalepilot_b200 as gx
+    x, y = _nodes("Lambda.conv.gamma", mat)
+    for lo, hi, tol in ((50.0, 1e7, 0.06), (10.0, 50.0, 0.15)):
+        sel = (x >= lo) & (x <= hi) & (y > 0)
+        built = dm.table_build(gx.TABLES.index("Lambda.conv.gamma"), mat, x[sel]).cpu().numpy()
+        np.testing.assert_allclose(built, y[sel], rtol=tol)
+    x, y = _nodes("LambdaPrim.phot.gamma", mat)
+    sel = (x >= 0.2) & (y > 0)
+    built = dm.table_build(gx.TABLES.index("LambdaPrim.phot.gamma"), mat, x[sel]).cpu().numpy()
+    ratio = built / y[sel]
+    if mat == 1:
+        assert np.all(np.abs(ratio - 1) < 0.06)
+    else:
+        assert np.all((ratio > 0.8) & (ratio < 0.9))
+
+
+def test_pair_integral_against_cpu(dm):
+    """The device's Bethe-Heitler quadrature against the same integral in
+    numpy (the sampler's screening functions, 8 x 8 Gauss-Legendre points)."""
+    import geantexascalepilot_b200 as gx
+    E = _grid(3.0, 1e6, 16)
+    built = dm.table_build(gx.TABLES.index("Lambda.conv.gamma"), 1, E).cpu().numpy()
+    Z, alpha, re = 82.0, 7.2973525376e-3, 2.8179402894e-12
+    n_atoms = 6.02214179e23 * 11.35 / 207.2 * 1e-3
+    az2 = (Z / 137.0) ** 2
+    fc = (0.0083 * az2 * az2 + 0.20206 + 1 / (1 + az2)) * az2 - (0.0020 * az2 * az2 + 0.0369) * az2 * az2
+    s1 = lambda d: np.where(d > 1, 42.24 - 8.368 * np.log(d + 0.952), 42.392 - d * (7.796 - 1.961 * d))
+    s2 = lambda d: np.where(d > 1, 42.24 - 8.368 * np.log(d + 0.952), 41.405 - d * (5.828 - 0.8945 * d))
+    xg, wg = np.polynomial.legendre.leggauss(8)
+    xg, wg = 0.5 * (xg + 1), 0.5 * wg
+    Z3 = Z ** (1 / 3)
+    xi = np.log(1440 / Z3 ** 2) / (np.log(183 / Z3) - fc)
+    for k, e in enumerate(E):
+        eps0 = ME / e
+        FZ = 8 * np.log(Z) / 3 + (8 * fc if e > 50 else 0)
+        h = (0.5 - eps0) / 8
+        eps = eps0 + (np.arange(8)[:, None] + xg[None, :]) * h
+        u = eps * (1 - eps)
+        d = 136 * eps0 / (Z3 * u)
+        f = (eps ** 2 + (1 - eps) ** 2) * np.maximum(s1(d) - FZ, 0) + 2 / 3 * u * np.maximum(s2(d) - FZ, 0)
+        ref = n_atoms * alpha * re * re * Z * (Z + xi) * (f * wg[None, :]).sum() * h
+        assert built[k] == pytest.approx(ref, rel=1e-6)
+
+
 def test_bhabha_and_brems_integrals_against_cpu(dm, oracle):
     """The device quadratures against the same integrals done in numpy
     (Bhabha analytically, Seltzer-Berger with 8 x 16 Gauss-Legendre points
@@ -102,7 +155,7 @@ def test_rebuilt_tables_and_computed_cuts_run_showers():
         dm = gx.ProxyDataManager()
         if rebuild:
             change = dm.rebuild_tables()
-            assert change < 0.01
+            assert change < 0.25  # the worst table: argon photo-electric (Sandia against the Geant4 build)
             dm.compute_cuts(0.7)
             v = ctypes.c_double()  # file-order entry 4 = e- in lead (see above)
             assert gx._lib.lib.gx_cut_value(dm.handle, 0, 1, ctypes.byref(v)) == 0
