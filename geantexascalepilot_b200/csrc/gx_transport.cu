@@ -354,14 +354,18 @@ template <class R> __device__ __forceinline__ void cross_sections(const Data &d,
     if (!(xs[i] > R(0))) xs[i] = R(0);
 }
 
-// ProxyIonization::AlongStepGPIL in physics mode (Geant4 step function, length cut)
-template <class R> __device__ __forceinline__ R range_limit(const Data &d, int type, int mat, R e)
+// ProxyIonization::AlongStepGPIL in physics mode (Geant4 step function, length
+// cut); raw: the range table's value at e, which the step's continuous loss
+// reuses (the energy does not change before it)
+template <class R> __device__ __forceinline__ R range_limit(const Data &d, int type, int mat, R e, R &raw)
 {
 #ifdef GX_PARITY
+  raw = R(-1);
   return ioni_along_gpil_ref(d, 1, type == 2 ? 1 : -1, mat, e);
 #endif
   const R dR = R(0.2), finalRange = R(10.0);
   R range = vec_value_fast<R>(d, d.vec[type == 2 ? GX_Range_ep : GX_Range_em][mat], e);
+  raw = range;
   if (e < R(kMinE)) range *= e / R(kMinE);
   R cut = (R)d.cut_length[1][mat];
   R finR = (finalRange < cut) ? finalRange : cut;
@@ -371,7 +375,9 @@ template <class R> __device__ __forceinline__ R range_limit(const Data &d, int t
 
 // ProxyIonization::AlongStepDoIt in physics mode; the inverse range (used when
 // the loss exceeds 1%, i.e. near the end of the range) is evaluated in FP64.
-template <class R> __device__ __forceinline__ R along_loss(const Data &d, int type, int mat, double step, R &e)
+// range0 >= 0: the range table's value at e, taken at the start of the step.
+template <class R>
+__device__ __forceinline__ R along_loss(const Data &d, int type, int mat, double step, R &e, R range0 = R(-1))
 {
 #ifdef GX_PARITY
   double edep = 0.0, ee = e;
@@ -381,7 +387,7 @@ template <class R> __device__ __forceinline__ R along_loss(const Data &d, int ty
 #endif
   bool ep = type == 2;
   R energy = e;
-  R range = vec_value_fast<R>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], energy);
+  R range = range0 >= R(0) ? range0 : vec_value_fast<R>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], energy);
   if (step >= (double)range || energy <= R(kMinE)) {
     e = R(0);
     return energy;
@@ -781,6 +787,7 @@ template <class R> struct StepCtx {
   // mean free path and energy at the start, the step's true length
   R lam0, e0;
   double ttrue;
+  R range0; // charged: the range table's value at the step's energy (-1: none)
   __device__ __forceinline__ R xs(int i) const { return i == 0 ? xs0 : (i == 1 ? xs1 : xs2); }
 };
 
@@ -853,8 +860,9 @@ __device__ __forceinline__ R step_gpil(const Data &d, const Geom &g, Track<R> &t
         sel = i;
       }
     }
+  c.range0 = R(-1);
   if (charged) {
-    R slim = range_limit<R>(d, t.type, mat, t.E);
+    R slim = range_limit<R>(d, t.type, mat, t.E, c.range0);
     if (slim < pstep) {
       pstep = slim;
       sel = -1;
@@ -1118,7 +1126,7 @@ __device__ __forceinline__ int step_end(const Data &d, const Geom &g, Track<R> &
     return kDone;
   }
   if (t.type != 0) {
-    R eloss = along_loss<R>(d, t.type, vol_material(g, c.vol0), step, t.E);
+    R eloss = along_loss<R>(d, t.type, vol_material(g, c.vol0), step, t.E, c.range0);
     L.deposit(t.event, c.vol0, (double)eloss);
     if (t.E <= R(0)) {
       if (t.type == 2) {
@@ -1506,12 +1514,18 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
         const long long i = (long long)base + __popc(need & lanemask_lt());
         if (i < n) {
           load_track(cur, i, PT, t);
-          L.st[S_READ0 + PT]++;
-          L.st[S_TREAD0 + PT]++;
           have = true;
           infield = false;
           nst = 0;
           gxs.have = 0; // a new photon energy
+        }
+      }
+      // records read: counted per warp (no per-thread counters held across the loop)
+      if ((int)lane_id() == leader) {
+        const long long got = min((long long)__popc(need), n - (long long)base);
+        if (got > 0) {
+          atomicAdd(&sm_stat[S_READ0 + PT], (unsigned long long)got);
+          atomicAdd(&sm_stat[S_TREAD0 + PT], (unsigned long long)got);
         }
       }
       if ((long long)base + __popc(need) >= n) more = false;
@@ -1542,21 +1556,25 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
       const long long v = warp_take1((unsigned long long *)&ctl->qcount[PT][p], w_int && proc == p);
       if (p == proc) q = v;
     }
+    bool queued = false;
     if (w_alive) {
       put_track(a, PT, slot, t, L);
-      L.st[S_WRITE0 + PT]++;
-      L.st[S_TWRITE0 + PT]++;
     } else if (w_int) {
       if (q < a.qcap) {
         store_track(a.ibuf[PT][proc], q, t);
-        L.st[S_WRITE0 + PT]++;
-        L.st[S_TWRITE0 + PT]++;
-        L.st[S_TQUEUE0 + PT]++;
+        queued = true;
       } else {
         L.err |= kErrOverflow;
         L.st[S_OVERFLOW]++;
         L.deposit(t.event, t.vol, (double)t.E);
       }
+    }
+    // records written (to the next store or an interaction buffer), per warp
+    const unsigned wr = __ballot_sync(0xffffffffu, w_alive || queued), wq = __ballot_sync(0xffffffffu, queued);
+    if (lane_id() == 0 && wr) {
+      atomicAdd(&sm_stat[S_WRITE0 + PT], (unsigned long long)__popc(wr));
+      atomicAdd(&sm_stat[S_TWRITE0 + PT], (unsigned long long)__popc(wr));
+      if (wq) atomicAdd(&sm_stat[S_TQUEUE0 + PT], (unsigned long long)__popc(wq));
     }
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
@@ -2549,6 +2567,7 @@ __device__ __forceinline__ void soa_ctx(const gx_track_soa &s, int i, const Trac
   c.lam0 = 0.0;
   c.e0 = t.E;
   c.ttrue = 0.0;
+  c.range0 = -1.0;
 }
 
 __device__ __forceinline__ void stage_local(Local &L, const StageArgs &a)
