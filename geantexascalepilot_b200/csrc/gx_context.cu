@@ -215,11 +215,14 @@ static double lrad_tsai_factor(double Z, double alpha, double rcl)
   return 4 * alpha * rcl * rcl * Z * (Z * (lrad - fc) + lprad);
 }
 
-static void material(Data &d, int m, double Z, double A, double density, double rcl, double lc, double alpha)
+static void material(Data &d, int m, double Z, double A, double density, double I, double rcl, double lc,
+                     double alpha)
 {
   const double avogadro = 6.02214179e+23;
   double n_atoms = avogadro * density / A * 1.e-3; // 1/mm3
   d.mat_Z[m] = Z;
+  d.mat_A[m] = A;
+  d.mat_I[m] = I;
   d.mat_density[m] = density;
   d.mat_nel[m] = Z * n_atoms;
   d.mat_dfactor[m] = d.mat_nel[m] * (4.0 * kPi * rcl * lc * lc); // n_el x the Migdal constant
@@ -284,6 +287,29 @@ int refit_vector(Ctx *ctx, int table, int mat, const double *ynew)
   return GX_OK;
 }
 
+// The same with new node abscissae as well (same count): the vector's
+// descriptor follows and the context's device copy is updated.
+int refit_vector_xy(Ctx *ctx, int table, int mat, const double *xnew, const double *ynew)
+{
+  Data &d = ctx->host;
+  VecDesc &vd = d.vec[table][mat];
+  const int n = vd.n;
+  cudaError_t e = cudaMemcpy(const_cast<double *>(d.x) + vd.off, xnew, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return cuda_error(e, "refit: node abscissae");
+  vd.emin = xnew[0];
+  vd.emax = xnew[n - 1];
+  vd.dbin = std::log(xnew[1] / vd.emin);
+  vd.base = std::log(vd.emin) / vd.dbin;
+  vd.invdbin = 1.0 / vd.dbin;
+  vd.eminf = (float)vd.emin;
+  vd.emaxf = (float)vd.emax;
+  vd.invdbinf = (float)vd.invdbin;
+  vd.basef = (float)vd.base;
+  if ((e = cudaMemcpy(ctx->dev, &d, sizeof(Data), cudaMemcpyHostToDevice)) != cudaSuccess)
+    return cuda_error(e, "refit: context upload");
+  return refit_vector(ctx, table, mat, ynew);
+}
+
 template <class T> static int upload(const std::vector<T> &h, T **d)
 {
   cudaError_t e = cudaMalloc((void **)d, sizeof(T) * (h.empty() ? 1 : h.size()));
@@ -336,9 +362,10 @@ int load_data(const char *datadir, Ctx *ctx)
   em_constants(&rcl, &lc, &alpha);
   d.pi_rcl2 = kPi * rcl * rcl;
   d.alpha = alpha;
-  material(d, 0, 1.0, 1.01, 1.e-25, rcl, lc, alpha);   // Galactic
-  material(d, 1, 82.0, 207.2, 11.35, rcl, lc, alpha);  // G4_Pb
-  material(d, 2, 18.0, 39.95, 1.396, rcl, lc, alpha);  // G4_lAr
+  // mean excitation energies: ICRU Report 37 (the NIST values of these materials)
+  material(d, 0, 1.0, 1.01, 1.e-25, 21.8e-6, rcl, lc, alpha); // Galactic
+  material(d, 1, 82.0, 207.2, 11.35, 823.0e-6, rcl, lc, alpha); // G4_Pb
+  material(d, 2, 18.0, 39.95, 1.396, 188.0e-6, rcl, lc, alpha); // G4_lAr
   double *px, *py, *pd2, *pc64, *pbind, *psandia;
   float *pc32;
   SBTable *psb;

@@ -210,6 +210,7 @@ struct Data {
   double cut_length[4][kNMat];
   int nshell[101], ishell[101], nint[101], cumint[101];
   double mat_Z[kNMat], mat_density[kNMat], mat_nel[kNMat], mat_dfactor[kNMat];
+  double mat_I[kNMat], mat_A[kNMat]; // mean excitation energy (MeV), atomic mass (g/mol)
   // multiple scattering, per material: radiation length (mm) and the Urban
   // model's Z-dependent constants {X0, th1, th2, ca, cb, cc, cd}
   double mat_msc[kNMat][7];

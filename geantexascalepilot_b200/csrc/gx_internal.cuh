@@ -58,6 +58,7 @@ int run_transport(Ctx *C, const gx_transport_config *cfg, int nprim, const int *
                   int *d_pstep, gx_transport_stats *stats, cudaStream_t s);
 } // namespace parity
 int refit_vector(Ctx *ctx, int table, int mat, const double *ynew);
+int refit_vector_xy(Ctx *ctx, int table, int mat, const double *xnew, const double *ynew);
 
 inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStream_t>(s); }
 

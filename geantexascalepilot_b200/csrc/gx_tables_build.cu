@@ -26,16 +26,32 @@
 //   LambdaPrim.phot   E x the Sandia photo-absorption parameterisation (the
 //     photo-electric cross section the transport already uses below 200 keV;
 //     the reference has none).
+//   DEDX.eIoni.e-/e+  the restricted collision stopping power of the
+//     Berger-Seltzer formula (ICRU Report 37; energy transfers below the e-
+//     production cut), with the density effect of Sternheimer and Peierls
+//     (Phys. Rev. B 3 (1971) 3681) from the mean excitation energy and the
+//     plasma energy; above 10 keV (below it the formula does not hold)
+//   DEDX.eBrem.e-     the restricted radiative loss: k dsigma/dk of the
+//     Seltzer-Berger tables (with the dielectric suppression) integrated from
+//     0 to the gamma cut, up to 1 GeV
+//   Range / InverseRange.eIoni.e-/e+  the range integral of 1 / (dE/dx) over
+//     the context's ionisation plus brems loss (rebuilt where built), from
+//     2 E0 / (dE/dx)(E0) at the lowest node (dE/dx proportional to beta
+//     there), 8-point Gauss-Legendre in ln E per node interval; the inverse
+//     range is the same pairs swapped (host side, in gx_ctx_rebuild_tables).
 // gx_ctx_rebuild_tables puts these values on the shipped tables' node
 // energies (materials Pb and LAr; brems up to 1 GeV and pairs up to 100 GeV,
 // where Geant4's tables switch to its relativistic models) and refits the
 // splines; the shipped values remain where no model here applies.  Against
 // the shipped Geant4 tables: Compton, ionisation to 2e-4 (the materials'
-// atomic masses), brems 0.5%, pairs within 5% from 50 MeV to 10 TeV (up to
-// +12% in lead at 10-30 MeV, where the Born approximation overestimates;
-// nothing below 2.5 MeV, where the screening functions go negative),
-// photo-electric within 6% in lead and 14-19% low in argon (the Sandia
-// parameterisation against the photo-electric model of the Geant4 build).
+// atomic masses), brems 0.5%, pairs within 6% from 50 MeV to 10 TeV (up to
+// +16% in lead at 10-30 MeV, where the Born approximation overestimates; the
+// shipped values are kept below 4 MeV, near threshold), photo-electric within
+// 6% in lead and 14-19% low in argon (the Sandia parameterisation against
+// the photo-electric model of the Geant4 build), collision stopping power
+// within 2.5% (lead: the density-effect parameters) and 1e-3 (argon),
+// radiative loss 0.2%, ranges within 4% (lead, whose shipped range integrates
+// a loss table 2% below its own DEDX table) and 2e-3 (argon).
 #include "gx_internal.cuh"
 
 #include <cmath>
@@ -106,6 +122,65 @@ __device__ double bh_xs_per_atom(double Z, double E, double alpha, double rcl2)
   return alpha * rcl2 * Z * (Z + xi) * s * h; // 2 x (1/2) x the bracket
 }
 
+// Density-effect correction of Sternheimer and Peierls for a condensed
+// material: C = 1 + 2 ln(I / hw_p), hw_p = 28.816 eV sqrt(rho Z / A); x0, x1
+// by their rules for I below / above 100 eV; m = 3.
+__device__ double density_effect(double x, double I, double Z, double A, double rho)
+{
+  const double hwp = 28.816e-6 * ::sqrt(rho * Z / A), C = 1.0 + 2.0 * ::log(I / hwp);
+  double x0, x1;
+  if (I < 100.0e-6) {
+    x1 = 2.0;
+    x0 = C < 3.681 ? 0.2 : 0.326 * C - 1.0;
+  } else {
+    x1 = 3.0;
+    x0 = C < 5.215 ? 0.2 : 0.326 * C - 1.5;
+  }
+  const double a = (C - 4.606 * x0) / ((x1 - x0) * (x1 - x0) * (x1 - x0));
+  if (x < x0) return 0.0;
+  if (x < x1) return 4.606 * x - C + a * (x1 - x) * (x1 - x) * (x1 - x);
+  return 4.606 * x - C;
+}
+
+// Restricted collision stopping power (MeV/mm) of an electron (positron = 0)
+// or positron (1) of kinetic energy T, energy transfers below cut: the
+// Berger-Seltzer formula, 2 pi r_e^2 m n_el / beta^2 [ln(2 (tau + 2) / (I/m)^2)
+// + F(tau, Delta) - delta].
+__device__ double bs_dedx(double T, double cut, double I, double Z, double A, double rho, double n_el,
+                          double twopi_mc2_rcl2, int positron)
+{
+  const double tau = T / kEMass, gam = tau + 1.0, b2 = tau * (tau + 2.0) / (gam * gam);
+  const double x = ::log10(::sqrt(tau * (tau + 2.0)));
+  const double lnI = ::log(2.0 * (tau + 2.0) / ((I / kEMass) * (I / kEMass)));
+  double F;
+  if (!positron) {
+    const double d = fmin(cut, 0.5 * T) / kEMass;
+    F = -1.0 - b2 + ::log((tau - d) * d) + tau / (tau - d) +
+        (0.5 * d * d + (2.0 * tau + 1.0) * ::log(1.0 - d / tau)) / (gam * gam);
+  } else {
+    const double d = fmin(cut, T) / kEMass, y = 1.0 / (1.0 + gam), d2 = d * d, d3 = d2 * d, d4 = d3 * d;
+    F = ::log(tau * d) - (b2 / tau) * (tau + 2.0 * d - 1.5 * d2 * y - (d - d3 / 3.0) * y * y -
+                                       (0.5 * d2 - tau * d3 / 3.0 + 0.25 * d4) * y * y * y);
+  }
+  return twopi_mc2_rcl2 * n_el / b2 * (lnI + F - density_effect(x, I, Z, A, rho));
+}
+
+// Restricted radiative loss per atom (MeV mm^2): the integral of k dsigma/dk
+// from 0 to min(kc, T) with the Seltzer-Berger tables (dsigma/dk = Z^2
+// chi(k/T, T) / (beta^2 k) millibarn) and the dielectric suppression.
+__device__ double sb_dedx_per_atom(const SBTable &t, double Z, double kin, double kc, double density_factor)
+{
+  const double E = kin + kEMass, beta2 = kin * (kin + 2.0 * kEMass) / (E * E), kp2 = density_factor * E * E;
+  const double kmax = fmin(kc, kin), dk = kmax / 16.0, lnT = ::log(kin);
+  double s = 0.0;
+  for (int l = 0; l < 16; ++l)
+    for (int i = 0; i < 8; ++i) {
+      const double k = (l + kGLx[i]) * dk;
+      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k));
+    }
+  return Z * Z / beta2 * s * dk * 1.0e-25;
+}
+
 __global__ void k_table_build(const Data *__restrict__ D, int table, int mat, const double *__restrict__ E,
                               double *__restrict__ out, int n)
 {
@@ -124,6 +199,14 @@ __global__ void k_table_build(const Data *__restrict__ D, int table, int mat, co
     v = n_atoms * sb_xs_per_atom(d.sb[mat == 1 ? 2 : 1], Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat]);
     break;
   case GX_Lambda_conv: v = n_atoms * bh_xs_per_atom(Z, e, d.alpha, d.pi_rcl2 / kPi); break;
+  case GX_DEDX_eIoni_em:
+  case GX_DEDX_eIoni_ep:
+    v = bs_dedx(e, d.cut_energy[1][mat], d.mat_I[mat], Z, d.mat_A[mat], d.mat_density[mat], n_el, twopi_mc2_rcl2,
+                table == GX_DEDX_eIoni_ep);
+    break;
+  case GX_DEDX_eBrem_em:
+    v = n_atoms * sb_dedx_per_atom(d.sb[mat == 1 ? 2 : 1], Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat]);
+    break;
   case GX_LambdaPrim_phot: v = e * pe_xs_sandia(d, (int)Z, d.mat_density[mat], e); break;
   default: v = 0.0;
   }
@@ -134,8 +217,66 @@ bool buildable(int table, int mat)
 {
   const bool t = table == GX_Lambda_compt || table == GX_LambdaPrim_compt || table == GX_Lambda_eIoni_em ||
                  table == GX_Lambda_eIoni_ep || table == GX_Lambda_eBrem_em || table == GX_Lambda_conv ||
-                 table == GX_LambdaPrim_phot;
+                 table == GX_LambdaPrim_phot || table == GX_DEDX_eIoni_em || table == GX_DEDX_eIoni_ep ||
+                 table == GX_DEDX_eBrem_em;
   return t && (mat == 1 || mat == 2); // the SB data cover lead and argon
+}
+
+// Values of the context's tables (the reference's spline) at n energies.
+__global__ void k_table_eval(const Data *__restrict__ D, int table, int mat, const double *__restrict__ E,
+                             double *__restrict__ out, int n)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] = vec_value_ref(*D, D->vec[table][mat], E[i]);
+}
+
+// Range and inverse range of e- (ep = 0) or e+ (1) in material mat from the
+// context's current loss tables (ionisation + brems), at the range table's
+// node energies; refits both vectors.
+int rebuild_range(Ctx *c, int mat, int ep)
+{
+  const int tr = ep ? GX_Range_ep : GX_Range_em, ti = ep ? GX_InverseRange_ep : GX_InverseRange_em;
+  const int tion = ep ? GX_DEDX_eIoni_ep : GX_DEDX_eIoni_em, tbr = ep ? GX_DEDX_eBrem_ep : GX_DEDX_eBrem_em;
+  const VecDesc &vd = c->host.vec[tr][mat];
+  const int n = vd.n;
+  std::vector<double> x(n);
+  cudaError_t e = cudaMemcpy(x.data(), c->host.x + vd.off, n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return cuda_error(e, "rebuild_range: nodes");
+  // 8-point Gauss-Legendre in ln E on each node interval, plus the lowest node
+  static const double gx[8] = {0.019855071751231856, 0.10166676129318664, 0.2372337950418355, 0.40828267875217510,
+                               0.59171732124782490,  0.7627662049581645,  0.89833323870681340, 0.98014492824876810};
+  static const double gw[8] = {0.050614268145188130, 0.11119051722668724, 0.15685332293894363, 0.18134189168918100,
+                               0.18134189168918100,  0.15685332293894363, 0.11119051722668724, 0.050614268145188130};
+  const int m = 1 + 8 * (n - 1);
+  std::vector<double> E(m), D(m, 0.0);
+  E[0] = x[0];
+  for (int j = 1; j < n; ++j)
+    for (int i = 0; i < 8; ++i) E[1 + 8 * (j - 1) + i] = std::exp(std::log(x[j - 1]) + gx[i] * std::log(x[j] / x[j - 1]));
+  double *dE = nullptr, *dV = nullptr;
+  if ((e = cudaMalloc((void **)&dE, 2 * m * sizeof(double))) != cudaSuccess) return cuda_error(e, "rebuild_range");
+  dV = dE + m;
+  cudaMemcpy(dE, E.data(), m * sizeof(double), cudaMemcpyHostToDevice);
+  std::vector<double> V(m);
+  for (int t : {tion, tbr}) {
+    k_table_eval<<<(m + 127) / 128, 128>>>(c->dev, t, mat, dE, dV, m);
+    if ((e = cudaMemcpy(V.data(), dV, m * sizeof(double), cudaMemcpyDeviceToHost)) != cudaSuccess) break;
+    for (int k = 0; k < m; ++k) D[k] += V[k];
+  }
+  cudaFree(dE);
+  if (e != cudaSuccess) return cuda_error(e, "rebuild_range: loss tables");
+  std::vector<double> r(n);
+  r[0] = 2.0 * x[0] / D[0];
+  for (int j = 1; j < n; ++j) {
+    double s = 0.0;
+    for (int i = 0; i < 8; ++i) {
+      const int k = 1 + 8 * (j - 1) + i;
+      s += gw[i] * E[k] / D[k];
+    }
+    r[j] = r[j - 1] + s * std::log(x[j] / x[j - 1]);
+  }
+  int rc = refit_vector(c, tr, mat, r.data());
+  if (rc) return rc;
+  return refit_vector_xy(c, ti, mat, r.data(), x.data());
 }
 
 } // namespace
@@ -164,7 +305,8 @@ int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change)
   cudaError_t e = cudaSetDevice(c->device);
   if (e != cudaSuccess) return cuda_error(e, "gx_ctx_rebuild_tables: cudaSetDevice");
   const int tables[] = {GX_Lambda_compt, GX_LambdaPrim_compt, GX_Lambda_eIoni_em, GX_Lambda_eIoni_ep,
-                        GX_Lambda_eBrem_em, GX_Lambda_conv, GX_LambdaPrim_phot};
+                        GX_Lambda_eBrem_em, GX_Lambda_conv, GX_LambdaPrim_phot, GX_DEDX_eIoni_em,
+                        GX_DEDX_eIoni_ep, GX_DEDX_eBrem_em};
   double *dv = nullptr;
   int nmax = 0;
   for (int t : tables)
@@ -189,13 +331,21 @@ int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change)
         if (t == GX_Lambda_eBrem_em && x[i] > 1.0e3) y[i] = old[i];
         // pairs: the Bethe-Heitler range (Geant4 changes to its relativistic,
         // LPM-suppressed model at 80 GeV)
-        if (t == GX_Lambda_conv && x[i] > 1.0e5) y[i] = old[i];
+        if (t == GX_Lambda_conv && (x[i] > 1.0e5 || x[i] < 4.0)) y[i] = old[i]; // and near threshold
+        // stopping powers: the formulas hold above 10 keV; radiative loss in
+        // the Seltzer-Berger range
+        if ((t == GX_DEDX_eIoni_em || t == GX_DEDX_eIoni_ep) && x[i] < 0.01) y[i] = old[i];
+        if (t == GX_DEDX_eBrem_em && x[i] > 1.0e3) y[i] = old[i];
         if (old[i] > 0.0 && y[i] > 0.0 && x[i] > 0.01) // above 10 keV (below it the shipped low-energy tails differ)
           worst = std::max(worst, std::fabs(y[i] / old[i] - 1.0));
       }
       rc = refit_vector(c, t, m, y.data());
     }
   cudaFree(dv);
+  if (rc) return rc;
+  // ranges from the rebuilt losses, and their inverses
+  for (int m = 1; m <= 2 && rc == GX_OK; ++m)
+    for (int ep = 0; ep <= 1 && rc == GX_OK; ++ep) rc = rebuild_range(c, m, ep);
   if (rc) return rc;
   if (max_rel_change) *max_rel_change = worst;
   return GX_OK;
