@@ -329,7 +329,7 @@ def main():
         cfg.precision, cfg.engine, cfg.profile = 1, 1, 0
         trials = gx.autotune(dm, cfg, dev["t"], dev["E"], dev["p"], dev["d"], nvol=nvol, repeats=2)
         tuned = {"best": trials[0], "trials": len(trials),
-                 "default": next((t for t in trials if t["block_size"] == 128 and t["blocks_per_sm"] == 4
+                 "default": next((t for t in trials if t["block_size"] == 128 and t["blocks_per_sm"] == 5
                                   and t["steps_per_launch"] == 16 and t["graph_iters"] == 16
                                   and t["wave_energy"] == 0), None)}
 
@@ -346,7 +346,7 @@ def main():
            "track_steps_per_step": n_steps // max(1, args.steps),
            "primaries_per_s": world * nprim * args.steps / (ms / 1e3),
            "stats": {k: st32[k] for k in ("steps", "substeps", "tracks", "iterations", "peak_in_flight", "errors")},
-           "launch": {"block": cfg.block_size or 128, "blocks_per_sm": cfg.blocks_per_sm or 4,
+           "launch": {"block": cfg.block_size or 128, "blocks_per_sm": cfg.blocks_per_sm or 5,
                       "steps_per_launch": cfg.steps_per_launch or 16,
                       "graph_iters": cfg.graph_iters or 16}}
     if tuned:

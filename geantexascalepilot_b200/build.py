@@ -46,11 +46,26 @@ PER_FILE = {"gx_kernels.cu": ["-fmad=false"], "gx_events.cu": ["-fmad=false"],
             "gx_transport_parity.cu": ["-fmad=false"]}
 
 
+def _includes(src, seen=None):
+    """src and the files of csrc/ it includes, directly or through others."""
+    seen = set() if seen is None else seen
+    if src in seen or not os.path.exists(src):
+        return seen
+    seen.add(src)
+    with open(src) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include \""):
+                _includes(os.path.join(CSRC, line.split('"')[1]), seen)
+    return seen
+
+
 def _compile(src, verbose):
     obj = os.path.join(BUILD, os.path.basename(src) + ".o")
-    # every source of the directory: headers, and .cu files that include others
-    deps = glob.glob(os.path.join(CSRC, "*")) + [os.path.join(os.path.dirname(PKG), "include", "gx_abi.h"),
-                                                 os.path.abspath(__file__)]
+    # the source, every header of the directory (headers include one another),
+    # the .cu files it includes, the ABI header and this script
+    deps = (sorted(_includes(src)) + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) +
+            [os.path.join(os.path.dirname(PKG), "include", "gx_abi.h"), os.path.abspath(__file__)])
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
     extra = PER_FILE.get(os.path.basename(src), [])

@@ -55,7 +55,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   int ntrials = 0, rc = GX_OK;
   double best_rate = -1.0;
   Trial best = {base.block_size > 0 ? base.block_size : default_block(1),
-                base.blocks_per_sm > 0 ? base.blocks_per_sm : kDefaultBlocksPerSM,
+                base.blocks_per_sm > 0 ? base.blocks_per_sm : default_blocks_per_sm(base),
                 base.steps_per_launch > 0 ? base.steps_per_launch : kDefaultStepsPerLaunch,
                 base.graph_iters > 0 ? base.graph_iters : 16,
                 base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy,
@@ -111,7 +111,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   // blocks above 256 threads only where their kernel variants exist
   const bool wide_ok = base.geometry != 2 && !base.msc && !base.field_map && !base.fp64_parity;
   const int blocks[] = {64, 128, 256, 512, 1024};
-  const int bpsms[] = {1, 2, 4, 8};
+  const int bpsms[] = {1, 2, 4, 5, 6, 8};
   for (int b : blocks)
     for (int p : bpsms) {
       if (b > 256 && (!wide_ok || b * p > 4096)) continue;

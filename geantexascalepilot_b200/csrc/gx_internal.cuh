@@ -64,9 +64,16 @@ inline cudaStream_t stream_of(gx_stream_t s) { return reinterpret_cast<cudaStrea
 
 // Launch defaults of the transport engines (the sweep of gx_transport_autotune
 // found 128-thread blocks fastest for the batched engine on C3; the plain loop
-// keeps 256).
+// keeps 256).  The FP32-mixed step kernels of the uniform field, layered
+// geometry and no multiple scattering are held to 96 registers, so five
+// 128-thread blocks fit on an SM (20 warps); the others take up to 128 (four).
 inline int default_block(int engine) { return engine == 1 ? 128 : 256; }
 constexpr int kDefaultBlocksPerSM = 4;
+inline int default_blocks_per_sm(const gx_transport_config &c)
+{
+  const bool plain = !c.field_map && c.geometry != 2 && !c.msc && !c.fp64_parity;
+  return c.engine == 1 && c.precision == 1 && plain ? 5 : kDefaultBlocksPerSM;
+}
 // Steps of one track per transport-kernel launch in the batched engine, at
 // most (a track is kept in registers while it neither interacts nor dies).
 constexpr int kDefaultStepsPerLaunch = 16;

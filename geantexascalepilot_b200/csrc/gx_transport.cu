@@ -1451,8 +1451,14 @@ template <class R, int PT, int K> __global__ void __launch_bounds__(256, 2) k_st
 // Resident 256-thread blocks per SM the step kernels are compiled for: the FP64
 // kernels would take 160-180 registers unbounded (12 warps per SM); bounded to
 // 128 they keep 16 warps at the cost of a few spills.  The FP32-mixed kernels
-// fit in 128 registers unbounded.
+// take 110-126 registers unbounded.  Held to 96 (kMaxRegs: the interaction
+// kernels and the transport kernels of the uniform field, layered geometry and
+// no multiple scattering) five 128-thread blocks fit on an SM instead of four,
+// and C3 and C4 run 7-8% faster although the kernels spill 0-30 words; the
+// field-map and multiple-scattering variants would spill 50-270 bytes there
+// and stay unbounded (255).
 template <class R> constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 0; // 0: no minimum
+template <class R, int K> constexpr int kMaxRegs = sizeof(R) == 8 ? 128 : (K == 0 ? 96 : 255);
 __device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
 // One slot per flagged lane in counter *ctr (ballot and popcount, one atomic
@@ -1582,7 +1588,7 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
 }
 
 template <class R, int PT, int K>
-__global__ void __launch_bounds__(256, kMinBlocks<R>) k_transport(const Args<R> *__restrict__ A)
+__global__ void __launch_bounds__(256, kMinBlocks<R>) __maxnreg__((kMaxRegs<R, K>)) k_transport(const Args<R> *__restrict__ A)
 {
   transport_body<R, PT, K>(A);
 }
@@ -1637,7 +1643,7 @@ template <class R, int PT, int PROC> __device__ __forceinline__ void interact_bo
 }
 
 template <class R, int PT, int PROC>
-__global__ void __launch_bounds__(256, kMinBlocks<R>) k_interact(const Args<R> *__restrict__ A)
+__global__ void __launch_bounds__(256, kMinBlocks<R>) __maxnreg__((kMaxRegs<R, 0>)) k_interact(const Args<R> *__restrict__ A)
 {
   interact_body<R, PT, PROC>(A);
 }
@@ -2288,7 +2294,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.a.nstores = nstores;
   L.a.refill_below = cfg->refill_below > 0 ? std::min(cfg->refill_below, cap) : cap / 2;
   L.block = cfg->block_size > 0 ? cfg->block_size : default_block(cfg->engine);
-  int bpsm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : kDefaultBlocksPerSM;
+  int bpsm = cfg->blocks_per_sm > 0 ? cfg->blocks_per_sm : default_blocks_per_sm(*cfg);
   L.grid = C->num_sms * bpsm;
   L.smem = 768 * sizeof(double);
 

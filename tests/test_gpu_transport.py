@@ -190,7 +190,7 @@ def test_autotune_and_launch_settings_leave_results_unchanged(dm):
     assert best["steps_per_ms"] == max(t["steps_per_ms"] for t in trials) > 0
     assert (cfg.block_size, cfg.blocks_per_sm, cfg.graph_iters, cfg.interaction_interval) == (
         best["block_size"], best["blocks_per_sm"], best["graph_iters"], best["interaction_interval"])
-    assert cfg.block_size in (64, 128, 256, 512, 1024) and cfg.blocks_per_sm in (1, 2, 4, 8)
+    assert cfg.block_size in (64, 128, 256, 512, 1024) and cfg.blocks_per_sm in (1, 2, 4, 5, 6, 8)
     e1, s1, ps1 = run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True)
     assert s1["steps"] == s0["steps"] and s1["tracks"] == s0["tracks"]
     assert np.array_equal(ps0, ps1)
