@@ -5,10 +5,15 @@
     python -m geantexascalepilot_b200.run c4 --n 4096 --autotune
     python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --profile --capacity 2097152
     python -m geantexascalepilot_b200.run c3 --geometry csg --msc 1 --field-map
+    python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --iterations 30
 
 Prints one JSON line: the workload, the transport statistics (steps,
 propagation sub-steps, tracks, secondaries, iterations, per-kernel device
-times in profile mode) and the device time of the transport loop.
+times in profile mode) and the device time of the transport loop.  With
+--iterations N the primaries go in as tracks (gx_transport_tracks) and the
+engine stops after N iterations: the statistics are those of the first N
+iterations, and the tracks still alive are handed back (their count is
+printed); the difference of two such runs gives one iteration's work.
 """
 import argparse
 import json
@@ -36,6 +41,8 @@ def main(argv=None):
                    help="multiple scattering: 0 off, 1 angular deflection, 2 with lateral displacement")
     p.add_argument("--field-map", action="store_true",
                    help="the shipped CMS field map (Runge-Kutta sub-steps) instead of the workload's uniform field")
+    p.add_argument("--iterations", type=int, default=0,
+                   help="stop after this many iterations and hand the live tracks back (0: run to completion)")
     p.add_argument("--device", type=int, default=0)
     a = p.parse_args(argv)
 
@@ -75,7 +82,15 @@ def main(argv=None):
         out["autotune_trials"] = trials
         cfg.profile = int(a.profile)
     for _ in range(a.repeat):
-        edep, st, _ = gx.transport(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)
+        if a.iterations > 0:
+            tin = gx.TrackSoA.from_primaries(cfg, *prims[:4], events=prims[4])
+            cap = min(4 * (a.capacity or (1 << 24)), 1 << 24)
+            live, edep, st = gx.transport_tracks(dm, cfg, tin, max_iterations=a.iterations, out=gx.TrackSoA(cap),
+                                                 nvol=nvol)
+            out["iterations"] = a.iterations
+            out["live_tracks"] = int(live.n)
+        else:
+            edep, st, _ = gx.transport(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)
     torch.cuda.synchronize()
     out["stats"] = st
     out["edep_total"] = float(edep.sum().item())
