@@ -34,6 +34,11 @@
 //   DEDX.eBrem.e-     the restricted radiative loss: k dsigma/dk of the
 //     Seltzer-Berger tables (with the dielectric suppression) integrated from
 //     0 to the gamma cut, up to 1 GeV
+//   Lambda.eBrem.e+, DEDX.eBrem.e+  the same integrals with the positron's
+//     Coulomb factor exp(2 pi alpha Z (1/beta1 - 1/beta2)) on the electron
+//     tables (beta1, beta2: the positron's speed before and after emitting k),
+//     the approximation of the positron-to-electron bremsstrahlung ratio that
+//     the Geant4 Physics Reference Manual gives for the Seltzer-Berger model
 //   Range / InverseRange.eIoni.e-/e+  the range integral of 1 / (dE/dx) over
 //     the context's ionisation plus brems loss (rebuilt where built), from
 //     2 E0 / (dE/dx)(E0) at the lowest node (dE/dx proportional to beta
@@ -50,8 +55,11 @@
 // 6% in lead and 14-19% low in argon (the Sandia parameterisation against
 // the photo-electric model of the Geant4 build), collision stopping power
 // within 2.5% (lead: the density-effect parameters) and 1e-3 (argon),
-// radiative loss 0.2%, ranges within 4% (lead, whose shipped range integrates
-// a loss table 2% below its own DEDX table) and 2e-3 (argon).
+// radiative loss 0.2%, positron brems: the shipped e+/e- ratio to 1e-4
+// (cross sections) and 1e-3 (radiative loss; 1% in lead at 20-60 keV, where
+// the factor leaves 10-20% of the electrons' loss), ranges within 4% (lead,
+// whose shipped range integrates a loss table 2% below its own DEDX table)
+// and 2e-3 (argon).
 #include "gx_internal.cuh"
 
 #include <cmath>
@@ -81,7 +89,20 @@ __device__ double bhabha_xs_per_electron(double kin, double cut, double twopi_mc
   return twopi_mc2_rcl2 / kin * I;
 }
 
-__device__ double sb_xs_per_atom(const SBTable &t, double Z, double kin, double cut, double density_factor)
+// Positron factor exp(2 pi alpha Z (1/beta1 - 1/beta2)) for emitting k at
+// kinetic energy kin (pos_coef = 2 pi alpha Z; 0 for electrons: factor 1).
+__device__ double positron_factor(double pos_coef, double kin, double k)
+{
+  if (pos_coef == 0.0) return 1.0;
+  const double t2 = kin - k;
+  if (!(t2 > 0.0)) return 0.0;
+  const double ib1 = (kin + kEMass) / ::sqrt(kin * (kin + 2.0 * kEMass));
+  const double ib2 = (t2 + kEMass) / ::sqrt(t2 * (t2 + 2.0 * kEMass));
+  return ::exp(pos_coef * (ib1 - ib2));
+}
+
+__device__ double sb_xs_per_atom(const SBTable &t, double Z, double kin, double cut, double density_factor,
+                                 double pos_coef)
 {
   if (!(cut < kin)) return 0.0;
   const double E = kin + kEMass, beta2 = kin * (kin + 2.0 * kEMass) / (E * E), kp2 = density_factor * E * E;
@@ -90,7 +111,7 @@ __device__ double sb_xs_per_atom(const SBTable &t, double Z, double kin, double 
   for (int l = 0; l < 16; ++l)
     for (int i = 0; i < 8; ++i) {
       const double k = ::exp(v0 + (l + kGLx[i]) * dv);
-      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k));
+      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k)) * positron_factor(pos_coef, kin, k);
     }
   return Z * Z / beta2 * s * dv * 1.0e-25; // millibarn -> mm^2
 }
@@ -168,7 +189,8 @@ __device__ double bs_dedx(double T, double cut, double I, double Z, double A, do
 // Restricted radiative loss per atom (MeV mm^2): the integral of k dsigma/dk
 // from 0 to min(kc, T) with the Seltzer-Berger tables (dsigma/dk = Z^2
 // chi(k/T, T) / (beta^2 k) millibarn) and the dielectric suppression.
-__device__ double sb_dedx_per_atom(const SBTable &t, double Z, double kin, double kc, double density_factor)
+__device__ double sb_dedx_per_atom(const SBTable &t, double Z, double kin, double kc, double density_factor,
+                                   double pos_coef)
 {
   const double E = kin + kEMass, beta2 = kin * (kin + 2.0 * kEMass) / (E * E), kp2 = density_factor * E * E;
   const double kmax = fmin(kc, kin), dk = kmax / 16.0, lnT = ::log(kin);
@@ -176,7 +198,7 @@ __device__ double sb_dedx_per_atom(const SBTable &t, double Z, double kin, doubl
   for (int l = 0; l < 16; ++l)
     for (int i = 0; i < 8; ++i) {
       const double k = (l + kGLx[i]) * dk;
-      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k));
+      s += kGLw[i] * sb_value<double>(t, k / kin, lnT) / (1.0 + kp2 / (k * k)) * positron_factor(pos_coef, kin, k);
     }
   return Z * Z / beta2 * s * dk * 1.0e-25;
 }
@@ -188,7 +210,8 @@ __global__ void k_table_build(const Data *__restrict__ D, int table, int mat, co
   if (i >= n) return;
   const Data &d = *D;
   const double e = E[i], Z = d.mat_Z[mat], n_el = d.mat_nel[mat], n_atoms = n_el / Z;
-  const double twopi_mc2_rcl2 = 2.0 * kEMass * d.pi_rcl2;
+  const double twopi_mc2_rcl2 = 2.0 * kEMass * d.pi_rcl2, pos_coef = 2.0 * kPi * d.alpha * Z;
+  const SBTable &sb = d.sb[mat == 1 ? 2 : 1];
   double v = 0.0;
   switch (table) {
   case GX_Lambda_compt: v = fmax(0.0, n_atoms * kn_xs_per_atom(Z, e)); break;
@@ -196,7 +219,9 @@ __global__ void k_table_build(const Data *__restrict__ D, int table, int mat, co
   case GX_Lambda_eIoni_em: v = n_atoms * mb_xs_per_atom(Z, e, twopi_mc2_rcl2, d.cut_energy[1][mat]); break;
   case GX_Lambda_eIoni_ep: v = n_el * bhabha_xs_per_electron(e, d.cut_energy[1][mat], twopi_mc2_rcl2); break;
   case GX_Lambda_eBrem_em:
-    v = n_atoms * sb_xs_per_atom(d.sb[mat == 1 ? 2 : 1], Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat]);
+  case GX_Lambda_eBrem_ep:
+    v = n_atoms * sb_xs_per_atom(sb, Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat],
+                                 table == GX_Lambda_eBrem_ep ? pos_coef : 0.0);
     break;
   case GX_Lambda_conv: v = n_atoms * bh_xs_per_atom(Z, e, d.alpha, d.pi_rcl2 / kPi); break;
   case GX_DEDX_eIoni_em:
@@ -205,7 +230,9 @@ __global__ void k_table_build(const Data *__restrict__ D, int table, int mat, co
                 table == GX_DEDX_eIoni_ep);
     break;
   case GX_DEDX_eBrem_em:
-    v = n_atoms * sb_dedx_per_atom(d.sb[mat == 1 ? 2 : 1], Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat]);
+  case GX_DEDX_eBrem_ep:
+    v = n_atoms * sb_dedx_per_atom(sb, Z, e, d.cut_energy[0][mat], d.mat_dfactor[mat],
+                                   table == GX_DEDX_eBrem_ep ? pos_coef : 0.0);
     break;
   case GX_LambdaPrim_phot: v = e * pe_xs_sandia(d, (int)Z, d.mat_density[mat], e); break;
   default: v = 0.0;
@@ -218,7 +245,7 @@ bool buildable(int table, int mat)
   const bool t = table == GX_Lambda_compt || table == GX_LambdaPrim_compt || table == GX_Lambda_eIoni_em ||
                  table == GX_Lambda_eIoni_ep || table == GX_Lambda_eBrem_em || table == GX_Lambda_conv ||
                  table == GX_LambdaPrim_phot || table == GX_DEDX_eIoni_em || table == GX_DEDX_eIoni_ep ||
-                 table == GX_DEDX_eBrem_em;
+                 table == GX_DEDX_eBrem_em || table == GX_Lambda_eBrem_ep || table == GX_DEDX_eBrem_ep;
   return t && (mat == 1 || mat == 2); // the SB data cover lead and argon
 }
 
@@ -306,7 +333,7 @@ int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change)
   if (e != cudaSuccess) return cuda_error(e, "gx_ctx_rebuild_tables: cudaSetDevice");
   const int tables[] = {GX_Lambda_compt, GX_LambdaPrim_compt, GX_Lambda_eIoni_em, GX_Lambda_eIoni_ep,
                         GX_Lambda_eBrem_em, GX_Lambda_conv, GX_LambdaPrim_phot, GX_DEDX_eIoni_em,
-                        GX_DEDX_eIoni_ep, GX_DEDX_eBrem_em};
+                        GX_DEDX_eIoni_ep, GX_DEDX_eBrem_em, GX_Lambda_eBrem_ep, GX_DEDX_eBrem_ep};
   double *dv = nullptr;
   int nmax = 0;
   for (int t : tables)
@@ -328,14 +355,14 @@ int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change)
       }
       for (int i = 0; i < vd.n; ++i) {
         // brems: the Seltzer-Berger range only (Geant4 changes model at 1 GeV)
-        if (t == GX_Lambda_eBrem_em && x[i] > 1.0e3) y[i] = old[i];
+        if ((t == GX_Lambda_eBrem_em || t == GX_Lambda_eBrem_ep) && x[i] > 1.0e3) y[i] = old[i];
         // pairs: the Bethe-Heitler range (Geant4 changes to its relativistic,
         // LPM-suppressed model at 80 GeV)
         if (t == GX_Lambda_conv && (x[i] > 1.0e5 || x[i] < 4.0)) y[i] = old[i]; // and near threshold
         // stopping powers: the formulas hold above 10 keV; radiative loss in
         // the Seltzer-Berger range
         if ((t == GX_DEDX_eIoni_em || t == GX_DEDX_eIoni_ep) && x[i] < 0.01) y[i] = old[i];
-        if (t == GX_DEDX_eBrem_em && x[i] > 1.0e3) y[i] = old[i];
+        if ((t == GX_DEDX_eBrem_em || t == GX_DEDX_eBrem_ep) && x[i] > 1.0e3) y[i] = old[i];
         if (old[i] > 0.0 && y[i] > 0.0 && x[i] > 0.01) // above 10 keV (below it the shipped low-energy tails differ)
           worst = std::max(worst, std::fabs(y[i] / old[i] - 1.0));
       }

@@ -126,11 +126,21 @@ int gx_ctx_compute_cuts(gx_ctx *ctx, double cut_mm);
  * Nishina, ProxyKleinNishina.hpp:62-93), GX_Lambda_eIoni_em (Moller with the
  * material's e- cut, ProxyMollerScattering.hpp:61-89), GX_Lambda_eIoni_ep
  * (Bhabha, integrated from the cut), GX_Lambda_eBrem_em (Seltzer-Berger
- * tables integrated from the gamma cut, with dielectric suppression). */
+ * tables integrated from the gamma cut, with dielectric suppression),
+ * GX_Lambda_eBrem_ep (the same with the positron Coulomb factor
+ * exp(2 pi alpha Z (1/beta1 - 1/beta2))), GX_Lambda_conv (Bethe-Heitler with
+ * the sampler's screening functions and Tsai's xi(Z) for the atomic
+ * electrons), GX_LambdaPrim_phot (E x the Sandia photo-absorption cross
+ * section), GX_DEDX_eIoni_em/ep (Berger-Seltzer restricted collision stopping
+ * power with the Sternheimer-Peierls density effect), GX_DEDX_eBrem_em/ep
+ * (Seltzer-Berger radiative loss below the gamma cut). */
 int gx_table_build(gx_ctx *ctx, int table, int mat, const double *d_E, double *d_out, int n, gx_stream_t s);
-/* Replaces the node values of those tables (brems up to 1 GeV) with the built
- * ones and refits their splines; *max_rel_change (optional) receives the
- * largest relative change above 10 keV.  Synchronous. */
+/* Replaces the node values of those tables with the built ones where their
+ * models hold (brems up to 1 GeV, pairs from 4 MeV to 100 GeV, stopping powers
+ * above 10 keV) and refits their splines, then rebuilds Range and
+ * InverseRange (e-, e+) as the range integral of the rebuilt losses;
+ * *max_rel_change (optional) receives the largest relative change of a table
+ * value above 10 keV.  Synchronous. */
 int gx_ctx_rebuild_tables(gx_ctx *ctx, double *max_rel_change);
 
 /* ------------------------------------------------------------- models */
@@ -268,7 +278,8 @@ typedef struct {
   int engine;              /* 0 plain loop (one mixed queue, host-driven), 1 batched (per-type queues, graph) */
   int block_size;          /* threads per block (0: default); above 256 (up to 1024) only for the batched
                               engine with the uniform field, layered geometry and no multiple scattering */
-  int blocks_per_sm;       /* resident blocks per SM for the grid (0: default) */
+  int blocks_per_sm;       /* resident blocks per SM for the grid (0: default, 5 for the FP32-mixed
+                              batched engine, 4 otherwise) */
   long long capacity;      /* track slots per particle type (0: default) */
   long long refill_below;  /* inject / refill when fewer tracks than this are in flight (0: default) */
   int graph_iters;         /* iterations per CUDA-graph launch between host checks (0: default) */
@@ -525,7 +536,7 @@ int gx_transport_tracks(gx_ctx *ctx, const gx_transport_config *cfg, const gx_tr
  * primaries (the whole batch, or a representative subset of it) once per
  * candidate: block size {64, 128, 256, 512, 1024} (512 and 1024 with the
  * uniform field, layered geometry and no multiple scattering, at most 4096
- * threads per SM) x resident blocks per SM {1, 2, 4, 8}, then steps per track
+ * threads per SM) x resident blocks per SM {1, 2, 4, 5, 6, 8}, then steps per track
  * and transport launch {1, 16, 64, 1024}, then iterations per CUDA-graph
  * launch {4, 8, 32, 64}, then the refill threshold {1/8, 1/4, 3/4 of the
  * capacity}, then the primary energy per injection wave {1/4, 1/2, 2 x the
