@@ -19,7 +19,8 @@ inside the timed region.  Beside it, on the same MRG32k3a streams:
   * the FP64 parity variant against the oracle's parity build on the whole
     batch: per-primary step counts and per-layer deposits;
   * C4 and C5 with the same arms (FP32-mixed, FP64 batched, FP64 plain loop
-    -- C5 on a bounded sample of its events --, agreement, CPU sample);
+    -- C5 on a bounded sample of its events --, agreement, CPU sample), and
+    C4 again at the setting gx_transport_autotune picks on a quarter of it;
   * the roofline of the dominant step kernel and the CPU oracle timed on the
     whole C3 batch on all host cores (the CPU baseline at equal statistics).
 
@@ -63,6 +64,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU time of each bounded C4 / C5 oracle sample")
     p.add_argument("--no-fp64", action="store_true", help="skip the FP64 comparison runs")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU oracle legs")
+    p.add_argument("--no-tune-c4", action="store_true",
+                   help="skip the launch-setting sweep on C4 (tuned on its first 16384 primaries)")
     p.add_argument("--autotune", action="store_true",
                    help="sweep the launch settings on the workload first (untimed) and time the winner")
     return p.parse_args()
@@ -456,6 +459,20 @@ def main():
                     "max_over_events": float(r.max()), "mean_over_events": float(r.mean()),
                     "median_over_events": float(np.median(r)), "layers": "> 2% of the event's deposit",
                     "event_total_rel_max": float((np.abs(a32.sum(1) - a64.sum(1)) / a64.sum(1)).max())}
+        if name == "c4" and not args.no_tune_c4:
+            # the launch-setting sweep on a quarter of C4 (one run per
+            # setting), then the whole of C4 at the winner (untimed sweep)
+            c.precision, c.engine, c.profile = 1, 1, 0
+            nt = 16384
+            trials = gx.autotune(dm, c, tens["t"][:nt], tens["E"][:nt], tens["p"][:nt], tens["d"][:nt], nvol=nv,
+                                 repeats=1)
+            mt, stt, _, _ = timed(1, 1, 1, 1, c=c, tens=tens, events=evx, out=ox)
+            rec["autotuned"] = {"track_steps_per_s": stt / (mt / 1e3), "primaries_per_s": len(pr[0]) / (mt / 1e3),
+                                "ms": mt, "steps": int(stt), "over_default": (stt / mt) / (s32 / m32),
+                                "setting": {k: trials[0][k] for k in LAUNCH_KEYS}, "trials": len(trials),
+                                "tuned_on": "primaries 0-%d, one run per setting" % (nt - 1)}
+            for k in LAUNCH_KEYS:
+                setattr(c, k, 0)
         extra[name] = rec
     out["other_workloads"] = extra
 
@@ -487,12 +504,15 @@ def main():
     stp = one(1, 1, profile=1)
     k = int(np.argmax(stp["transport_ms"]))
     launches_k = max(1, stp["step_launches"][k])
+    k_ms = stp["transport_ms"][k]
+    k_steps = stp["transport_steps"][k]
+    k_records = stp["transport_read"][k] + stp["transport_written"][k]
     # algorithmic bytes: one read and one write of the track record per step
     # (a step reads and writes the state once); the kernel keeps a track in
     # registers across steps, so the records it actually moves are fewer
-    nbytes = stp["transport_steps"][k] * 2 * stp["bytes_per_track"]
-    moved = (stp["transport_read"][k] + stp["transport_written"][k]) * stp["bytes_per_track"]
-    achieved = nbytes / (stp["transport_ms"][k] / 1e3) / 1e9
+    nbytes = k_steps * 2 * stp["bytes_per_track"]
+    moved = k_records * stp["bytes_per_track"]
+    achieved = nbytes / (k_ms / 1e3) / 1e9
     peaks = {}
     try:
         peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
@@ -510,7 +530,7 @@ def main():
             if len(f) == 2 and not line.startswith("#"):
                 per[int(f[0])] = float(f[1])
         if k in per:
-            traffic = per[k] * (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k
+            traffic = per[k] * k_records / launches_k
     pipes = None
     pf = os.path.join(REPO, "profiles", "transport_kernel_pipes.txt")
     if os.path.exists(pf):
@@ -522,15 +542,16 @@ def main():
                 pipes = {"fp64_pct": float(f[1]), "fp32_fma_pct": float(f[2]), "alu_pct": float(f[3]),
                          "issue_pct": float(f[4]), "active_lanes_of_32": float(f[5]), "source": "ncu"}
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                       "traffic": traffic, "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
+                       "traffic": traffic,
+                       "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
                        "peak_source": "measured" if "hbm_gbs" in peaks else "fallback",
                        "algorithmic_bytes_per_launch": nbytes / launches_k,
-                       "steps_per_launch": stp["transport_steps"][k] / launches_k,
+                       "steps_per_launch": k_steps / launches_k,
                        "record_bytes_moved_per_launch": moved / launches_k,
-                       "record_bytes_moved_gbs": moved / (stp["transport_ms"][k] / 1e3) / 1e9,
-                       "avg_launch_ms": stp["transport_ms"][k] / launches_k,
-                       "share_of_step_kernel_time": stp["transport_ms"][k] / max(1e-9, sum(stp["step_ms"])),
-                       "records_per_launch": (stp["transport_read"][k] + stp["transport_written"][k]) / launches_k,
+                       "record_bytes_moved_gbs": moved / (k_ms / 1e3) / 1e9,
+                       "avg_launch_ms": k_ms / launches_k,
+                       "share_of_step_kernel_time": k_ms / max(1e-9, sum(stp["step_ms"])),
+                       "records_per_launch": k_records / launches_k,
                        "pipes": pipes}
 
     if rank == 0 and not args.no_cpu:

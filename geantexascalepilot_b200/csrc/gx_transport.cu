@@ -3000,7 +3000,7 @@ int gx_transport_run_host(gx_ctx *ctx, const gx_transport_config *cfg, int nprim
 // that must start from zero (the control block) before its first launch.
 // Calls that overlap on the GPU (two streams, two host threads) race on it.
 // The first call on a device sets up that device (cudaGetSymbolAddress and
-// the skip-ahead table upload) and should come before any stream capture.
+// the skip-ahead table upload).
 // Every call synchronises its stream after each iteration (the host reads the
 // control block to decide whether to go on).  The set-up is kept for the life
 // of the process: a cudaDeviceReset while the library is loaded is not

@@ -576,8 +576,8 @@ int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, cons
  * not fit are scored where they were).  precision must be 0 (FP64); engine is
  * ignored; d_edep is added to as in gx_transport_run.  Every call shares the
  * array; calls that overlap on the GPU race on it.  The first call on a device
- * sets that device up and should come before any stream capture.  Each call
- * synchronises its stream after every iteration.  A cudaDeviceReset while the
+ * sets that device up (a symbol lookup and the skip-ahead table upload).  Each
+ * call synchronises its stream after every iteration.  A cudaDeviceReset while the
  * library is loaded is not supported (the set-up is kept per process). */
 #define GX_NOALLOC_CAPACITY 16384
 #define GX_NOALLOC_MAX_PRIMARIES 4096
