@@ -53,21 +53,6 @@ constexpr double kM1 = 4294967087.0;
 constexpr double kM2 = 4294944443.0;
 constexpr double kNorm = 1.0 / (4294967087.0 + 1.0);
 constexpr double kA12 = 1403580.0, kA13n = 810728.0, kA21 = 527612.0, kA23n = 1370589.0;
-// 1/m as the unevaluated sum rh + rl of two doubles (rh = 1/m rounded, rl the
-// rest rounded), for the exact quotient trunc(p rh + p rl) of a draw.  Derived
-// here with Dekker's exact product (T. J. Dekker, Numer. Math. 18 (1971)
-// 224-242; Veltkamp's split at 2^27 + 1): m rh = ph + pl exactly, so
-// 1/m - rh = (1 - m rh) / m = ((1 - ph) - pl) / m, where 1 - ph is exact.
-constexpr double dekker_hi(double a) { return 134217729.0 * a - (134217729.0 * a - a); }
-constexpr double dekker_prod_err(double a, double b)
-{
-  return ((dekker_hi(a) * dekker_hi(b) - a * b) + dekker_hi(a) * (b - dekker_hi(b)) +
-          (a - dekker_hi(a)) * dekker_hi(b)) +
-         (a - dekker_hi(a)) * (b - dekker_hi(b));
-}
-constexpr double recip_lo(double m) { return ((1.0 - m * (1.0 / m)) - dekker_prod_err(m, 1.0 / m)) / m; }
-constexpr double kRh1 = 1.0 / kM1, kRl1 = recip_lo(kM1);
-constexpr double kRh2 = 1.0 / kM2, kRl2 = recip_lo(kM2);
 
 // ------------------------------------------------------------------- errors
 enum : int {
@@ -116,53 +101,64 @@ template <> struct M<float> {
 };
 
 // ------------------------------------------------------------------ MRG32k3a
-// Six FP64 integers in registers; the recurrence is exact in FP64 (all
-// products < 2^53), the quotient uses the device branch of
-// MRG32k3a::Kernel (source/Geant/random/src/MRG32k3a.cpp:124-163).
+// The state as six 32-bit words in registers.  The recurrence of
+// MRG32k3a::Kernel (source/Geant/random/src/MRG32k3a.cpp:124-163) is done in
+// exact integer arithmetic: a12 s1 - a13n s0 = a12 s1 + a13n (m1 - s0)
+// (mod m1), every term non-negative and the sum below 2^54, reduced modulo
+// m = 2^32 - c (c = 209 for m1, 22853 for m2) by folding the high word twice,
+// h 2^32 + l = h c + l (mod m), and one conditional subtraction.  The
+// reference's FP64 form (a quotient from 1/m as two doubles) is exact as
+// well, so both give the same residues and the same draws; the integer form
+// keeps the state in 6 registers instead of 12 and needs no conversions
+// between the words and FP64.
 struct Mrg {
-  double s[6];
+  uint32_t s[6];
+  static constexpr uint32_t kM1u = 4294967087u, kM2u = 4294944443u;
+  static constexpr uint32_t kC1 = 209u, kC2 = 22853u; // 2^32 - m
+  static constexpr uint32_t kA12u = 1403580u, kA13nu = 810728u, kA21u = 527612u, kA23nu = 1370589u;
+  // x mod (2^32 - c) for x < 2^54
+  static __device__ __forceinline__ uint32_t mod_m(uint64_t x, uint32_t c, uint32_t m)
+  {
+    x = (x >> 32) * c + (x & 0xffffffffull); // < 2^22 c + 2^32
+    x = (x >> 32) * c + (x & 0xffffffffull); // < 2^32 + 64 c
+    return (x >= m) ? (uint32_t)(x - m) : (uint32_t)x;
+  }
 
   __device__ __forceinline__ void load(const uint32_t *st, long long n, long long i)
   {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) s[k] = (double)__ldg(&st[k * n + i]);
+    for (int k = 0; k < 6; ++k) s[k] = __ldg(&st[k * n + i]);
   }
   __device__ __forceinline__ void store(uint32_t *st, long long n, long long i) const
   {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) st[k * n + i] = (uint32_t)s[k];
+    for (int k = 0; k < 6; ++k) st[k * n + i] = s[k];
   }
-  // the state as six words (a track carries it so: 6 registers, not 12)
   __device__ __forceinline__ void from_words(const uint32_t w[6])
   {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) s[k] = (double)w[k];
+    for (int k = 0; k < 6; ++k) s[k] = w[k];
   }
   __device__ __forceinline__ void to_words(uint32_t w[6]) const
   {
 #pragma unroll
-    for (int k = 0; k < 6; ++k) w[k] = (uint32_t)s[k];
+    for (int k = 0; k < 6; ++k) w[k] = s[k];
   }
   // draw numerator z in [1, m1]
-  __device__ __forceinline__ double next()
+  __device__ __forceinline__ uint32_t next_u32()
   {
-    double p1 = kA12 * s[1] - kA13n * s[0];
-    double k = trunc(fma(p1, kRh1, p1 * kRl1));
-    p1 -= k * kM1;
-    if (p1 < 0.) p1 += kM1;
+    const uint32_t p1 = mod_m((uint64_t)kA12u * s[1] + (uint64_t)kA13nu * (kM1u - s[0]), kC1, kM1u);
     s[0] = s[1];
     s[1] = s[2];
     s[2] = p1;
-    double p2 = kA21 * s[5] - kA23n * s[3];
-    k = trunc(fma(p2, kRh2, p2 * kRl2));
-    p2 -= k * kM2;
-    if (p2 < 0.) p2 += kM2;
+    const uint32_t p2 = mod_m((uint64_t)kA21u * s[5] + (uint64_t)kA23nu * (kM2u - s[3]), kC2, kM2u);
     s[3] = s[4];
     s[4] = s[5];
     s[5] = p2;
-    return (p1 > p2) ? (p1 - p2) : (p1 - p2 + kM1);
+    return (p1 > p2) ? (p1 - p2) : (p1 + (kM1u - p2));
   }
-  __device__ __forceinline__ double u01() { return next() * kNorm; }
+  __device__ __forceinline__ double next() { return (double)next_u32(); }
+  __device__ __forceinline__ double u01() { return (double)next_u32() * kNorm; }
   template <class R> __device__ __forceinline__ R u();
   // Stream of a secondary track: six draw numerators of this stream reduced
   // mod m1 (words 0-2) and m2 (words 3-5); an all-zero component becomes 1.
@@ -170,12 +166,11 @@ struct Mrg {
   {
 #pragma unroll
     for (int k = 0; k < 6; ++k) {
-      double z = next();
-      double m = (k < 3) ? kM1 : kM2;
+      const uint32_t z = next_u32(), m = (k < 3) ? kM1u : kM2u;
       c.s[k] = (z >= m) ? z - m : z;
     }
-    if (c.s[0] == 0 && c.s[1] == 0 && c.s[2] == 0) c.s[0] = 1;
-    if (c.s[3] == 0 && c.s[4] == 0 && c.s[5] == 0) c.s[3] = 1;
+    if ((c.s[0] | c.s[1] | c.s[2]) == 0u) c.s[0] = 1u;
+    if ((c.s[3] | c.s[4] | c.s[5]) == 0u) c.s[3] = 1u;
   }
 };
 template <> __device__ __forceinline__ double Mrg::u<double>() { return u01(); }

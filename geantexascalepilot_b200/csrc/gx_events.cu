@@ -96,8 +96,8 @@ __global__ void __launch_bounds__(256) k_egamma_gun(const uint64_t *__restrict__
     }
   Mrg r;
   for (int c = 0; c < 3; ++c) {
-    r.s[c] = (double)v1[c];
-    r.s[3 + c] = (double)v2[c];
+    r.s[c] = (uint32_t)v1[c];
+    r.s[3 + c] = (uint32_t)v2[c];
   }
   for (long long i = first; i < last; ++i) {
     const bool gamma = r.u01() < g.gamma_fraction;
@@ -181,8 +181,8 @@ __global__ void __launch_bounds__(256) k_spot_gun(const uint64_t *__restrict__ J
     }
   Mrg r;
   for (int c = 0; c < 3; ++c) {
-    r.s[c] = (double)v1[c];
-    r.s[3 + c] = (double)v2[c];
+    r.s[c] = (uint32_t)v1[c];
+    r.s[3 + c] = (uint32_t)v2[c];
   }
   for (long long i = first; i < last; ++i) {
     double u[5];
