@@ -47,6 +47,17 @@
 namespace gx {
 
 enum { kCsgBox = 0, kCsgTube = 1, kCsgSphere = 2, kCsgPoly = 3 };
+// Sets of solids (bit k: solid kind k).  The navigation routines take the set
+// a tree can hold as a template argument: a kernel for trees of boxes only
+// (the calorimeters') carries none of the other solids' code.
+constexpr int kSolidsAll = 0xF, kSolidsBox = 1 << kCsgBox;
+// whether node n is of kind k, for a tree of solids S (constant when S decides)
+template <int S> __host__ __device__ __forceinline__ bool csg_is(int kind, int k)
+{
+  if ((S & (1 << k)) == 0) return false;
+  if (S == (1 << k)) return true;
+  return kind == k;
+}
 constexpr int kCsgMaxPlanes = 32;   // planes of one polyhedron, at most
 constexpr double kCsgTol = 1e-9;    // surface tolerance (mm)
 constexpr double kCsgPad = 1e-6;    // bounding-box padding (mm)
@@ -73,6 +84,7 @@ struct CsgView {
   const int *slab;     // per slab: first candidate, candidates (pairs)
   const int *cand;     // candidates (touchable indices)
   const double *planes; // polyhedra: (nx, ny, nz, d) per plane
+  int solids;           // the solid kinds present (bit k: kind k)
 };
 
 // Slab of coordinate x in a touchable's grid (host and device alike).
@@ -226,11 +238,12 @@ __device__ __forceinline__ double csg_poly(const double *__restrict__ pl, int p0
 }
 
 // inside, or on the surface and not moving out through it
+template <int S = kSolidsAll>
 __device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const double *q, const double *e, double tol,
                                                    const double *pl)
 {
-  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyContains, tol) != 0.0;
-  if (n.kind == kCsgBox) {
+  if (csg_is<S>(n.kind, kCsgPoly)) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyContains, tol) != 0.0;
+  if (csg_is<S>(n.kind, kCsgBox)) {
     const double h0 = n.a, h1 = n.b, h2 = n.c;
     const double a0 = fabs(q[0]), a1 = fabs(q[1]), a2 = fabs(q[2]);
     if (a0 > h0 + tol || a1 > h1 + tol || a2 > h2 + tol) return false;
@@ -240,7 +253,7 @@ __device__ __forceinline__ bool csg_contains_local(const CsgNode &n, const doubl
     return true;
   }
   double r, out;
-  if (n.kind == kCsgTube) {
+  if (csg_is<S>(n.kind, kCsgTube)) {
     const double az = fabs(q[2]);
     if (az > n.c + tol) return false;
     if (az >= n.c - tol && cmul(q[2], e[2]) > 0.0) return false;
@@ -271,12 +284,13 @@ __device__ __forceinline__ double near_root(double a, double b, double c, double
 }
 
 // distance to leave the solid from a point inside it (or on its surface)
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const double *q, const double *e,
                                                      const double *pl)
 {
   double s = kCsgInf;
-  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyOut, 0.0);
-  if (n.kind == kCsgBox) {
+  if (csg_is<S>(n.kind, kCsgPoly)) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyOut, 0.0);
+  if (csg_is<S>(n.kind, kCsgBox)) {
     const double h[3] = {n.a, n.b, n.c};
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -290,7 +304,7 @@ __device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const dou
     return s < 0.0 ? 0.0 : s;
   }
   double a, b, r2;
-  if (n.kind == kCsgTube) {
+  if (csg_is<S>(n.kind, kCsgTube)) {
     if (e[2] > 0.0)
       s = (n.c - q[2]) / e[2];
     else if (e[2] < 0.0)
@@ -311,17 +325,18 @@ __device__ __forceinline__ double csg_dist_out_local(const CsgNode &n, const dou
       if (D2 >= 0.0) s = fmin(s, near_root(a, b, c2, sqrt(D2)));
     }
   }
-  if (n.kind == kCsgTube && n.np) s = fmin(s, csg_wedge(n, pl).out(q, e, kCsgTol));
+  if (csg_is<S>(n.kind, kCsgTube) && n.np) s = fmin(s, csg_wedge(n, pl).out(q, e, kCsgTol));
   return s < 0.0 ? 0.0 : s;
 }
 
 // distance to enter the solid from a point outside it; kCsgInf if missed
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const double *q, const double *e,
                                                     const double *pl)
 {
   const double tol = kCsgTol;
-  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyIn, tol);
-  if (n.kind == kCsgBox) {
+  if (csg_is<S>(n.kind, kCsgPoly)) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], e[0], e[1], e[2], kPolyIn, tol);
+  if (csg_is<S>(n.kind, kCsgBox)) {
     const double h[3] = {n.a, n.b, n.c};
     double tmin = -kCsgInf, tmax = kCsgInf;
 #pragma unroll
@@ -345,7 +360,7 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
   double s = kCsgInf;
   const double rmin = n.a, rmax = n.b;
   double a, b, r2;
-  if (n.kind == kCsgTube) {
+  if (csg_is<S>(n.kind, kCsgTube)) {
     const double dz = n.c;
     const bool seg = n.np != 0;
     Wedge w{0.0, 0.0, 0.0, 0.0, 0};
@@ -414,11 +429,12 @@ __device__ __forceinline__ double csg_dist_in_local(const CsgNode &n, const doub
   return s;
 }
 
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const double *q, const double *pl)
 {
-  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeOut, 0.0);
-  if (n.kind == kCsgBox) return fmin(fmin(n.a - fabs(q[0]), n.b - fabs(q[1])), n.c - fabs(q[2]));
-  if (n.kind == kCsgTube) {
+  if (csg_is<S>(n.kind, kCsgPoly)) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeOut, 0.0);
+  if (csg_is<S>(n.kind, kCsgBox)) return fmin(fmin(n.a - fabs(q[0]), n.b - fabs(q[1])), n.c - fabs(q[2]));
+  if (csg_is<S>(n.kind, kCsgTube)) {
     const double r = sqrt(dot2(q, q));
     double s = fmin(n.c - fabs(q[2]), n.b - r);
     if (n.a > 0.0) s = fmin(s, r - n.a);
@@ -429,11 +445,12 @@ __device__ __forceinline__ double csg_safety_out_local(const CsgNode &n, const d
 }
 
 // a lower bound of the distance to the solid from a point outside it
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_safety_in_local(const CsgNode &n, const double *q, const double *pl)
 {
-  if (n.kind == kCsgPoly) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeIn, 0.0);
-  if (n.kind == kCsgBox) return fmax(fmax(fabs(q[0]) - n.a, fabs(q[1]) - n.b), fabs(q[2]) - n.c);
-  if (n.kind == kCsgTube) {
+  if (csg_is<S>(n.kind, kCsgPoly)) return csg_poly(pl, n.p0, n.np, q[0], q[1], q[2], 0.0, 0.0, 0.0, kPolySafeIn, 0.0);
+  if (csg_is<S>(n.kind, kCsgBox)) return fmax(fmax(fabs(q[0]) - n.a, fabs(q[1]) - n.b), fabs(q[2]) - n.c);
+  if (csg_is<S>(n.kind, kCsgTube)) {
     const double r = sqrt(dot2(q, q));
     const double s = fmax(fmax(fabs(q[2]) - n.c, r - n.b), n.a - r);
     return n.np ? fmax(s, csg_wedge(n, pl).safety_in(q)) : s;
@@ -472,16 +489,18 @@ __device__ __forceinline__ double csg_bbox_ray(const CsgNode &n, const double *p
   return tmax < tmin ? kCsgInf : tmin;
 }
 
+template <int S = kSolidsAll>
 __device__ __forceinline__ bool csg_contains(const CsgView &g, int v, const double *p, const double *d, double tol)
 {
   const CsgNode &n = g.node[v];
   if (csg_bbox_gap(n, p) > 0.0) return false;
   double q[3], e[3];
   csg_local(n, p, d, q, e);
-  return csg_contains_local(n, q, e, tol, g.planes);
+  return csg_contains_local<S>(n, q, e, tol, g.planes);
 }
 
 // the deepest touchable at or below v (which contains p) that contains p
+template <int S = kSolidsAll>
 __device__ __forceinline__ int csg_descend(const CsgView &g, int v, const double *p, const double *d, double tol)
 {
   for (int depth = 0; depth < kCsgMaxDepth; ++depth) {
@@ -492,13 +511,13 @@ __device__ __forceinline__ int csg_descend(const CsgView &g, int v, const double
       const int j0 = g.slab[2 * sl], nj = g.slab[2 * sl + 1];
       for (int j = 0; j < nj && next < 0; ++j) {
         const int c = g.cand[j0 + j];
-        if (csg_contains(g, c, p, d, tol)) next = c;
+        if (csg_contains<S>(g, c, p, d, tol)) next = c;
       }
     } else {
       const int k0 = n.kid0, nk = n.nkid;
       for (int k = 0; k < nk && next < 0; ++k) {
         const int c = g.kids[k0 + k];
-        if (csg_contains(g, c, p, d, tol)) next = c;
+        if (csg_contains<S>(g, c, p, d, tol)) next = c;
       }
     }
     if (next < 0) return v;
@@ -508,11 +527,12 @@ __device__ __forceinline__ int csg_descend(const CsgView &g, int v, const double
 }
 
 // from touchable v up until one contains p, then down; -1 outside the world
+template <int S = kSolidsAll>
 __device__ __forceinline__ int csg_locate(const CsgView &g, int v, const double *p, const double *d, double tol)
 {
   if (v < 0) v = 0;
   for (int depth = 0; v >= 0 && depth <= kCsgMaxDepth; ++depth) {
-    if (csg_contains(g, v, p, d, tol)) return csg_descend(g, v, p, d, tol);
+    if (csg_contains<S>(g, v, p, d, tol)) return csg_descend<S>(g, v, p, d, tol);
     v = g.node[v].parent;
   }
   return -1;
@@ -521,19 +541,20 @@ __device__ __forceinline__ int csg_locate(const CsgView &g, int v, const double 
 // distance to the next boundary from p in v; children whose bounding box the
 // ray reaches only beyond `limit` are skipped (the result is then >= limit);
 // hit = the child entered, -1 when leaving v
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_step(const CsgView &g, int v, const double *p, const double *d, double limit,
                                            int &hit)
 {
   double q[3], e[3];
   const CsgNode &n = g.node[v];
   csg_local(n, p, d, q, e);
-  double s = csg_dist_out_local(n, q, e, g.planes);
+  double s = csg_dist_out_local<S>(n, q, e, g.planes);
   hit = -1;
   auto child = [&](int c) {
     const double tb = csg_bbox_ray(g.node[c], p, d);
     if (!(tb < s && tb < limit)) return;
     csg_local(g.node[c], p, d, q, e);
-    const double t = csg_dist_in_local(g.node[c], q, e, g.planes);
+    const double t = csg_dist_in_local<S>(g.node[c], q, e, g.planes);
     if (t < s || (t == s && hit >= 0 && c < hit)) {
       s = t;
       hit = c;
@@ -562,18 +583,19 @@ __device__ __forceinline__ double csg_step(const CsgView &g, int v, const double
   return s;
 }
 
+template <int S = kSolidsAll>
 __device__ __forceinline__ double csg_safety(const CsgView &g, int v, const double *p)
 {
   double q[3];
   const CsgNode &n = g.node[v];
   csg_local_point(n, p, q);
-  double s = csg_safety_out_local(n, q, g.planes);
+  double s = csg_safety_out_local<S>(n, q, g.planes);
   auto child = [&](int c) {
     const CsgNode &m = g.node[c];
     const double gap = csg_bbox_gap(m, p);
     if (gap >= s) return;
     csg_local_point(m, p, q);
-    s = fmin(s, fmax(gap, csg_safety_in_local(m, q, g.planes)));
+    s = fmin(s, fmax(gap, csg_safety_in_local<S>(m, q, g.planes)));
   };
   if (n.gaxis >= 0) {
     // children farther than the safety along the axis cannot lower it
@@ -592,10 +614,11 @@ __device__ __forceinline__ double csg_safety(const CsgView &g, int v, const doub
 }
 
 // the touchable entered at p after csg_step's crossing out of v
+template <int S = kSolidsAll>
 __device__ __forceinline__ int csg_cross(const CsgView &g, int v, int hit, const double *p, const double *d)
 {
-  if (hit >= 0) return csg_descend(g, hit, p, d, kCsgTol);
-  return csg_locate(g, g.node[v].parent, p, d, kCsgTol);
+  if (hit >= 0) return csg_descend<S>(g, hit, p, d, kCsgTol);
+  return csg_locate<S>(g, g.node[v].parent, p, d, kCsgTol);
 }
 
 } // namespace gx

@@ -236,6 +236,9 @@ bool orthonormal(const double *R)
   return true;
 }
 
+// S: the solids the tree holds (the box-only instantiation for trees of boxes,
+// as the transport kernels use it)
+template <int S>
 __global__ void k_geom_probe(CsgView g, int n, const double *__restrict__ pos, const double *__restrict__ dir,
                              const double *__restrict__ limit, int *__restrict__ vol, double *__restrict__ snext,
                              int *__restrict__ next, double *__restrict__ safety)
@@ -244,7 +247,7 @@ __global__ void k_geom_probe(CsgView g, int n, const double *__restrict__ pos, c
   if (i >= n) return;
   const double p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
   const double d[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
-  const int v = csg_locate(g, 0, p, d, kCsgTol);
+  const int v = csg_locate<S>(g, 0, p, d, kCsgTol);
   vol[i] = v;
   if (v < 0) {
     snext[i] = -1.0;
@@ -253,12 +256,12 @@ __global__ void k_geom_probe(CsgView g, int n, const double *__restrict__ pos, c
     return;
   }
   int hit;
-  const double s = csg_step(g, v, p, d, limit[i], hit);
+  const double s = csg_step<S>(g, v, p, d, limit[i], hit);
   snext[i] = s;
-  safety[i] = csg_safety(g, v, p);
+  safety[i] = csg_safety<S>(g, v, p);
   if (s < limit[i]) {
     const double x[3] = {cadd(p[0], cmul(s, d[0])), cadd(p[1], cmul(s, d[1])), cadd(p[2], cmul(s, d[2]))};
-    next[i] = csg_cross(g, v, hit, x, d);
+    next[i] = csg_cross<S>(g, v, hit, x, d);
   } else {
     next[i] = v;
   }
@@ -470,6 +473,9 @@ int gx_ctx_load_geometry(gx_ctx *ctx, const gx_geom *g)
   c->csg_planes = dp;
   c->csg_n = (int)nn;
   c->csg_nscore = g->nscore;
+  int solids = 0;
+  for (const CsgNode &n : g->nodes) solids |= 1 << n.kind;
+  c->csg_solids = solids;
   return GX_OK;
 }
 
@@ -481,9 +487,10 @@ int gx_geom_probe(gx_ctx *ctx, int n, const double *d_pos, const double *d_dir, 
   Ctx *c = reinterpret_cast<Ctx *>(ctx);
   if (!c->csg_node) return set_error(GX_ERR_ARG, "gx_geom_probe: no geometry loaded (gx_ctx_load_geometry)");
   if (n == 0) return GX_OK;
-  CsgView v{c->csg_node, c->csg_kids, c->csg_slab, c->csg_cand, c->csg_planes};
-  k_geom_probe<<<(n + 127) / 128, 128, 0, stream_of(s)>>>(v, n, d_pos, d_dir, d_limit, d_vol, d_snext, d_next,
-                                                         d_safety);
+  CsgView v{c->csg_node, c->csg_kids, c->csg_slab, c->csg_cand, c->csg_planes, c->csg_solids};
+  (c->csg_solids == kSolidsBox ? k_geom_probe<kSolidsBox> : k_geom_probe<kSolidsAll>)<<<(n + 127) / 128, 128, 0,
+                                                                                      stream_of(s)>>>(
+      v, n, d_pos, d_dir, d_limit, d_vol, d_snext, d_next, d_safety);
   cudaError_t e = cudaGetLastError();
   return e == cudaSuccess ? GX_OK : cuda_error(e, "k_geom_probe");
 }

@@ -27,6 +27,7 @@ struct Ctx {
   int *csg_kids = nullptr, *csg_score = nullptr, *csg_slab = nullptr, *csg_cand = nullptr;
   double *csg_planes = nullptr;
   int csg_n = 0, csg_nscore = 0;
+  int csg_solids = 0; // the solid kinds in the tree (bit k: kind k)
   double *stage_scratch = nullptr; // escaped energy of the stage calls (gx_along_step)
   // gx_transport_run_host: its stream and device staging buffer, kept across calls
   cudaStream_t host_stream = nullptr;

@@ -280,13 +280,16 @@ __device__ __forceinline__ int relocate(const Geom &g, int vol, double *p, const
 // Kernel variants, template parameters so that each kernel carries only the
 // code it runs: bit 0 follows the field map (Runge-Kutta sub-steps) instead of
 // the uniform field's helix, bit 1 navigates the CSG tree (gx_csg.cuh) instead
-// of the analytic volumes above, bit 2 applies multiple scattering.
-enum { kKindFieldMap = 1, kKindCsg = 2, kKindMsc = 4 };
+// of the analytic volumes above, bit 2 applies multiple scattering, bit 3
+// (with bit 1, FP32-mixed kernels) navigates a tree of boxes only: the
+// navigator's code for the other solids is left out of those kernels.
+enum { kKindFieldMap = 1, kKindCsg = 2, kKindMsc = 4, kKindBoxes = 8 };
+template <int K> constexpr int kSolidsOf = (K & kKindBoxes) != 0 ? kSolidsBox : kSolidsAll;
 
 template <int K> __device__ __forceinline__ double nav_safety(const Geom &g, int vol, const double *p)
 {
   if constexpr ((K & kKindCsg) != 0)
-    return csg_safety(g.csg, vol, p);
+    return csg_safety<kSolidsOf<K>>(g.csg, vol, p);
   else
     return safety(g, vol, p);
 }
@@ -298,14 +301,14 @@ __device__ __forceinline__ double nav_distance(const Geom &g, int vol, const dou
                                                int &plane)
 {
   if constexpr ((K & kKindCsg) != 0)
-    return csg_step(g.csg, vol, p, d, limit, plane);
+    return csg_step<kSolidsOf<K>>(g.csg, vol, p, d, limit, plane);
   else
     return dist_to_out(g, vol, p, d, plane);
 }
 template <int K> __device__ __forceinline__ int nav_relocate(const Geom &g, int vol, double *p, const double *d)
 {
   if constexpr ((K & kKindCsg) != 0)
-    return csg_locate(g.csg, vol, p, d, kSnap);
+    return csg_locate<kSolidsOf<K>>(g.csg, vol, p, d, kSnap);
   else
     return relocate(g, vol, p, d);
 }
@@ -918,7 +921,7 @@ __device__ __forceinline__ bool step_move_begin(const Geom &g, Track<R> &t, Step
     c.crossed = true;
     if constexpr ((K & kKindCsg) != 0) {
       for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
-      c.newvol = csg_cross(g.csg, t.vol, plane, t.pos, dir);
+      c.newvol = csg_cross<kSolidsOf<K>>(g.csg, t.vol, plane, t.pos, dir);
     } else {
       c.newvol = next_volume(g, t.vol, plane);
       for (int k = 0; k < 3; ++k) t.pos[k] += dd * dir[k];
@@ -1967,9 +1970,11 @@ __global__ void k_fold_touchables(const double *__restrict__ vt, const int *__re
 }
 
 // The variant of the step kernels for a geometry and field (kKind* bits).
-static int kernel_kind(const Geom &g)
+template <class R> static int kernel_kind(const Geom &g)
 {
-  return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0) | (g.msc ? kKindMsc : 0);
+  const bool boxes = sizeof(R) == 4 && g.geometry == 2 && g.csg.solids == kSolidsBox;
+  return (g.field_map ? kKindFieldMap : 0) | (g.geometry == 2 ? kKindCsg : 0) | (g.msc ? kKindMsc : 0) |
+         (boxes ? kKindBoxes : 0);
 }
 template <class R, int PT, int K> static void (*transport_variant())(const Args<R> *)
 {
@@ -1980,7 +1985,16 @@ template <class R, int PT, int K> static void (*transport_variant())(const Args<
 }
 template <class R, int PT> static void (*transport_kernel(int kind))(const Args<R> *)
 {
-  switch (kind) {
+  if constexpr (sizeof(R) == 4) {
+    switch (kind) {
+    case 10: return transport_variant<R, PT, 10>();
+    case 11: return transport_variant<R, PT, 11>();
+    case 14: return transport_variant<R, PT, 14>();
+    case 15: return transport_variant<R, PT, 15>();
+    default: break;
+    }
+  }
+  switch (kind & 7) {
   case 1: return transport_variant<R, PT, 1>();
   case 2: return transport_variant<R, PT, 2>();
   case 3: return transport_variant<R, PT, 3>();
@@ -1993,7 +2007,16 @@ template <class R, int PT> static void (*transport_kernel(int kind))(const Args<
 }
 template <class R> static void (*step_kernel_p(int kind))(const Args<R> *)
 {
-  switch (kind) {
+  if constexpr (sizeof(R) == 4) {
+    switch (kind) {
+    case 10: return k_step_p<R, 3, 10>;
+    case 11: return k_step_p<R, 3, 11>;
+    case 14: return k_step_p<R, 3, 14>;
+    case 15: return k_step_p<R, 3, 15>;
+    default: break;
+    }
+  }
+  switch (kind & 7) {
   case 1: return k_step_p<R, 3, 1>;
   case 2: return k_step_p<R, 3, 2>;
   case 3: return k_step_p<R, 3, 3>;
@@ -2012,7 +2035,7 @@ template <class R, int PT> static void (*transport_for(const Launch<R> &L))(cons
 #ifndef GX_PARITY
   if (L.block > 256) return k_transport_wide<R, PT, 0>;
 #endif
-  return transport_kernel<R, PT>(kernel_kind(L.a.g));
+  return transport_kernel<R, PT>(kernel_kind<R>(L.a.g));
 }
 template <class R, int PT, int PROC> static void (*interact_for(const Launch<R> &L))(const Args<R> *)
 {
@@ -2040,7 +2063,7 @@ static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, boo
     // plain loop: one fused step kernel over the mixed store
     k_refill_p<R><<<L.grid, L.block, 0, s>>>(A);
     k_refill_done<<<1, 1, 0, s>>>(L.a.ctl);
-    step_kernel_p<R>(kernel_kind(L.a.g))<<<L.grid, L.block, L.smem, s>>>(A);
+    step_kernel_p<R>(kernel_kind<R>(L.a.g))<<<L.grid, L.block, L.smem, s>>>(A);
     k_finish<<<1, 1, 0, s>>>(L.a.ctl, L.a.st[0][0].cap, L.a.st[0][1].cap, L.a.st[0][2].cap, L.a.nstores, 1);
     return;
   }
@@ -2276,7 +2299,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   L.a.pstep = d_pstep;
   if (cfg->geometry == 2) {
     // the kernels score per (event, touchable); folded into d_edep at the end
-    g.csg = CsgView{C->csg_node, C->csg_kids, C->csg_slab, C->csg_cand, C->csg_planes};
+    g.csg = CsgView{C->csg_node, C->csg_kids, C->csg_slab, C->csg_cand, C->csg_planes, C->csg_solids};
     g.nvol = C->csg_n;
     const long long nt = (long long)cfg->nevents * C->csg_n;
     if (nt > E->vtally_cap) {
@@ -2353,7 +2376,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
         for (int q = 0; q < nstores; ++q) {
           cudaEventRecord(ea[q], s);
           if (!batched) {
-            step_kernel_p<R>(kernel_kind(L.a.g))<<<L.grid, L.block, L.smem, s>>>(
+            step_kernel_p<R>(kernel_kind<R>(L.a.g))<<<L.grid, L.block, L.smem, s>>>(
                 (const Args<R> *)E->dargs);
             cudaEventRecord(em[q], s);
           } else {
@@ -2393,7 +2416,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     // (re)capture the iteration graph when its launch shape or its kernels
     // (field kind, geometry kind) change; the arguments themselves are read
     // from the device copy uploaded above
-    int shape[6] = {G, L.block, L.grid, L.smem, kernel_kind(L.a.g), every};
+    int shape[6] = {G, L.block, L.grid, L.smem, kernel_kind<R>(L.a.g), every};
     std::vector<char> key(sizeof(shape) + 2 * sizeof(void *));
     const void *ptrs[2] = {E->dargs, E->ctl};
     std::memcpy(key.data(), shape, sizeof(shape));
