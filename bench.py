@@ -541,8 +541,9 @@ def main():
             if len(f) >= 6 and not line.startswith("#") and int(f[0]) == k:
                 pipes = {"fp64_pct": float(f[1]), "fp32_fma_pct": float(f[2]), "alu_pct": float(f[3]),
                          "issue_pct": float(f[4]), "active_lanes_of_32": float(f[5]), "source": "ncu"}
-                if len(f) >= 7:  # the same kernel on launches of the full batch
+                if len(f) >= 8:  # the same kernel on launches of the full batch
                     pipes["active_lanes_of_32_full_size"] = float(f[6])
+                    pipes["issue_pct_full_size"] = float(f[7])
     out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                        "traffic": traffic,
                        "kernel": "k_transport<float,%d,0> (%s)" % (k, ["gamma", "e-", "e+"][k]),
