@@ -344,22 +344,42 @@ __device__ __forceinline__ int bin2d(const double *v, int nn, double z)
   }
   return hi;
 }
-template <class R> __device__ __forceinline__ R sb_value(const SBTable &t, R xr, R yr)
+// The y part of a lookup (y = ln T fixed while a sampler tries several x):
+// the row, and the weights' factors, found once.
+struct SBRow {
+  int iy;
+  double wy2, wy1, dy; // y2 - y, y - y1, y2 - y1
+};
+__device__ __forceinline__ SBRow sb_row(const SBTable &t, double y)
 {
-  double x = xr, y = yr;
-  if (x < t.x[0])
-    x = t.x[0];
-  else if (x > t.x[31])
-    x = t.x[31];
   if (y < t.y[0])
     y = t.y[0];
   else if (y > t.y[56])
     y = t.y[56];
-  int ix = bin2d(t.x, 32, x), iy = bin2d(t.y, 57, y);
-  double x1 = t.x[ix], x2 = t.x[ix + 1], y1 = t.y[iy], y2 = t.y[iy + 1];
+  SBRow r;
+  r.iy = bin2d(t.y, 57, y);
+  const double y1 = t.y[r.iy], y2 = t.y[r.iy + 1];
+  r.wy2 = y2 - y;
+  r.wy1 = y - y1;
+  r.dy = y2 - y1;
+  return r;
+}
+template <class R> __device__ __forceinline__ R sb_value_row(const SBTable &t, const SBRow &w, R xr)
+{
+  double x = xr;
+  if (x < t.x[0])
+    x = t.x[0];
+  else if (x > t.x[31])
+    x = t.x[31];
+  const int ix = bin2d(t.x, 32, x), iy = w.iy;
+  double x1 = t.x[ix], x2 = t.x[ix + 1];
   double v11 = t.v[iy][ix], v12 = t.v[iy][ix + 1], v21 = t.v[iy + 1][ix], v22 = t.v[iy + 1][ix + 1];
-  return (R)(((y2 - y) * (v11 * (x2 - x) + v12 * (x - x1)) + ((y - y1) * (v21 * (x2 - x) + v22 * (x - x1)))) /
-             ((x2 - x1) * (y2 - y1)));
+  return (R)((w.wy2 * (v11 * (x2 - x) + v12 * (x - x1)) + (w.wy1 * (v21 * (x2 - x) + v22 * (x - x1)))) /
+             ((x2 - x1) * w.dy));
+}
+template <class R> __device__ __forceinline__ R sb_value(const SBTable &t, R xr, R yr)
+{
+  return sb_value_row<R>(t, sb_row(t, (double)yr), xr);
 }
 
 // ------------------------------------------------------- cross sections per atom
@@ -696,9 +716,10 @@ template <class R> __device__ int sb_sample(Mrg &r, const ModelParams &p, Inter<
   R xmax = M<R>::log(emax * emax + densityCorr);
   R y = M<R>::log(kin);
   R x0 = cut / kin;
-  R vmax = sb_value<R>(T, x0, y) * R(1.02);
+  const SBRow row = sb_row(T, (double)y); // y is the same for every lookup below but one
+  R vmax = sb_value_row<R>(T, row, x0) * R(1.02);
   if (x0 < R(0.97) && ((kin > R(300.0)) || (kin < R(10 * keV)))) {
-    R ylim = fmin(sb_value<R>(T, R(0.97), R(4 * 2.302585092994046)), R(1.1) * sb_value<R>(T, R(0.97), y));
+    R ylim = fmin(sb_value<R>(T, R(0.97), R(4 * 2.302585092994046)), R(1.1) * sb_value_row<R>(T, row, R(0.97)));
     if (ylim > vmax) vmax = ylim;
   }
   if (x0 < R(0.05)) vmax *= R(1.2);
@@ -710,7 +731,7 @@ template <class R> __device__ int sb_sample(Mrg &r, const ModelParams &p, Inter<
     if (x < R(0)) x = R(0);
     gE = M<R>::sqrt(x);
     R x1 = gE / kin;
-    v = sb_value<R>(T, x1, y);
+    v = sb_value_row<R>(T, row, x1);
     if (++it > kRejectCap) {
       *err |= kErrRejectCap;
       break;
