@@ -63,10 +63,13 @@ struct Geom {
 };
 
 constexpr int kNStat = 28;
-// S_READ/S_WRITE: track records read and written by all step kernels of a
-// type; S_TREAD/S_TWRITE: by its transport kernel alone; S_TQUEUE: of those
-// writes, the records put in an interaction buffer; S_TSTEP: steps completed
-// in the transport kernel of a type.
+// S_READ/S_WRITE: track records read and written by the step kernels of a
+// type other than its transport kernel (the interaction kernels, the plain
+// loop's fused kernel); S_TREAD/S_TWRITE: by its transport kernel (the host
+// reports the sums as the type's records read and written); S_TQUEUE: of the
+// transport kernel's writes, the records put in an interaction buffer (added
+// up by k_finish from the buffers' counters); S_TSTEP: steps completed in the
+// transport kernel of a type.
 enum { S_STEPS, S_SUBSTEPS, S_TRACKS, S_SEC0, S_SEC1, S_SEC2, S_PAIR, S_ANNIH, S_ERR, S_OVERFLOW,
        S_READ0, S_READ1, S_READ2, S_WRITE0, S_WRITE1, S_WRITE2, S_TREAD0, S_TREAD1, S_TREAD2,
        S_TWRITE0, S_TWRITE1, S_TWRITE2, S_TQUEUE0, S_TQUEUE1, S_TQUEUE2, S_TSTEP0, S_TSTEP1, S_TSTEP2 };
@@ -1529,13 +1532,11 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
           gxs.have = 0; // a new photon energy
         }
       }
-      // records read: counted per warp (no per-thread counters held across the loop)
+      // records read: counted per warp (no per-thread counters held across
+      // the loop; the host adds them to the type's total of records read)
       if ((int)lane_id() == leader) {
         const long long got = min((long long)__popc(need), n - (long long)base);
-        if (got > 0) {
-          atomicAdd(&sm_stat[S_READ0 + PT], (unsigned long long)got);
-          atomicAdd(&sm_stat[S_TREAD0 + PT], (unsigned long long)got);
-        }
+        if (got > 0) atomicAdd(&sm_stat[S_TREAD0 + PT], (unsigned long long)got);
       }
       if ((long long)base + __popc(need) >= n) more = false;
     }
@@ -1578,13 +1579,11 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
         L.deposit(t.event, t.vol, (double)t.E);
       }
     }
-    // records written (to the next store or an interaction buffer), per warp
-    const unsigned wr = __ballot_sync(0xffffffffu, w_alive || queued), wq = __ballot_sync(0xffffffffu, queued);
-    if (lane_id() == 0 && wr) {
-      atomicAdd(&sm_stat[S_WRITE0 + PT], (unsigned long long)__popc(wr));
-      atomicAdd(&sm_stat[S_TWRITE0 + PT], (unsigned long long)__popc(wr));
-      if (wq) atomicAdd(&sm_stat[S_TQUEUE0 + PT], (unsigned long long)__popc(wq));
-    }
+    // records written (to the next store or an interaction buffer), per warp;
+    // those queued for interactions are counted by k_finish from the buffers'
+    // counters, and the host adds these to the type's total of records written
+    const unsigned wr = __ballot_sync(0xffffffffu, w_alive || queued);
+    if (lane_id() == 0 && wr) atomicAdd(&sm_stat[S_TWRITE0 + PT], (unsigned long long)__popc(wr));
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err, S_TSTEP0 + PT);
@@ -1668,10 +1667,13 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
   long long buffered = 0;
   for (int q = 0; q < 3; ++q) {
     for (int p = 0; p < 3; ++p) {
-      if (interacted)
+      if (interacted) {
+        // the records the transport kernels queued for this interaction
+        ctl->stat[S_TQUEUE0 + q] += (unsigned long long)ctl->qcount[q][p];
         ctl->qcount[q][p] = 0;
-      else
+      } else {
         buffered += ctl->qcount[q][p];
+      }
     }
     ctl->take[q] = 0;
   }
@@ -2503,8 +2505,9 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     for (int q = 0; q < 3; ++q) {
       stats->step_ms[q] = step_ms[q];
       stats->step_launches[q] = step_launches[q];
-      stats->tracks_read[q] = (long long)c.stat[S_READ0 + q];
-      stats->tracks_written[q] = (long long)c.stat[S_WRITE0 + q];
+      // the transport kernels count their records in the transport entries only
+      stats->tracks_read[q] = (long long)(c.stat[S_READ0 + q] + c.stat[S_TREAD0 + q]);
+      stats->tracks_written[q] = (long long)(c.stat[S_WRITE0 + q] + c.stat[S_TWRITE0 + q]);
       stats->transport_ms[q] = transport_ms[q];
       stats->transport_read[q] = (long long)c.stat[S_TREAD0 + q];
       stats->transport_written[q] = (long long)c.stat[S_TWRITE0 + q];

@@ -237,6 +237,27 @@ def test_steps_per_launch_leaves_results_unchanged(dm):
     assert runs[2][1]["iterations"] < runs[0][1]["iterations"]
 
 
+@pytest.mark.parametrize("profile", [0, 1])
+def test_record_counters_are_consistent(dm, profile):
+    """The record statistics of the batched engine, counted in three places
+    (the transport kernels per warp, k_finish from the interaction buffers'
+    counters, the interaction kernels per lane): every record a transport
+    kernel queued is read once by an interaction kernel, a transport kernel
+    writes no more records than it read, and its steps are the run's steps;
+    with the graph (profile 0) and without it (profile 1)."""
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(40, 40)
+    _, st, _ = run_gpu(dm, cfg, prims, nvol, precision=1, profile=profile)
+    cfg.profile = 0
+    assert st["errors"] == 0
+    for q in range(3):
+        assert st["transport_queued"][q] <= st["transport_written"][q] <= st["transport_read"][q]
+        assert st["tracks_read"][q] - st["transport_read"][q] == st["transport_queued"][q], q
+        assert st["tracks_written"][q] >= st["transport_written"][q]
+    assert sum(st["transport_steps"]) == st["steps"]
+    assert st["transport_read"][0] > 0 and st["transport_read"][1] > 0 and st["transport_queued"][2] > 0
+
+
 def test_step_count_distributions_fp32_vs_fp64(dm):
     """Two-sample Kolmogorov-Smirnov test on the primaries' step counts,
     FP32-mixed against FP64 on the same streams."""
