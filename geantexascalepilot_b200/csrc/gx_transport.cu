@@ -1250,22 +1250,24 @@ template <class R> __device__ __forceinline__ void store_track(const Store<R> &s
 
 __device__ __forceinline__ unsigned lane_id() { return threadIdx.x & 31u; }
 
-// Reserve `cnt` consecutive slots per lane in counter *ctr: one atomic per
-// warp, returns this lane's first slot.
+__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Reserve `cnt` consecutive slots per lane (0 <= cnt <= 3: a survivor and up
+// to two secondaries) in counter *ctr: one atomic per warp, returns this
+// lane's first slot.  The lanes' counts go in as two ballots (their bits 0
+// and 1), so the exclusive prefix is two popcounts instead of a shuffle scan;
+// the slots are those of the scan, in lane order.
 __device__ __forceinline__ long long warp_reserve(unsigned long long *ctr, int cnt)
 {
-  unsigned lane = lane_id();
-  int incl = cnt;
-#pragma unroll
-  for (int off = 1; off < 32; off <<= 1) {
-    int v = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= (unsigned)off) incl += v;
-  }
-  int total = __shfl_sync(0xffffffffu, incl, 31);
+  const unsigned b0 = __ballot_sync(0xffffffffu, cnt & 1), b1 = __ballot_sync(0xffffffffu, cnt & 2);
+  const int total = __popc(b0) + 2 * __popc(b1);
+  if (total == 0) return 0;
+  const unsigned lt = lanemask_lt();
+  const int leader = __ffs(b0 | b1) - 1;
   unsigned long long base = 0;
-  if (lane == 31 && total > 0) base = atomicAdd(ctr, (unsigned long long)total);
-  base = __shfl_sync(0xffffffffu, base, 31);
-  return (long long)base + incl - cnt;
+  if ((int)lane_id() == leader) base = atomicAdd(ctr, (unsigned long long)total);
+  base = __shfl_sync(0xffffffffu, base, leader);
+  return (long long)base + __popc(b0 & lt) + 2 * __popc(b1 & lt);
 }
 
 // Write a track to store q, or to q's overflow stack when the store is full.
@@ -1465,7 +1467,6 @@ template <class R, int PT, int K> __global__ void __launch_bounds__(256, 2) k_st
 // and stay unbounded (255).
 template <class R> constexpr int kMinBlocks = sizeof(R) == 8 ? 2 : 0; // 0: no minimum
 template <class R, int K> constexpr int kMaxRegs = sizeof(R) == 8 ? 128 : (K == 0 ? 96 : 255);
-__device__ __forceinline__ unsigned lanemask_lt() { return (1u << lane_id()) - 1u; }
 
 // One slot per flagged lane in counter *ctr (ballot and popcount, one atomic
 // per warp when any lane is flagged); returns this lane's slot, 0 for lanes
@@ -2080,12 +2081,17 @@ static void enqueue_iteration(const Launch<R> &L, Engine *e, cudaStream_t s, boo
     se = e->s1;
     sp = e->s2;
   }
-  transport_for<R, 0>(L)<<<L.grid, L.block, L.smem, sg>>>(A);
-  if (interact) enqueue_interactions<R, 0>(L, A, sg);
-  transport_for<R, 1>(L)<<<L.grid, L.block, L.smem, se>>>(A);
-  if (interact) enqueue_interactions<R, 1>(L, A, se);
+  // Each type's transport kernel fills every SM, so the three run nearly one
+  // after another, the next one's blocks taking the SMs the previous one's
+  // blocks leave.  Positrons go first: their chain (a transport kernel with
+  // about one record per lane, then three interaction kernels) is the one
+  // that ends an iteration most often when it is dispatched last.
   transport_for<R, 2>(L)<<<L.grid, L.block, L.smem, sp>>>(A);
   if (interact) enqueue_interactions<R, 2>(L, A, sp);
+  transport_for<R, 1>(L)<<<L.grid, L.block, L.smem, se>>>(A);
+  if (interact) enqueue_interactions<R, 1>(L, A, se);
+  transport_for<R, 0>(L)<<<L.grid, L.block, L.smem, sg>>>(A);
+  if (interact) enqueue_interactions<R, 0>(L, A, sg);
   if (concurrent) {
     cudaEventRecord(e->ev_j1, e->s1);
     cudaEventRecord(e->ev_j2, e->s2);
