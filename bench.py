@@ -471,10 +471,13 @@ def main():
             mt, stt, _, _ = timed(1, 1, 1, 1, c=c, tens=tens, events=evx, out=ox)
             rec["autotuned"] = {"track_steps_per_s": stt / (mt / 1e3), "primaries_per_s": len(pr[0]) / (mt / 1e3),
                                 "ms": mt, "steps": int(stt), "over_default": (stt / mt) / (s32 / m32),
-                                "setting": {k: trials[0][k] for k in LAUNCH_KEYS}, "trials": len(trials),
+                                "setting": dict({k: trials[0][k] for k in LAUNCH_KEYS},
+                                                fetch_min_gamma=trials[0]["fetch_min_gamma"]),
+                                "trials": len(trials),
                                 "tuned_on": "primaries 0-%d, one run per setting" % (nt - 1)}
             for k in LAUNCH_KEYS:
                 setattr(c, k, 0)
+            c.fetch_min_by_type[0] = 0
         extra[name] = rec
     out["other_workloads"] = extra
 

@@ -44,7 +44,7 @@ class TransportConfig(C.Structure):
                 ("engine", I), ("block_size", I), ("blocks_per_sm", I), ("capacity", LL), ("refill_below", LL),
                 ("graph_iters", I), ("profile", I), ("wave_energy", D), ("steps_per_launch", I), ("msc", I),
                 ("field_map", I), ("steps_per_launch_by_type", I * 3), ("interaction_interval", I),
-                ("fp64_parity", I)]
+                ("fp64_parity", I), ("fetch_min_by_type", I * 3)]
 
 
 class TrackSoAStruct(C.Structure):
@@ -97,11 +97,12 @@ class AutotuneReport(C.Structure):
                 ("graph_iters", I * AUTOTUNE_MAX_TRIALS),
                 ("refill_below", LL * AUTOTUNE_MAX_TRIALS), ("wave_energy", D * AUTOTUNE_MAX_TRIALS),
                 ("interaction_interval", I * AUTOTUNE_MAX_TRIALS),
-                ("kernel_ms", D * AUTOTUNE_MAX_TRIALS), ("steps_per_ms", D * AUTOTUNE_MAX_TRIALS)]
+                ("kernel_ms", D * AUTOTUNE_MAX_TRIALS), ("steps_per_ms", D * AUTOTUNE_MAX_TRIALS),
+                ("fetch_min_gamma", I * AUTOTUNE_MAX_TRIALS)]
 
     def as_list(self):
         keys = ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy",
-                "interaction_interval", "kernel_ms", "steps_per_ms")
+                "interaction_interval", "fetch_min_gamma", "kernel_ms", "steps_per_ms")
         return [{k: getattr(self, k)[i] for k in keys} for i in range(self.trials)]
 
 

@@ -9,7 +9,9 @@
 // transport launch, then the number of iterations per CUDA-graph launch, then
 // the refill threshold, then the primary energy per injection wave, then the
 // compaction interval (how many iterations interacting tracks wait in their
-// buffers before the interaction kernels compact them back into the stores).
+// buffers before the interaction kernels compact them back into the stores),
+// then the idle lanes a warp of the photon transport kernel waits for before
+// it takes new records.
 // Each candidate transports the caller's primaries completely; its score is
 // track-steps per millisecond of device time, the best of `repeats` runs (the
 // first run of a new launch shape also captures its graph).
@@ -25,6 +27,7 @@ struct Trial {
   long long refill_below;
   double wave_energy;
   int interval;
+  int fetch_g; // idle lanes before a warp of the photon kernel takes new records
 };
 
 } // namespace
@@ -59,7 +62,8 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
                 base.steps_per_launch > 0 ? base.steps_per_launch : kDefaultStepsPerLaunch,
                 base.graph_iters > 0 ? base.graph_iters : 16,
                 base.refill_below > 0 ? base.refill_below : cap / 2, base.wave_energy,
-                base.interaction_interval > 0 ? base.interaction_interval : 1};
+                base.interaction_interval > 0 ? base.interaction_interval : 1,
+                base.fetch_min_by_type[0] > 0 ? base.fetch_min_by_type[0] : default_fetch_min(base, 0)};
 
   auto measure = [&](const Trial &t) -> double {
     gx_transport_config c = base;
@@ -70,6 +74,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     c.refill_below = t.refill_below;
     c.wave_energy = t.wave_energy;
     c.interaction_interval = t.interval;
+    c.fetch_min_by_type[0] = t.fetch_g;
     double best_ms = 0.0, rate = 0.0;
     for (int r = 0; r < repeats; ++r) {
       cudaMemsetAsync(edep, 0, nt * sizeof(double), s);
@@ -92,6 +97,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
       rep->refill_below[ntrials] = t.refill_below;
       rep->wave_energy[ntrials] = t.wave_energy;
       rep->interaction_interval[ntrials] = t.interval;
+      rep->fetch_min_gamma[ntrials] = t.fetch_g;
       rep->kernel_ms[ntrials] = best_ms;
       rep->steps_per_ms[ntrials] = rate;
     }
@@ -152,6 +158,13 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
     t.interval = k;
     consider(t);
   }
+  const Trial after_interval = best;
+  for (int f : {1, 8, 16, 24}) {
+    if (f == after_interval.fetch_g) continue;
+    Trial t = after_interval;
+    t.fetch_g = f;
+    consider(t);
+  }
   cudaFree(edep);
   if (rep) rep->trials = ntrials < GX_AUTOTUNE_MAX_TRIALS ? ntrials : GX_AUTOTUNE_MAX_TRIALS;
   if (rc) return rc;
@@ -163,5 +176,6 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   cfg->refill_below = best.refill_below;
   cfg->wave_energy = best.wave_energy;
   cfg->interaction_interval = best.interval;
+  cfg->fetch_min_by_type[0] = best.fetch_g;
   return GX_OK;
 }

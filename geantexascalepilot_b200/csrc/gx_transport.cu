@@ -129,6 +129,7 @@ template <class R> struct Args {
   Store<R> ibuf[3][3];
   long long qcap;
   int step_budget[3]; // steps of one track per transport launch, at most, per particle type
+  int fetch_min[3];   // idle lanes of a warp before it takes new records, per particle type
 };
 
 // ---------------------------------------------------------------- geometry
@@ -1508,7 +1509,7 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
   if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
-  const int budget = a.step_budget[PT];
+  const int budget = a.step_budget[PT], fetch_min = a.fetch_min[PT];
   Track<R> t;
   StepCtx<R> c;
   GammaXs<R> gxs;
@@ -1517,8 +1518,9 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
   bool infield = false;           // in the middle of a step (helix sub-steps)
   int nst = 0;
   for (;;) {
+    // new records once fetch_min lanes are idle (or all are: the last ones)
     const unsigned need = __ballot_sync(0xffffffffu, !have);
-    if (need && more) {
+    if (need && more && (__popc(need) >= fetch_min || need == 0xffffffffu)) {
       const int leader = __ffs(need) - 1;
       unsigned long long base = 0;
       if ((int)lane_id() == leader) base = atomicAdd((unsigned long long *)&ctl->take[PT], (unsigned long long)__popc(need));
@@ -2262,6 +2264,12 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
     for (int q = 0; q < 3; ++q)
       L.a.step_budget[q] = cfg->steps_per_launch_by_type[q] > 0 ? cfg->steps_per_launch_by_type[q]
                                                                 : (q == 2 ? std::max(1, spl / 4) : spl);
+    // a warp refills when this many of its lanes are idle: a photon takes a
+    // few cheap boundary-crossing steps, so the new-track work (record load,
+    // NIL draws, cross sections) would otherwise run for one or two lanes in
+    // most passes of the photon kernel
+    for (int q = 0; q < 3; ++q)
+      L.a.fetch_min[q] = cfg->fetch_min_by_type[q] > 0 ? cfg->fetch_min_by_type[q] : default_fetch_min(*cfg, q);
   }
   if (off > E->pool_bytes) return set_error(GX_ERR_OVERFLOW, "transport pool layout");
   L.a.d = C->dev;
@@ -2862,6 +2870,9 @@ static int check_config(const Ctx *C, const gx_transport_config *cfg, int nvol, 
                                  "layered geometry and no multiple scattering", who);
   if (cfg->interaction_interval < 0 || cfg->interaction_interval > 64)
     return set_error(GX_ERR_ARG, "%s: interaction_interval must be 0 .. 64", who);
+  for (int q = 0; q < 3; ++q)
+    if (cfg->fetch_min_by_type[q] < 0 || cfg->fetch_min_by_type[q] > 32)
+      return set_error(GX_ERR_ARG, "%s: fetch_min_by_type must be 0 .. 32", who);
   if (cfg->field_map && !C->host.fmap)
     return set_error(GX_ERR_ARG, "%s: field_map = 1 without a field map (gx_ctx_load_field_map)", who);
   if (cfg->geometry < 0 || cfg->geometry > 2) return set_error(GX_ERR_ARG, "%s: bad geometry", who);

@@ -304,6 +304,13 @@ typedef struct {
                               spline and ionisation forms, the general helix step and the elementary functions
                               of gx_math.h, the operations of the CPU oracle in its order, so that the two
                               agree track by track; 0: the library's FP64 kernels */
+  int fetch_min_by_type[3]; /* batched engine: a warp of the transport kernel of gamma, e-, e+ takes new
+                              records from its store only once at least this many of its 32 lanes are
+                              idle (or all are): the record loads, NIL draws and cross sections of new
+                              tracks then run for several lanes at once instead of one or two in every
+                              pass (0: the defaults -- 12 for the photons of the FP32-mixed engine in
+                              the layered geometry, 1 for the rest; 1 to 32).  Results do not depend
+                              on it. */
 } gx_transport_config;
 
 typedef struct {
@@ -541,11 +548,12 @@ int gx_transport_tracks(gx_ctx *ctx, const gx_transport_config *cfg, const gx_tr
  * launch {4, 8, 32, 64}, then the refill threshold {1/8, 1/4, 3/4 of the
  * capacity}, then the primary energy per injection wave {1/4, 1/2, 2 x the
  * default}, then the compaction interval (interaction_interval) {2, 4, 8},
- * each coordinate from the best so far.  Score: track-steps per millisecond of
+ * then the photon kernel's fetch threshold (fetch_min_by_type[0]) {1, 8, 16,
+ * 24} beside the default, each coordinate from the best so far.  Score: track-steps per millisecond of
  * device time, best of `repeats` runs (at least 1; the first run of a new
  * launch shape includes its graph capture).  Writes the winner into
  * cfg->block_size, blocks_per_sm, steps_per_launch, graph_iters,
- * refill_below, wave_energy and interaction_interval; report (optional) lists
+ * refill_below, wave_energy, interaction_interval and fetch_min_by_type[0]; report (optional) lists
  * every trial.  cfg->engine must be 1; the precision and capacity are kept. */
 #define GX_AUTOTUNE_MAX_TRIALS 64
 typedef struct {
@@ -557,6 +565,7 @@ typedef struct {
   int interaction_interval[GX_AUTOTUNE_MAX_TRIALS];
   double kernel_ms[GX_AUTOTUNE_MAX_TRIALS];    /* device time, best of the repeats (0: did not complete) */
   double steps_per_ms[GX_AUTOTUNE_MAX_TRIALS]; /* track-steps per device millisecond */
+  int fetch_min_gamma[GX_AUTOTUNE_MAX_TRIALS];  /* fetch_min_by_type[0] of the trial */
 } gx_autotune_report;
 int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, const int *d_type, const double *d_E,
                           const double *d_pos, const double *d_dir, const int *d_event, int nvol, int repeats,

@@ -186,10 +186,12 @@ def test_autotune_and_launch_settings_leave_results_unchanged(dm):
     # the sweep spans 64- to 1024-thread blocks and the compaction interval
     assert {t["block_size"] for t in trials} == {64, 128, 256, 512, 1024}
     assert {t["interaction_interval"] for t in trials} >= {1, 2, 4, 8}
+    assert {t["fetch_min_gamma"] for t in trials} >= {1, 8, 16, 24}
     best = trials[0]
     assert best["steps_per_ms"] == max(t["steps_per_ms"] for t in trials) > 0
     assert (cfg.block_size, cfg.blocks_per_sm, cfg.graph_iters, cfg.interaction_interval) == (
         best["block_size"], best["blocks_per_sm"], best["graph_iters"], best["interaction_interval"])
+    assert cfg.fetch_min_by_type[0] == best["fetch_min_gamma"]
     assert cfg.block_size in (64, 128, 256, 512, 1024) and cfg.blocks_per_sm in (1, 2, 4, 5, 6, 8)
     e1, s1, ps1 = run_gpu(dm, cfg, prims, nvol, precision=1, primary_steps=True)
     assert s1["steps"] == s0["steps"] and s1["tracks"] == s0["tracks"]
@@ -198,6 +200,7 @@ def test_autotune_and_launch_settings_leave_results_unchanged(dm):
     for k in ("block_size", "blocks_per_sm", "steps_per_launch", "graph_iters", "refill_below", "wave_energy",
               "interaction_interval"):
         setattr(cfg, k, 0)
+    cfg.fetch_min_by_type[0] = 0
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -235,6 +238,31 @@ def test_steps_per_launch_leaves_results_unchanged(dm):
         assert np.array_equal(ps, runs[0][2])
         np.testing.assert_allclose(e, runs[0][0], rtol=1e-5, atol=1e-6 * runs[0][0].max())
     assert runs[2][1]["iterations"] < runs[0][1]["iterations"]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_fetch_threshold_leaves_results_unchanged(dm, precision):
+    """Warps of the transport kernels that take new records only once many of
+    their lanes are idle (up to all 32) transport the same tracks as warps that
+    refill every idle lane at once; out-of-range thresholds are refused."""
+    import geantexascalepilot_b200 as g
+    from geantexascalepilot_b200 import configs
+    cfg, prims, nvol = configs.c3(8, 8)
+    runs = []
+    for fm in ((1, 1, 1), (0, 0, 0), (32, 32, 32), (7, 5, 3)):
+        for q in range(3):
+            cfg.fetch_min_by_type[q] = fm[q]
+        runs.append(run_gpu(dm, cfg, prims, nvol, precision=precision, primary_steps=True))
+    for e, st, ps in runs[1:]:
+        assert st["steps"] == runs[0][1]["steps"] and st["tracks"] == runs[0][1]["tracks"]
+        assert np.array_equal(ps, runs[0][2])
+        np.testing.assert_allclose(e, runs[0][0], rtol=1e-9, atol=1e-9 * runs[0][0].max())
+    for bad in (33, -1):
+        cfg.fetch_min_by_type[1] = bad
+        with pytest.raises(g.GxError):
+            run_gpu(dm, cfg, prims, nvol, precision=precision)
+    for q in range(3):
+        cfg.fetch_min_by_type[q] = 0
 
 
 @pytest.mark.parametrize("profile", [0, 1])
