@@ -145,6 +145,8 @@ _SIGS = {
                                   C.POINTER(TransportStats)]),
     "gx_transport_autotune": (I, [P, C.POINTER(TransportConfig), I, P, P, P, P, P, I, I, C.POINTER(AutotuneReport),
                                   P]),
+    "gx_timeline_reset": (I, [P]),
+    "gx_timeline_read": (I, [P, P, LL]),
     "gx_egamma_gun": (I, [C.POINTER(GunParams), P, P, P, P, P, P, P]),
     "gx_pdg_to_type": (I, [I]),
     "gx_hepevt_read": (I, [C.c_char_p, I, I, I, P, P, P, P, C.POINTER(I), C.POINTER(I), C.POINTER(I)]),

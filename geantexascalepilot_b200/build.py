@@ -3,6 +3,15 @@
 Compiles every csrc/*.cu for sm_100a (B200) with nvcc and links
 geantexascalepilot_b200/lib/libgxb200.so.  Nothing is JIT-compiled at run
 time; the library is loaded with ctypes by geantexascalepilot_b200._lib.
+
+    python geantexascalepilot_b200/build.py [-v] [--timeline]
+
+--timeline builds the tracing variant instead, lib/libgxb200_timeline.so
+(objects in _build_timeline/): the same sources with GX_TIMELINE defined for
+the transport engine, whose step kernels then record when each kernel of an
+iteration starts and ends (gx_timeline_read).  Load it in place of the
+product with GX_LIB_PATH, e.g. for `python -m geantexascalepilot_b200.run c3
+--timeline out.npy`.
 """
 import concurrent.futures as cf
 import glob
@@ -16,6 +25,8 @@ CSRC = os.path.join(PKG, "csrc")
 LIBDIR = os.path.join(PKG, "lib")
 BUILD = os.path.join(os.path.dirname(PKG), "_build")
 LIB = os.path.join(LIBDIR, "libgxb200.so")
+BUILD_TIMELINE = os.path.join(os.path.dirname(PKG), "_build_timeline")
+LIB_TIMELINE = os.path.join(LIBDIR, "libgxb200_timeline.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
@@ -60,8 +71,8 @@ def _includes(src, seen=None):
     return seen
 
 
-def _compile(src, verbose):
-    obj = os.path.join(BUILD, os.path.basename(src) + ".o")
+def _compile(src, verbose, build_dir=BUILD, timeline=False):
+    obj = os.path.join(build_dir, os.path.basename(src) + ".o")
     # the source, every header of the directory (headers include one another),
     # the .cu files it includes, the ABI header and this script
     deps = (sorted(_includes(src)) + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h")) +
@@ -69,6 +80,8 @@ def _compile(src, verbose):
     if os.path.exists(obj) and os.path.getmtime(obj) >= max(os.path.getmtime(d) for d in deps):
         return obj, ""
     extra = PER_FILE.get(os.path.basename(src), [])
+    if timeline and os.path.basename(src) == "gx_transport.cu":
+        extra = extra + ["-DGX_TIMELINE"]
     cmd = [nvcc()] + ARCH + FLAGS + extra + (["-Xptxas", "-v"] if verbose else []) + ["-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -76,28 +89,29 @@ def _compile(src, verbose):
     return obj, r.stderr
 
 
-def build(verbose=False):
-    os.makedirs(BUILD, exist_ok=True)
+def build(verbose=False, timeline=False):
+    build_dir, lib = (BUILD_TIMELINE, LIB_TIMELINE) if timeline else (BUILD, LIB)
+    os.makedirs(build_dir, exist_ok=True)
     os.makedirs(LIBDIR, exist_ok=True)
     srcs = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
     with cf.ThreadPoolExecutor(max_workers=min(8, len(srcs))) as ex:
-        results = list(ex.map(lambda s: _compile(s, verbose), srcs))
+        results = list(ex.map(lambda s: _compile(s, verbose, build_dir, timeline), srcs))
     objs = [o for o, _ in results]
     if verbose:
         for _, log in results:
             if log:
                 print(log, file=sys.stderr)
-    if os.path.exists(LIB) and os.path.getmtime(LIB) >= max(os.path.getmtime(o) for o in objs):
-        return LIB
-    cmd = [nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+    if os.path.exists(lib) and os.path.getmtime(lib) >= max(os.path.getmtime(o) for o in objs):
+        return lib
+    cmd = [nvcc()] + ARCH + ["-shared", "-o", lib] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"]
     cxx = system_libstdcxx()
     if cxx:
         cmd += ["-Xlinker", cxx]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError("link failed:\n%s\n%s" % (r.stdout, r.stderr))
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":
-    print(build(verbose="-v" in sys.argv))
+    print(build(verbose="-v" in sys.argv, timeline="--timeline" in sys.argv))

@@ -1483,6 +1483,42 @@ __device__ __forceinline__ long long warp_take1(unsigned long long *ctr, bool fl
   return flag ? (long long)base + __popc(m & lanemask_lt()) : 0;
 }
 
+// Timeline tracing (the library built with GX_TIMELINE, a separate build of
+// this file): per iteration and step kernel, the global timer when the first
+// block of the kernel starts and when the last one ends, so that a run shows
+// how the kernels of an iteration follow or overlap one another.  Kernel ids:
+// 0 refill, 1 refill bookkeeping, 2-4 transport of gamma, e-, e+, 5 + 3 type +
+// process the interaction kernels, 14 end of iteration; 512 iterations kept
+// (iteration i in row (i + 1) mod 512; row 0 holds the planning launch).
+// Without GX_TIMELINE the marks compile to nothing.
+#if defined(GX_TIMELINE) && !defined(GX_PARITY)
+constexpr int kTimelineRows = 512, kTimelineKernels = 16;
+__device__ unsigned long long g_timeline[kTimelineRows * kTimelineKernels][2];
+__device__ __forceinline__ int timeline_slot(const Ctl *ctl, int id)
+{
+  const long long it = ((volatile const Ctl *)ctl)->iterations + 1;
+  return (int)((it & (kTimelineRows - 1)) * kTimelineKernels + id);
+}
+__device__ __forceinline__ void timeline_mark(int slot, int end)
+{
+  if (threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (end)
+      atomicMax(&g_timeline[slot][1], t);
+    else
+      atomicMin(&g_timeline[slot][0], t);
+  }
+}
+#define GX_TL_BEGIN(ctl, id)                                                                                          \
+  const int gx_tl_slot = timeline_slot(ctl, id);                                                                     \
+  timeline_mark(gx_tl_slot, 0)
+#define GX_TL_END() timeline_mark(gx_tl_slot, 1)
+#else
+#define GX_TL_BEGIN(ctl, id)
+#define GX_TL_END()
+#endif
+
 // Transport of the tracks of type PT: each lane keeps its track in registers
 // and steps it until the track interacts (it then goes to the interaction
 // buffer of its process), dies, leaves the world, or has taken step_budget
@@ -1505,8 +1541,12 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
   Ctl *ctl = a.ctl;
   const int par = ctl->parity;
   const Store<R> &cur = a.st[par][PT];
+  GX_TL_BEGIN(ctl, 2 + PT);
   const long long n = min(ctl->count[par][PT], cur.cap);
-  if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
+  if ((long long)blockIdx.x * blockDim.x >= n) { // no work for this block (uniform exit)
+    GX_TL_END();
+    return;
+  }
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
   const int budget = a.step_budget[PT], fetch_min = a.fetch_min[PT];
@@ -1590,6 +1630,7 @@ template <class R, int PT, int K> __device__ __forceinline__ void transport_body
     if (done && (r != kAlive || nst >= budget)) have = false;
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err, S_TSTEP0 + PT);
+  GX_TL_END();
 }
 
 template <class R, int PT, int K>
@@ -1624,8 +1665,12 @@ template <class R, int PT, int PROC> __device__ __forceinline__ void interact_bo
   Ctl *ctl = a.ctl;
   const int par = ctl->parity;
   const Store<R> &buf = a.ibuf[PT][PROC];
+  GX_TL_BEGIN(ctl, 5 + 3 * PT + PROC);
   const long long n = min(ctl->qcount[PT][PROC], a.qcap);
-  if ((long long)blockIdx.x * blockDim.x >= n) return; // no work for this block (uniform exit)
+  if ((long long)blockIdx.x * blockDim.x >= n) { // no work for this block (uniform exit)
+    GX_TL_END();
+    return;
+  }
   Local L;
   tally_begin(L, a.g, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
   const long long stride = (long long)gridDim.x * blockDim.x;
@@ -1645,6 +1690,7 @@ template <class R, int PT, int PROC> __device__ __forceinline__ void interact_bo
     emit_tracks<R, PT>(a, ctl, par, active, alive, t, sec, L);
   }
   tally_end(L, ctl, a.edep, sm_edep, sm_stat, sm_esc, &sm_err);
+  GX_TL_END();
 }
 
 template <class R, int PT, int PROC>
@@ -1664,6 +1710,7 @@ __global__ void __launch_bounds__(1024, 1) k_interact_wide(const Args<R> *__rest
 // tracks waiting in them count as pending.
 __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap2, int nstores, int interacted)
 {
+  GX_TL_BEGIN(ctl, 14);
   int par = ctl->parity, np = par ^ 1;
   const long long cap[3] = {cap0, cap1, cap2};
   const long long refill_below = ctl->refill_below, stack_cap = ctl->stack_cap;
@@ -1734,6 +1781,7 @@ __global__ void k_finish(Ctl *ctl, long long cap0, long long cap1, long long cap
   ctl->in_flight = fl;
   ctl->pending = pend;
   if (fl > ctl->peak) ctl->peak = fl;
+  GX_TL_END();
 }
 
 // Inclusive prefix sum of the primary energies, one block: each thread scans a
@@ -1869,11 +1917,18 @@ template <class R> __device__ __forceinline__ void refill_body(const Args<R> &a)
 
 // launched with the step kernels' block size, up to 1024 threads
 template <class R> __global__ void __launch_bounds__(1024) k_refill(Args<R> a) { refill_body(a); }
-template <class R> __global__ void __launch_bounds__(1024) k_refill_p(const Args<R> *__restrict__ A) { refill_body(*A); }
+template <class R> __global__ void __launch_bounds__(1024) k_refill_p(const Args<R> *__restrict__ A)
+{
+  GX_TL_BEGIN(A->ctl, 0);
+  refill_body(*A);
+  GX_TL_END();
+}
 
 // Bookkeeping after a refill: the primary cursor.  One thread.
 __global__ void k_refill_done(Ctl *ctl)
 {
+  GX_TL_BEGIN(ctl, 1);
+  GX_TL_END();
   for (int q = 0; q < 3; ++q) ctl->take_stack[q] = 0;
   ctl->prim_next += ctl->take_prim;
   ctl->take_prim = 0;
@@ -2850,6 +2905,47 @@ void gx_transport_config_default(gx_transport_config *c)
   c->nevents = 1;
   c->precision = 0;
   c->engine = 1;
+}
+
+int gx_timeline_reset(gx_ctx *ctx)
+{
+#ifdef GX_TIMELINE
+  if (!ctx) return set_error(GX_ERR_ARG, "gx_timeline_reset: null context");
+  cudaError_t e = cudaSetDevice(reinterpret_cast<Ctx *>(ctx)->device);
+  if (e != cudaSuccess) return cuda_error(e, "gx_timeline_reset: cudaSetDevice");
+  static unsigned long long h[kTimelineRows * kTimelineKernels][2];
+  for (int i = 0; i < kTimelineRows * kTimelineKernels; ++i) {
+    h[i][0] = ~0ULL; // first start: a minimum
+    h[i][1] = 0ULL;  // last end: a maximum
+  }
+  if ((e = cudaMemcpyToSymbol(g_timeline, h, sizeof(h))) != cudaSuccess) return cuda_error(e, "gx_timeline_reset");
+  return GX_OK;
+#else
+  (void)ctx;
+  return set_error(GX_ERR_ARG, "gx_timeline_reset: the library was built without GX_TIMELINE "
+                               "(python geantexascalepilot_b200/build.py --timeline builds libgxb200_timeline.so)");
+#endif
+}
+
+int gx_timeline_read(gx_ctx *ctx, unsigned long long *h_out, long long n)
+{
+#ifdef GX_TIMELINE
+  if (!ctx || !h_out) return set_error(GX_ERR_ARG, "gx_timeline_read: null argument");
+  if (n != (long long)kTimelineRows * kTimelineKernels * 2)
+    return set_error(GX_ERR_ARG, "gx_timeline_read: n must be %d", kTimelineRows * kTimelineKernels * 2);
+  cudaError_t e = cudaSetDevice(reinterpret_cast<Ctx *>(ctx)->device);
+  if (e != cudaSuccess) return cuda_error(e, "gx_timeline_read: cudaSetDevice");
+  if ((e = cudaDeviceSynchronize()) != cudaSuccess) return cuda_error(e, "gx_timeline_read: synchronize");
+  if ((e = cudaMemcpyFromSymbol(h_out, g_timeline, sizeof(g_timeline))) != cudaSuccess)
+    return cuda_error(e, "gx_timeline_read");
+  return GX_OK;
+#else
+  (void)ctx;
+  (void)h_out;
+  (void)n;
+  return set_error(GX_ERR_ARG, "gx_timeline_read: the library was built without GX_TIMELINE "
+                               "(python geantexascalepilot_b200/build.py --timeline builds libgxb200_timeline.so)");
+#endif
 }
 
 // The checks of a transport configuration shared by the entry points.

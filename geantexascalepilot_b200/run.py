@@ -6,6 +6,8 @@
     python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --profile --capacity 2097152
     python -m geantexascalepilot_b200.run c3 --geometry csg --msc 1 --field-map
     python -m geantexascalepilot_b200.run c3 --electrons 2000 --photons 2000 --iterations 30
+    GX_LIB_PATH=geantexascalepilot_b200/lib/libgxb200_timeline.so \
+        python -m geantexascalepilot_b200.run c3 --repeat 2 --timeline c3.npy
 
 Prints one JSON line: the workload, the transport statistics (steps,
 propagation sub-steps, tracks, secondaries, iterations, per-kernel device
@@ -14,6 +16,9 @@ times in profile mode) and the device time of the transport loop.  With
 engine stops after N iterations: the statistics are those of the first N
 iterations, and the tracks still alive are handed back (their count is
 printed); the difference of two such runs gives one iteration's work.
+With --timeline FILE (the library's tracing build, see build.py) the last
+repetition's per-iteration kernel timeline is saved to FILE (numpy) and
+summarised in the JSON line.
 """
 import argparse
 import json
@@ -43,6 +48,8 @@ def main(argv=None):
                    help="the shipped CMS field map (Runge-Kutta sub-steps) instead of the workload's uniform field")
     p.add_argument("--iterations", type=int, default=0,
                    help="stop after this many iterations and hand the live tracks back (0: run to completion)")
+    p.add_argument("--timeline", default=None,
+                   help="with the tracing build of the library: save the last repetition's kernel timeline here")
     p.add_argument("--device", type=int, default=0)
     a = p.parse_args(argv)
 
@@ -81,7 +88,11 @@ def main(argv=None):
         out["autotune"] = trials[0]
         out["autotune_trials"] = trials
         cfg.profile = int(a.profile)
-    for _ in range(a.repeat):
+    for rep in range(a.repeat):
+        if a.timeline and rep == a.repeat - 1:
+            from geantexascalepilot_b200 import timeline
+            torch.cuda.synchronize()
+            timeline.reset(dm)
         if a.iterations > 0:
             tin = gx.TrackSoA.from_primaries(cfg, *prims[:4], events=prims[4])
             cap = min(4 * (a.capacity or (1 << 24)), 1 << 24)
@@ -92,6 +103,11 @@ def main(argv=None):
         else:
             edep, st, _ = gx.transport(dm, cfg, *prims[:4], events=prims[4], nvol=nvol)
     torch.cuda.synchronize()
+    if a.timeline:
+        import numpy as np
+        rec = timeline.read(dm)
+        np.save(a.timeline, rec)
+        out["timeline"] = timeline.summary(rec, st["iterations"])
     out["stats"] = st
     out["edep_total"] = float(edep.sum().item())
     out["track_steps_per_s"] = st["steps"] / (st["kernel_ms"] / 1e3) if st["kernel_ms"] > 0 else None

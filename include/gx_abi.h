@@ -571,6 +571,20 @@ int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int nprim, cons
                           const double *d_pos, const double *d_dir, const int *d_event, int nvol, int repeats,
                           gx_autotune_report *report, gx_stream_t s);
 
+/* Timeline tracing of the batched engine, in the library's tracing build
+ * (geantexascalepilot_b200/build.py --timeline: lib/libgxb200_timeline.so);
+ * the reference traces with timemory (its TIMEMORY_* markers), which has no
+ * place in this build.  The step kernels of that build record, per iteration
+ * and kernel, the GPU global timer (ns) at the start of their first block and
+ * at the end of their last: h_out[((r * 16 + k) * 2) + {0, 1}] for row r =
+ * (iteration + 1) mod 512 and kernel k (0 refill, 1 refill bookkeeping, 2-4
+ * transport of gamma, e-, e+, 5 + 3 type + process interactions, 14 end of
+ * iteration); a start of 2^64 - 1 means the kernel did not run.  reset clears
+ * the record, read copies it out after a device synchronisation (n = 16384).
+ * The product library returns GX_ERR_ARG from both. */
+int gx_timeline_reset(gx_ctx *ctx);
+int gx_timeline_read(gx_ctx *ctx, unsigned long long *h_out, long long n);
+
 /* gx_transport_run without any device allocation.  No counterpart in the
  * reference.  For callers that must not allocate device memory while they
  * run: a host framework whose caching allocator already owns the device
