@@ -1351,8 +1351,24 @@ template <class T> __device__ __forceinline__ T take3(T (&v)[3], int q, T inc)
   return r;
 }
 
+// The NIL of every discrete process of track t that has none (<= 0), drawn
+// from the track's stream in process order -- the draws its next GPIL would
+// make first.  Drawn where a track is created or survives an interaction,
+// right after the stream's other draws there, they are the same numbers in
+// the same order on the same stream, and the transport kernels' GPIL then
+// finds them set: the draws run convergently in the kernel that makes the
+// tracks instead of for one or two lanes in most passes of a transport warp.
+template <class R> __device__ __forceinline__ void draw_nils(Track<R> &t, Mrg &rng)
+{
+  const int np = (t.type == 1) ? 2 : 3;
+#pragma unroll
+  for (int i = 0; i < 3; ++i)
+    if (i < np && t.nil[i] <= R(0)) t.nil[i] = -M<R>::log(rng.template u<R>());
+}
+
 // After a track's interaction: its secondaries (streams seeded from the
-// parent, in order) and the survivor go to the next stores, destination =
+// parent, in order, their NILs drawn) and the survivor (its spent NIL drawn
+// anew) go to the next stores, destination =
 // particle type, or store 0 with one mixed store.  Every lane of the warp
 // calls this (the slot reservations are warp-wide); `active` lanes write.
 // SRC is the store the tracks were read from (for the write statistics).
@@ -1388,6 +1404,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
     c.msc_r0 = R(-1);
     Mrg cr;
     rng.seed_child(cr);
+    draw_nils(c, cr);
     c.set_rng(cr);
     c.vol = t.vol;
     c.event = t.event;
@@ -1401,6 +1418,7 @@ __device__ __forceinline__ void emit_tracks(const Args<R> &a, Ctl *ctl, int par,
     L.st[S_SEC2] = sc[2];
     L.st[S_WRITE0 + SRC]++;
   }
+  if (alive) draw_nils(t, rng);
   t.set_rng(rng);
   if (alive) {
     const int q = mixed ? 0 : t.type;
