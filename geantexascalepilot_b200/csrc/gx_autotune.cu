@@ -146,7 +146,7 @@ extern "C" int gx_transport_autotune(gx_ctx *ctx, gx_transport_config *cfg, int 
   }
   const Trial after_refill = best;
   // multiples of the engine's default widen or narrow the injection waves
-  const double wave0 = default_wave_energy(cap, 0.8);
+  const double wave0 = default_wave_energy(cap, kWaveFillBatched);
   for (double m : {0.25, 0.5, 2.0}) {
     Trial t = after_refill;
     t.wave_energy = m * wave0;

@@ -2424,7 +2424,7 @@ static int run(Ctx *C, const gx_transport_config *cfg, int nprim, const int *d_t
   h.nprim = nprim;
   h.iterations = -1; // the planning launch below is not an iteration
   h.cumE = E->cumE;
-  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, batched ? 0.8 : 0.4);
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, batched ? kWaveFillBatched : kWaveFillPlain);
   h.refill_below = L.a.refill_below;
   h.stack_cap = stack_cap;
   err = cudaMemcpyAsync(E->ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s);
@@ -3299,7 +3299,7 @@ extern "C" int gx_transport_run_noalloc(gx_ctx *ctx, const gx_transport_config *
   h.nprim = nprim;
   h.iterations = -1;
   h.cumE = cumE;
-  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, 0.4);
+  h.wave_energy = cfg->wave_energy > 0 ? cfg->wave_energy : default_wave_energy(cap, kWaveFillPlain);
   h.refill_below = L.a.refill_below;
   h.stack_cap = cap;
   if ((err = cudaMemcpyAsync(ctl, &h, sizeof(Ctl), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
