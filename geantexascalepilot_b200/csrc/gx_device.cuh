@@ -294,6 +294,51 @@ __device__ __forceinline__ double vec_invrange_ref(const Data &d, const VecDesc 
          ((a * a * a - a) * __ldg(&d2[n1]) + (b * b * b - b) * __ldg(&d2[n1 + 1])) * delta * delta / 6.0;
 }
 
+// The FP64 value of the polynomial form at e with the bin found from the FP32
+// logarithm and checked against the two nodes around it (the FP32 log is off
+// by far less than one bin, so one step down or up gives the interval that
+// holds e): the FP32-mixed engine's range at the start of a step that loses
+// more than 1% of its energy, without an FP64 logarithm.
+__device__ __forceinline__ double vec_value_f64_f32bin(const Data &d, const VecDesc &v, double e)
+{
+  if (e <= v.emin) return __ldg(&d.c64[6 * v.off + 2]);
+  if (e >= v.emax) return __ldg(&d.y[v.off + v.n - 1]);
+  int bin = (int)(__logf((float)e) * v.invdbinf - v.basef);
+  bin = min(max(bin, 0), v.n - 2);
+  const double *c = d.c64 + 6 * (v.off + bin);
+  double x1 = __ldg(&c[0]);
+  if (bin > 0 && e < x1) {
+    c -= 6;
+    x1 = __ldg(&c[0]);
+  } else if (bin < v.n - 2 && e >= __ldg(&c[6])) {
+    c += 6;
+    x1 = __ldg(&c[0]);
+  }
+  double u = (e - x1) * __ldg(&c[1]);
+  return __ldg(&c[2]) + u * (__ldg(&c[3]) + u * (__ldg(&c[4]) + u * __ldg(&c[5])));
+}
+// InvRangeValue in FP64 with one reciprocal of the interval instead of three
+// divisions (the FP32-mixed engine; the reference form is vec_invrange_ref).
+__device__ __forceinline__ double vec_invrange_fast(const Data &d, const VecDesc &v, double e)
+{
+  const double *x = d.x + v.off, *y = d.y + v.off, *d2 = d.d2 + v.off;
+  if (e <= v.emin) return __ldg(&y[0]);
+  if (e >= v.emax) return __ldg(&y[v.n - 1]);
+  int n1 = 0, n2 = v.n / 2, n3 = v.n - 1;
+  while (n1 != n3 - 1) {
+    if (e > __ldg(&x[n2]))
+      n1 = n2;
+    else
+      n3 = n2;
+    n2 = n1 + (n3 - n1 + 1) / 2;
+  }
+  const double x1 = __ldg(&x[n1]), x2 = __ldg(&x[n1 + 1]);
+  const double delta = x2 - x1, inv = 1.0 / delta;
+  const double a = (x2 - e) * inv, b = (e - x1) * inv;
+  return a * __ldg(&y[n1]) + b * __ldg(&y[n1 + 1]) +
+         ((a * a * a - a) * __ldg(&d2[n1]) + (b * b * b - b) * __ldg(&d2[n1 + 1])) * (delta * delta * (1.0 / 6.0));
+}
+
 // Value() in the polynomial form y = c0 + u (c1 + u (c2 + u c3)), u = (E - x1)/delta:
 // one 24/48-byte record per bin.  Same spline, same bin choice.
 template <class R> __device__ __forceinline__ R vec_value_fast(const Data &d, const VecDesc &v, R e);

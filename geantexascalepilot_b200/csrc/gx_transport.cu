@@ -403,8 +403,16 @@ __device__ __forceinline__ R along_loss(const Data &d, int type, int mat, double
   if (energy < R(kMinE)) dedx *= M<R>::sqrt(energy / R(kMinE));
   R eloss = (R)step * dedx;
   if (eloss > energy * R(0.01)) {
-    double r64 = vec_value_fast<double>(d, d.vec[ep ? GX_Range_ep : GX_Range_em][mat], (double)energy) - step;
-    eloss = (R)((double)energy - vec_invrange_ref(d, d.vec[ep ? GX_InverseRange_ep : GX_InverseRange_em][mat], r64));
+    const VecDesc &vr = d.vec[ep ? GX_Range_ep : GX_Range_em][mat];
+    const VecDesc &vi = d.vec[ep ? GX_InverseRange_ep : GX_InverseRange_em][mat];
+    if constexpr (sizeof(R) == 4) {
+      // the FP32-mixed engine: bin from the FP32 logarithm, one reciprocal
+      const double r64 = vec_value_f64_f32bin(d, vr, (double)energy) - step;
+      eloss = (R)((double)energy - vec_invrange_fast(d, vi, r64));
+    } else {
+      const double r64 = vec_value_fast<double>(d, vr, (double)energy) - step;
+      eloss = (R)((double)energy - vec_invrange_ref(d, vi, r64));
+    }
   }
   R finalE = energy - eloss;
   if (finalE < R(kMinE)) {
