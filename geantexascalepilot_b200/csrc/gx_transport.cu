@@ -229,6 +229,50 @@ __device__ __forceinline__ double dist_to_out(const Geom &g, int vol, const doub
   return dist < 0 ? 0 : dist;
 }
 
+// The same distance with one division (the FP32-mixed engine): each plane's
+// candidate kept as a fraction num / den with den > 0, candidates compared by
+// cross-multiplication in the order the loop above takes them (axis planes
+// first, ties to the earlier), and only the nearest divided out.
+__device__ __forceinline__ double dist_to_out_1div(const Geom &g, int vol, const double *p, const double *d,
+                                                   int &plane)
+{
+  int a = g.axis;
+  double lo, hi;
+  slab_bounds(g, vol, lo, hi);
+  plane = 0;
+  double num = 1.7976931348623157e308, den = 1.0;
+  const double pa = comp(p, a), da = comp(d, a);
+  if (da > 0) {
+    num = hi - pa;
+    den = da;
+    plane = 1;
+  } else if (da < 0) {
+    num = pa - lo;
+    den = -da;
+    plane = -1;
+  }
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    if (b == a) continue;
+    const double h = thalf(g, b), q = p[b] - tcentre(g, b);
+    double n = 0.0, m = 0.0;
+    if (d[b] > 0) {
+      n = h - q;
+      m = d[b];
+    } else if (d[b] < 0) {
+      n = h + q;
+      m = -d[b];
+    }
+    if (m > 0 && n * den < num * m) {
+      num = n;
+      den = m;
+      plane = 2;
+    }
+  }
+  const double dist = num / den;
+  return dist < 0 ? 0 : dist;
+}
+
 __device__ __forceinline__ double safety(const Geom &g, int vol, const double *p)
 {
   int a = g.axis;
@@ -299,13 +343,16 @@ template <int K> __device__ __forceinline__ double nav_safety(const Geom &g, int
 }
 // Straight-line distance to the next boundary.  plane: the analytic
 // navigator's face code, or the CSG child entered (-1: leaving the volume);
-// the CSG navigator skips children met only beyond limit.
-template <int K>
+// the CSG navigator skips children met only beyond limit.  ONE_DIV (the
+// FP32-mixed engine): the analytic navigator's distance with one division.
+template <int K, bool ONE_DIV = false>
 __device__ __forceinline__ double nav_distance(const Geom &g, int vol, const double *p, const double *d, double limit,
                                                int &plane)
 {
   if constexpr ((K & kKindCsg) != 0)
     return csg_step<kSolidsOf<K>>(g.csg, vol, p, d, limit, plane);
+  else if constexpr (ONE_DIV)
+    return dist_to_out_1div(g, vol, p, d, plane);
   else
     return dist_to_out(g, vol, p, d, plane);
 }
@@ -927,7 +974,7 @@ __device__ __forceinline__ bool step_move_begin(const Geom &g, Track<R> &t, Step
   int plane;
   double dir[3] = {(double)t.dir[0], (double)t.dir[1], (double)t.dir[2]};
   double ps = (double)pstep;
-  double dd = nav_distance<K>(g, t.vol, t.pos, dir, ps, plane);
+  double dd = nav_distance<K, sizeof(R) == 4>(g, t.vol, t.pos, dir, ps, plane);
   if (dd < ps) {
     c.total = dd;
     c.crossed = true;
@@ -1050,7 +1097,8 @@ __device__ __forceinline__ bool field_substep(const Data &d, const Geom &g, Trac
   double saf = nav_safety<K>(g, t.vol, t.pos);
   double snext = (saf > remaining)
                      ? remaining
-                     : fmax(2e-9, fmin(nav_distance<K>(g, t.vol, t.pos, dd, remaining, plane), remaining) + 2e-9);
+                     : fmax(2e-9, fmin(nav_distance<K, sizeof(R) == 4>(g, t.vol, t.pos, dd, remaining, plane),
+                                       remaining) + 2e-9);
   double s;
   if constexpr ((K & kKindFieldMap) != 0) {
     s = field_map_substep<R>(d, g, t, remaining, saf, snext);
