@@ -997,6 +997,22 @@ __device__ __forceinline__ double pe_xs_sandia(const Data &d, int Z, double dens
   double s = i1 * (__ldg(&a[1]) + i1 * (__ldg(&a[2]) + i1 * (__ldg(&a[3]) + i1 * __ldg(&a[4]))));
   return fmax(s, 0.0) * density * 0.1;
 }
+// The same for the FP32-mixed engine: the energy scaled by a multiplication,
+// the interval found in FP64 as above, the polynomial in 1/E in FP32 (its
+// reciprocal from the FP32 unit) instead of two FP64 divisions.
+__device__ __forceinline__ float pe_xs_sandia_f(const Data &d, int Z, float density, float e)
+{
+  const double ekev = (double)e * (1.0 / keV);
+  int first = d.cumint[Z - 1], n = d.nint[Z];
+  int row = first + n - 1;
+  while (row > first && ekev < __ldg(&d.sandia[5 * row])) --row;
+  if (ekev < __ldg(&d.sandia[5 * row])) return 0.0f;
+  const double *a = d.sandia + 5 * row;
+  const float i1 = __frcp_rn((float)ekev);
+  const float s = i1 * ((float)__ldg(&a[1]) +
+                        i1 * ((float)__ldg(&a[2]) + i1 * ((float)__ldg(&a[3]) + i1 * (float)__ldg(&a[4]))));
+  return fmaxf(s, 0.0f) * density * 0.1f;
+}
 
 // ------------------------------------------------------------------ helix
 // ConstFieldHelixStepper::DoStep, ConstFieldHelixStepper.hpp:164-239 (FP64)

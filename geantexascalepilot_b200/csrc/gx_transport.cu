@@ -393,8 +393,12 @@ template <class R> __device__ __forceinline__ void cross_sections(const Data &d,
     xs[0] = (e < R(1)) ? tab_value<R>(d, d.vec[GX_Lambda_compt][mat], e)
                        : tab_value<R>(d, d.vec[GX_LambdaPrim_compt][mat], e) / e;
     xs[1] = lambda_tab<R>(d, GX_Lambda_conv, mat, e);
-    xs[2] = (e >= R(0.2)) ? tab_value<R>(d, d.vec[GX_LambdaPrim_phot][mat], e) / e
-                          : (R)pe_xs_sandia(d, (int)d.mat_Z[mat], d.mat_density[mat], (double)e);
+    if (e >= R(0.2))
+      xs[2] = tab_value<R>(d, d.vec[GX_LambdaPrim_phot][mat], e) / e;
+    else if constexpr (sizeof(R) == 4)
+      xs[2] = pe_xs_sandia_f(d, (int)d.mat_Z[mat], (float)d.mat_density[mat], e);
+    else
+      xs[2] = (R)pe_xs_sandia(d, (int)d.mat_Z[mat], d.mat_density[mat], (double)e);
   } else if (type == 1) {
     xs[0] = lambda_tab<R>(d, GX_Lambda_eIoni_em, mat, e);
     xs[1] = lambda_tab<R>(d, GX_Lambda_eBrem_em, mat, e);
